@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Frames/s of the KinectFusion frame step on B200 (one JSON line on rank 0).
+
+Workload (default): the single-session precision form at 512^3 over a 3 m cube, FP16
+TSDF + uint16 weight, split-BF16 J^T J, FP64 solve, ICP {10,5,4}, 512x424 uint16 depth of
+a seeded analytic scene (8 spheres + 2 boxes, ground plane) on an orbit; marching cubes
+every 100 frames.  A step is one frame of src/kinect.cpp:654-695: depth ingest + pyramid,
+ICP, integrate, (recover), raycast.
+
+  value  frames/s with the depth frames already resident in HBM (device timed)
+  e2e    frames/s through the C ABI from pinned host frames: every step copies the
+         uint16 frame host->device and reads the pose/flags back device->host
+Multi-GPU: independent sessions, one per rank (replicas, no collective on the data
+path); value is the total over ranks divided by the slowest rank's time.
+`--impl reference` times the FP64 CPU port of the reference algorithm (the oracle) on
+this host's cores for the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--size", type=int, default=512)
+    p.add_argument("--storage", choices=["f16u16", "f32f32", "rg16i"], default="f16u16")
+    p.add_argument("--jtj", choices=["bf16", "fp32"], default="bf16")
+    p.add_argument("--cpu-frames", type=int, default=4, help="oracle frames timed for cpu_baseline")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(args, n_frames):
+    from oglfusionkinectv2_b200 import synth, _lib as L
+    storage = {"f16u16": L.KF_STORAGE_F16U16, "f32f32": L.KF_STORAGE_F32F32, "rg16i": L.KF_STORAGE_RG16I}[args.storage]
+    jtj = L.KF_JTJ_SPLIT_BF16 if args.jtj == "bf16" else L.KF_JTJ_FP32
+    return synth.precision_c2(n_frames=n_frames, storage=storage, jtj=jtj, size=args.size)
+
+
+def _gen(args_tuple):
+    size, storage, jtj, n, idx = args_tuple
+    from oglfusionkinectv2_b200 import synth
+    w = synth.precision_c2(n_frames=n, storage=storage, jtj=jtj, size=size)
+    return idx, w.frame(idx)
+
+
+def gen_frames(w, indices, procs):
+    """Render frames in a spawn pool (started before any CUDA call)."""
+    import multiprocessing as mp
+    c = w.config
+    jobs = [(c.volumeSize[0], c.storage, c.jtj, w.n_frames, i) for i in indices]
+    if procs <= 1 or len(jobs) < 4:
+        return {i: w.frame(i) for i in indices}
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        return dict(pool.map(_gen, jobs, chunksize=4))
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while the timed region runs."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, device_index: int):
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            self.N = N
+            import torch
+            bus = torch.cuda.get_device_properties(device_index).pci_bus_id if hasattr(
+                torch.cuda.get_device_properties(device_index), "pci_bus_id") else None
+            if bus:
+                self._h = N.nvmlDeviceGetHandleByPciBusId(bus.encode() if isinstance(bus, str) else bus)
+            else:
+                self._h = N.nvmlDeviceGetHandleByIndex(int(os.environ.get("LOCAL_RANK", device_index)))
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self._h, N.NVML_CLOCK_SM)
+        except Exception as e:  # NVML unavailable: report what we could not sample
+            self.error = str(e)
+
+    def _run(self):
+        N = self.N
+        while not self._stop.is_set():
+            try:
+                self.samples.append(N.nvmlDeviceGetClockInfo(self._h, N.NVML_CLOCK_SM))
+                mask = N.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if mask & bit and bit != 0x1:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.05)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+
+    def summary(self):
+        if self._h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        s = sorted(self.samples)
+        return {"sm_mhz": s[len(s) // 2] if s else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(s)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(cfg, stage):
+    """Per-launch algorithmic bytes of a stage (the per-unit byte model times the units)."""
+    n = int(np.prod(cfg.volumeSize))
+    bv = 8 if cfg.storage == 0 else 4          # bytes per voxel (value + weight)
+    p0 = 512 * 424
+    if stage == "integrate":                   # read + write every voxel, depth in
+        return 2 * bv * n + 4 * p0
+    if stage == "raycast":                     # value plane read once, vertex + normal out
+        return (bv // 2) * n + 32 * p0
+    raise ValueError(stage)
+
+
+def cpu_baseline(args, w, frames_by_idx):
+    """Time the FP64 oracle (CPU port of the reference algorithm) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import kf_oracle as O
+    O.Oracle.set_threads(0)
+    o = O.Oracle(w.config, w.intrinsics)
+    o.Reset(w.poses[0])
+    warm = 2
+    n = max(1, args.cpu_frames)
+    for i in range(warm):
+        o.frameStep(frames_by_idx[i])
+    t0 = time.perf_counter()
+    for i in range(warm, warm + n):
+        o.frameStep(frames_by_idx[i])
+    dt = time.perf_counter() - t0
+    cores = O.Oracle.threads()
+    o.close()
+    return {"value": n / dt, "unit": "frames/s", "cores": cores, "kind": "port",
+            "sample": f"frames {warm}-{warm + n - 1} of the same {w.config.volumeSize[0]}^3 sequence "
+                      f"after {warm} untimed frames (FP64 oracle, OpenMP, {cores} threads)"}
+
+
+def run_reference(args):
+    """--impl reference: the reference algorithm's CPU port on this host, same workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, 12))   # a bounded sample of the workload
+    warm = max(1, min(args.warmup, 3))
+    w = workload(args, warm + steps)
+    frames = {i: w.frame(i) for i in range(warm + steps)}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import kf_oracle as O
+    O.Oracle.set_threads(0)
+    o = O.Oracle(w.config, w.intrinsics)
+    o.Reset(w.poses[0])
+    for i in range(warm):
+        o.frameStep(frames[i])
+    t0 = time.perf_counter()
+    for i in range(warm, warm + steps):
+        o.frameStep(frames[i])
+    dt = time.perf_counter() - t0
+    v = steps / dt
+    cores = O.Oracle.threads()
+    line = {"impl": "reference", "metric": "frames/s at 512^3 TSDF (single session)", "value": v,
+            "unit": "frames/s", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": 1000 * dt / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "volume": list(w.config.volumeSize), "dim_m": 3.0,
+                       "depth": "512x424 uint16", "icp_iterations": [10, 5, 4]},
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": cores, "kind": "port",
+                             "sample": f"{steps} frames after {warm} untimed (requested {args.steps})"},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    K, W = args.steps, max(3, args.warmup)
+    n_e2e = 0 if args.no_e2e else K
+    n_frames = W + K + n_e2e + 1
+    w = workload(args, n_frames)
+    ncpu = os.cpu_count() or 1
+    frames = gen_frames(w, range(n_frames), max(1, min(16, ncpu // max(1, world))))
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    from oglfusionkinectv2_b200 import GFusion, MCubes, _lib as L
+
+    g = GFusion(w.config, w.intrinsics)
+    g.Reset(w.poses[0])
+    mc = MCubes(g)
+    stream = torch.cuda.ExternalStream(g.stream())
+    stack = np.stack([frames[i] for i in range(n_frames)]).view(np.int16)
+    dframes = torch.from_numpy(stack).cuda()
+    fbytes = 512 * 424 * 2
+    base = dframes.data_ptr()
+    mc_calls = 0
+    mc_ms = []
+
+    def maybe_mc(i):
+        nonlocal mc_calls
+        if w.mc_every and (i + 1) % w.mc_every == 0:
+            t = time.perf_counter()
+            mc.generateMarchingCubes(L.KF_MC_HISTOPYRAMID)
+            mc_ms.append(1000 * (time.perf_counter() - t))
+            mc_calls += 1
+
+    for i in range(W):
+        g.frameStepDevice(base + i * fbytes, sync=False)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    g.resetStageStats()
+    launches0 = g.launchCount()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(W, W + K):
+            g.frameStepDevice(base + i * fbytes, sync=False)
+            maybe_mc(i - W)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    dev_ms = ev0.elapsed_time(ev1)
+    launches = g.launchCount() - launches0
+    stage_mean, stage_frames = g.stageStats()
+    tracked_ok = g.frameStepDevice(base + (W + K) * fbytes)  # a synchronised step: state readable
+
+    # end to end: pinned host frames through kf_frame_step_u16 (H2D frame + D2H pose/flags)
+    e2e = None
+    if n_e2e:
+        pinned = torch.empty((n_e2e, 424, 512), dtype=torch.int16).pin_memory()
+        pinned.copy_(torch.from_numpy(stack[W + K + 1:W + K + 1 + n_e2e]))
+        hp = pinned.data_ptr()
+        lib = L.load()
+        import ctypes as C
+        t = C.c_int()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t0 = time.perf_counter()
+        for i in range(n_e2e):
+            st = lib.kf_frame_step_u16(g.handle, C.c_void_p(hp + i * fbytes), C.byref(t))
+            if st:
+                raise L.KfError(st, "kf_frame_step_u16")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e2e_ms = e0.elapsed_time(e1)
+        e2e = {"ms": e2e_ms, "wall_s": wall}
+
+    # max over ranks of the timed durations
+    times = torch.tensor([dev_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    dev_ms_max, e2e_ms_max = float(times[0]), float(times[1])
+
+    out = None
+    if rank == 0:
+        value = world * K / (dev_ms_max / 1000.0)
+        stages = ["pyramid", "track", "integrate", "recover", "raycast"]
+        per = {s: float(stage_mean[i]) for i, s in enumerate(stages)}
+        dom = "integrate" if per["integrate"] >= per["raycast"] else "raycast"
+        peak, peak_kind = measured_peak_hbm()
+        algo = algorithmic_bytes(w.config, dom)
+        achieved = algo / (per[dom] / 1000.0) / 1e9 if per[dom] > 0 else None
+        out = {
+            "metric": "frames/s at 512^3 TSDF (single session, plain frame step)",
+            "value": value, "unit": "frames/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "volume": list(w.config.volumeSize), "dim_m": 3.0,
+                       "storage": args.storage, "jtj": args.jtj, "solve": "f64 cholesky",
+                       "depth": "512x424 uint16", "icp_iterations": [10, 5, 4],
+                       "quirks": hex(w.config.quirks), "parallelism": f"replicas x{world}",
+                       "l2": "volume > L2 (126 MB); inputs resident",
+                       "mc_every": w.mc_every, "mc_calls": mc_calls,
+                       "mc_ms_mean": (float(np.mean(mc_ms)) if mc_ms else None)},
+            "stage_ms": per, "stage_frames": stage_frames,
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak if achieved else None),
+                         "peak_source": peak_kind, "algorithmic_bytes": algo, "traffic": None},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "tracked_last": bool(tracked_ok),
+        }
+        if e2e:
+            out["e2e"] = {"value": world * n_e2e / (e2e_ms_max / 1000.0), "unit": "frames/s",
+                          "h2d_bytes_per_step": fbytes, "d2h_bytes_per_step": 144,
+                          "wall_frames_per_s": n_e2e / e2e["wall_s"]}
+    g.close()
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        out["cpu_baseline"] = cpu_baseline(args, w, frames)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,245 @@
+/*
+ * kf.h — C ABI of the B200 KinectFusion core.
+ *
+ * This is the drop-in boundary for the compute path of philipNoonan/oglFusionKinectV2:
+ * the `gFusion` class (include/gFusion.h:124-624, src/gFusion.cpp) and the `MCubes`
+ * class (include/mcubes.h:48-168, src/mcubes.cpp).  Every entry point below names the
+ * reference member it replaces.  The reference has no FFI of its own (it is one
+ * in-process C++ class used by src/kinect.cpp), so these are the calls such a binding
+ * would make: plain pointers and sizes, POD structs, int status codes, no exceptions and
+ * no process exit across the boundary (the reference calls exit() on shader errors,
+ * src/gFusion.cpp:69-72, src/mcubes.cpp:32-35; here that is KF_ERR_*).
+ *
+ * Conventions
+ *   - Poses are camera-to-world 4x4 matrices, column-major (glm layout, the reference's
+ *     m_pose), passed as double[16].  The device keeps the pose in FP64.
+ *   - The volume covers world [0, dim]^3 (raycast.cs:141-143); voxel (x,y,z) has its
+ *     centre at ((x+0.5)*dim_x/nx, ...) (integrate.cs:16-19) and linear index
+ *     x + nx*(y + ny*z) in each of its two planes (values, then weights).
+ *   - Maps are row-major W x H (level l: (W>>l) x (H>>l)) of float4 (RGBA32F textures).
+ *   - Every call is enqueued on the session's own CUDA stream; calls that return data to
+ *     the host synchronise that stream first.  One session is used by one host thread.
+ */
+#ifndef KF_H
+#define KF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KF_ABI_VERSION 1
+
+#if defined(KF_BUILDING_LIBRARY) && defined(__GNUC__)
+#define KF_API __attribute__((visibility("default")))
+#else
+#define KF_API
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define KF_OK 0
+#define KF_ERR_INVALID_ARGUMENT (-1)
+#define KF_ERR_OUT_OF_MEMORY (-2)
+#define KF_ERR_CUDA (-3)
+#define KF_ERR_NO_DEVICE (-4)
+#define KF_ERR_TIMEOUT (-5)       /* a bounded device-side wait gave up */
+#define KF_ERR_STATE (-6)         /* call out of order (e.g. export before extract) */
+#define KF_ERR_IO (-7)            /* file could not be written */
+#define KF_ERR_CAPACITY (-8)      /* output larger than the caller's buffer / static limit */
+#define KF_ERR_ADMISSION (-9)     /* not enough free device memory for a new session */
+
+/* ---- volume storage (gFusion.cpp:223 uses GL_RG16I) --------------------------------- */
+#define KF_STORAGE_F32F32 0 /* float TSDF + float weight, 8 B/voxel                     */
+#define KF_STORAGE_F16U16 1 /* half TSDF + uint16 weight, 4 B/voxel (FP32 update math)  */
+#define KF_STORAGE_RG16I 2  /* int16 TSDF*32766 + int16 weight, 4 B/voxel (reference)   */
+
+/* ---- J^T J contraction ----------------------------------------------------------- */
+#define KF_JTJ_FP32 0       /* FP32 FMAs on the CUDA cores                                */
+#define KF_JTJ_SPLIT_BF16 1 /* split-BF16 (hi+lo) tensor-core mma, FP32 accumulation      */
+
+/* ---- tracking mode (kinect.h:143-144 trackDepthToPoint / trackDepthToVolume) ------- */
+#define KF_TRACK_ICP 0
+#define KF_TRACK_SDF 1
+
+/* ---- reference behaviours that can be reproduced ("faithful") or fixed ("clean") -----
+ * Each bit, when set, reproduces the reference behaviour named beside it.            */
+#define KF_Q1_LAST_GROUP_ONLY (1u << 0)  /* getReduction keeps only rows y%8==7,        \
+                                            gFusion.cpp:1143-1149, 1206-1212             */
+#define KF_Q3_DOWN_FROM_LEFT (1u << 1)   /* vertToNorm "down" reads column x-1,          \
+                                            vertToNorm.cs:26                             */
+#define KF_Q6_SDF_D2_TWICE (1u << 2)     /* reduceSDF adds D^2 twice, reduceSDF.cs:52,60 */
+#define KF_Q7_SDF_LAST_COLUMN (1u << 3)  /* trackSDF skips x=W-1, the reduction reads   \
+                                            the stale row, trackSDF.cs:413               */
+#define KF_Q13_MC_FIRST_SEVEN (1u << 4)  /* MC "positive found" ignores corner 7,        \
+                                            histoPyramids.cs:140                          */
+#define KF_Q15_MC_BORDER_SKIP (1u << 5)  /* MC classify skips cubes within 10 of the     \
+                                            border, histoPyramids.cs:117-120              */
+#define KF_Q18_STL_COUNT_X4 (1u << 6)    /* STL header count = 4x triangles,             \
+                                            mcubes.cpp:451-457                            */
+#define KF_Q23_SDF_XY_OFFSET (1u << 7)   /* trackSDF subtracts 0.5 twice from x and y of \
+                                            the voxel coordinate, trackSDF.cs:429         */
+#define KF_Q8_NARROW_BAND (1u << 9)     /* integrate keeps a value only while the running \
+                                            average is below 0.2, clamped to [-0.1, 0.2]; \
+                                            clear: the reference's earlier update, clamp  \
+                                            to [-1, 1] (integrate.cs:80-113 vs 115-150)   */
+#define KF_Q4_SAME_PIXEL (1u << 10)      /* ICP projects with the current estimate, so   \
+                                            the association is the same pixel; clear:    \
+                                            project with the raycast (previous) pose,    \
+                                            gFusion.cpp:747-755                          */
+#define KF_Q19_EIG_TRANSLATION (1u << 8) /* resetPose seeds the SDF pose chain with the     \
+                                            translation only, gFusion.cpp:275-287         */
+/* Exactly the reference's behaviour. */
+#define KF_QUIRKS_REFERENCE                                                                  \
+  (KF_Q1_LAST_GROUP_ONLY | KF_Q3_DOWN_FROM_LEFT | KF_Q4_SAME_PIXEL | KF_Q6_SDF_D2_TWICE |      \
+   KF_Q7_SDF_LAST_COLUMN | KF_Q8_NARROW_BAND | KF_Q13_MC_FIRST_SEVEN | KF_Q15_MC_BORDER_SKIP |  \
+   KF_Q19_EIG_TRANSLATION | KF_Q23_SDF_XY_OFFSET)
+/* Default: the reference, with the J^T J reduction over the whole image (Q1 cleared). */
+#define KF_QUIRKS_DEFAULT (KF_QUIRKS_REFERENCE & ~KF_Q1_LAST_GROUP_ONLY)
+/* Default with projective association from the raycast pose and the reference's earlier
+ * [-1, 1] TSDF update (Q4, Q8 cleared): with a truncation of a few voxels the reference's
+ * 0.2*mu band is thinner than a voxel and same-pixel association biases every step. */
+#define KF_QUIRKS_TRACKING (KF_QUIRKS_DEFAULT & ~(KF_Q4_SAME_PIXEL | KF_Q8_NARROW_BAND))
+
+/* ---- marching-cubes method ---------------------------------------------------------- */
+#define KF_MC_HISTOPYRAMID 0 /* histoPyramids.cs + traverseHistoPyramids.cs (live path)   */
+#define KF_MC_SCAN 1         /* marchingCubes.cs classify/compact/generate + prefix sum   */
+
+/* gFusionConfig (include/gFusion.h:42-82) plus the storage/precision/quirk policy. */
+typedef struct kf_config {
+  int32_t nx, ny, nz;         /* volumeSize, voxels                                        */
+  float dim_x, dim_y, dim_z;  /* volumeDimensions, metres                                  */
+  float mu;                   /* truncation, metres                                        */
+  float max_weight;           /* maxWeight                                                 */
+  float near_plane, far_plane;/* raycast clip, metres                                      */
+  float dist_threshold;       /* ICP gating distance, metres                               */
+  float normal_threshold;     /* ICP gating normal dot                                     */
+  int32_t iterations[3];      /* per pyramid level, index 0 = finest (gFusion.cpp:661-666) */
+  int32_t storage;            /* KF_STORAGE_*                                              */
+  int32_t jtj;                /* KF_JTJ_*                                                  */
+  int32_t tracking;           /* KF_TRACK_*                                                */
+  uint32_t quirks;            /* KF_Q*                                                     */
+  int32_t integrate_every;    /* counter % integrate_every == 0 (kinect.cpp:677, 1)        */
+  int32_t reserved[7];
+} kf_config;
+
+/* Depth camera intrinsics; setCameraParams(vec4(fx, fy, cx, cy)) (gFusion.h:184-188). */
+typedef struct kf_intrinsics {
+  float fx, fy, cx, cy;
+  int32_t width, height; /* 512 x 424 for the Kinect v2 (gFusion.h:555-556) */
+} kf_intrinsics;
+
+/* Non-owning view of the TSDF volume (replaces getVolume() -> GL texture name).
+ * The volume is two planes: nx*ny*nz TSDF values (x fastest), then as many weights.
+ * F32F32: float + float; F16U16: IEEE half + uint16; RG16I: int16 (TSDF*32766) + int16. */
+typedef struct kf_volume_view {
+  void* device_ptr;            /* value plane; valid until kf_reset(.., 1) or kf_destroy */
+  int32_t nx, ny, nz;
+  int32_t storage;             /* KF_STORAGE_*                                           */
+  int64_t value_bytes;         /* bytes per value (and per weight): 4 or 2              */
+  int64_t weight_offset_bytes; /* weight plane = device_ptr + weight_offset_bytes       */
+  int64_t row_pitch_bytes;     /* nx * value_bytes                                      */
+  int64_t slice_pitch_bytes;   /* nx * ny * value_bytes                                 */
+} kf_volume_view;
+
+typedef struct kf_session kf_session;
+
+/* ---- library --------------------------------------------------------------------- */
+KF_API int kf_abi_version(void);
+KF_API const char* kf_status_string(int status);
+/* gFusionConfig() defaults (gFusion.h:56-69) with storage F32F32, FP32 J^T J, ICP. */
+KF_API int kf_config_default(kf_config* cfg);
+
+/* ---- lifecycle: initTextures/initVolume/allocateBuffers (gFusion.cpp:200-383) ------ */
+KF_API int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out);
+KF_API int kf_destroy(kf_session* s);
+KF_API const char* kf_last_error(const kf_session* s);
+/* Bytes a session with this config holds on the device (admission control). */
+KF_API int kf_session_device_bytes(const kf_config* cfg, const kf_intrinsics* intr, uint64_t* bytes);
+
+/* Reset(pose, deleteFlag) (gFusion.cpp:226-240): zero or reallocate the volume, clear
+ * the pose library, resetPose(pose). */
+KF_API int kf_reset(kf_session* s, const double pose[16], int delete_flag);
+KF_API int kf_reset_volume(kf_session* s);                 /* resetVolume, gFusion.cpp:242-273 */
+KF_API int kf_reset_pose(kf_session* s, const double pose[16]); /* resetPose, :275-287 */
+KF_API int kf_set_pose(kf_session* s, const double pose[16]);   /* setPose, gFusion.h:177-180 */
+KF_API int kf_get_pose(kf_session* s, double pose[16]);         /* getPose, gFusion.h:173-176 */
+KF_API int kf_set_config(kf_session* s, const kf_config* cfg);  /* setConfig (same volume size) */
+
+/* ---- depth ingest: depthToVertex (gFusion.cpp:496-526) ------------------------------
+ * Uploads one depth frame, builds the 3-level mip pyramid (2x2 box mean including zeros,
+ * glGenerateMipmap at :508) and the vertex maps.  _f32 takes millimetres as float (the
+ * reference's input); _u16 takes uint16 millimetres; _device reads a device pointer. */
+KF_API int kf_depth_to_vertex_f32(kf_session* s, const float* host_depth_mm);
+KF_API int kf_depth_to_vertex_u16(kf_session* s, const uint16_t* host_depth_mm);
+KF_API int kf_depth_to_vertex_u16_device(kf_session* s, const uint16_t* device_depth_mm);
+KF_API int kf_vertex_to_normal(kf_session* s); /* vertexToNormal, gFusion.cpp:528-547 */
+
+/* ---- tracking ------------------------------------------------------------------------ */
+/* Track() (gFusion.cpp:648-740): coarse-to-fine projective point-to-plane ICP with the
+ * 27-term reduction, an on-device FP64 solve and pose update.  *tracked may be NULL (then
+ * the call does not synchronise). */
+KF_API int kf_track_icp(kf_session* s, int* tracked);
+/* TrackSDF() (gFusion.cpp:835-1038): direct SDF tracking, LM-damped, SE(3) exponential. */
+KF_API int kf_track_sdf(kf_session* s, int* tracked);
+/* recoverPose() (gFusion.cpp:1616-1653): TrackSDF from each pose of the pose library. */
+KF_API int kf_recover_pose(kf_session* s, int* found);
+/* Alignment energy and the 32-float reduction row of the last ICP / SDF iteration
+ * (getReduction / getSDFReduction, gFusion.cpp:1127-1168, 1195-1232). */
+KF_API int kf_get_alignment_energy(kf_session* s, float* ae);
+KF_API int kf_get_reduction(kf_session* s, float sums[32]);
+
+/* ---- volume ------------------------------------------------------------------------- */
+KF_API int kf_integrate(kf_session* s); /* integrate(), gFusion.cpp:1234-1287 */
+KF_API int kf_raycast(kf_session* s);   /* raycast(),   gFusion.cpp:1289-1366 */
+
+/* One frame of src/kinect.cpp:654-695: depthToVertex, vertexToNormal, Track (or
+ * TrackSDF), integrate when tracked (or inside the reset window), recoverPose when not
+ * tracked, raycast.  Replayed from a CUDA graph after the first call. */
+KF_API int kf_frame_step_u16(kf_session* s, const uint16_t* host_depth_mm, int* tracked);
+KF_API int kf_frame_step_u16_device(kf_session* s, const uint16_t* device_depth_mm, int* tracked);
+
+/* ---- accessors (getVerts/getNorms/getDepthImage/getVolume/getTrackImage) ------------- */
+KF_API int kf_get_raycast(kf_session* s, float* vertex4, float* normal4);            /* W*H*4 each */
+KF_API int kf_get_vertex_map(kf_session* s, int level, float* vertex4);
+KF_API int kf_get_normal_map(kf_session* s, int level, float* normal4);
+KF_API int kf_get_depth_map(kf_session* s, int level, float* depth_mm);
+KF_API int kf_get_track_status(kf_session* s, int level, int32_t* status); /* trackOutput.result */
+KF_API int kf_get_volume(kf_session* s, kf_volume_view* view);
+KF_API int kf_copy_volume_to_host(kf_session* s, void* dst, uint64_t bytes);
+KF_API int kf_copy_volume_from_host(kf_session* s, const void* src, uint64_t bytes);
+KF_API int kf_get_cum_twist(kf_session* s, double twist[6]); /* getCumTwist, gFusion.h:260-265 */
+KF_API int kf_get_pose_library_size(kf_session* s, int* n);
+/* Device times in milliseconds of the last call of each stage, in the order
+ * pyramid, track, integrate, raycast, recover, mc. */
+KF_API int kf_get_stage_times(kf_session* s, float ms[6]);
+/* Mean device milliseconds per stage (same order) over every kf_frame_step_* call since
+ * the last kf_reset_stage_stats; read from per-frame events without stalling the stream. */
+KF_API int kf_get_stage_stats(kf_session* s, double mean_ms[6], uint64_t* frames);
+KF_API int kf_reset_stage_stats(kf_session* s);
+/* Kernels this session has launched (a frame step counts every kernel of its graph). */
+KF_API int kf_get_launch_count(kf_session* s, uint64_t* launches);
+KF_API int kf_get_stream(kf_session* s, void** cuda_stream);
+
+/* ---- marching cubes (MCubes, mcubes.cpp:206-509) ---------------------------------------
+ * kf_mc_extract = setIsolevel + generateMarchingCubes; *n_triangles is the triangle count
+ * (getNumberTriangles() returns 3x that).  Vertices are float4 in voxel-index units,
+ * w = 0 (traverseHistoPyramids.cs:218-241). */
+KF_API int kf_mc_extract(kf_session* s, float iso, int method, uint32_t* n_triangles);
+KF_API int kf_mc_copy_vertices(kf_session* s, float* vertex4, uint64_t max_vertices);
+/* Base level: numTri | cubeIndex << 16 per cube (RG16UI, histoPyramids.cs:170). */
+KF_API int kf_mc_copy_base_level(kf_session* s, uint32_t* base, uint64_t count);
+KF_API int kf_mc_export_stl(kf_session* s, const char* path);  /* exportMesh, :429-509 */
+KF_API int kf_mc_export_ply(kf_session* s, const char* path);  /* exportPointCloud, :391-427 */
+
+/* ---- prefix sum (prefixSum.cs, MCubes::prefixSum mcubes.cpp:136-204) --------------------
+ * Exclusive scan of n uint32 device values on `stream` (0 = legacy default); *total, if
+ * not NULL, receives sum(in) (lastElement + lastScanElement).  Any n up to 2^32-1. */
+KF_API int kf_prefix_sum_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* total,
+                      void* cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KF_H */

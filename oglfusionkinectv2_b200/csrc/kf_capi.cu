@@ -1,0 +1,763 @@
+// kf_capi.cu — the C ABI (include/kf.h): sessions, state hand-off, frame step, accessors.
+//
+// Reference: the public members of class gFusion (include/gFusion.h:134-274) and the
+// per-frame loop of src/kinect.cpp:654-695.  A session owns its CUDA stream, its device
+// buffers and a device control block (KfDevState) that holds the FP64 pose, the pose
+// library and the frame-policy flags, so a whole frame runs without a host round trip.
+// The first kf_frame_step_* call captures the device part of a frame into a CUDA graph;
+// later calls replay it.
+#include <algorithm>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <new>
+
+#include "kf_internal.cuh"
+
+namespace {
+
+const double kIdentity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+
+int fail(kf_session* s, int code, const std::string& msg) {
+  if (s) s->last_error = msg;
+  return code;
+}
+
+template <class T>
+int dalloc(kf_session* s, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return KF_OK;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(s, e == cudaErrorMemoryAllocation ? KF_ERR_OUT_OF_MEMORY : KF_ERR_CUDA,
+                std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  return KF_OK;
+}
+
+int validate(const kf_config* c, const kf_intrinsics* in) {
+  if (!c || !in) return KF_ERR_INVALID_ARGUMENT;
+  if (c->nx < 4 || c->ny < 4 || c->nz < 4 || c->nx > 4096 || c->ny > 4096 || c->nz > 4096)
+    return KF_ERR_INVALID_ARGUMENT;
+  if (!(c->dim_x > 0) || !(c->dim_y > 0) || !(c->dim_z > 0) || !(c->mu > 0)) return KF_ERR_INVALID_ARGUMENT;
+  if (!(c->max_weight > 0) || !(c->far_plane > c->near_plane)) return KF_ERR_INVALID_ARGUMENT;
+  if (c->storage < KF_STORAGE_F32F32 || c->storage > KF_STORAGE_RG16I) return KF_ERR_INVALID_ARGUMENT;
+  if (c->jtj != KF_JTJ_FP32 && c->jtj != KF_JTJ_SPLIT_BF16) return KF_ERR_INVALID_ARGUMENT;
+  if (c->tracking != KF_TRACK_ICP && c->tracking != KF_TRACK_SDF) return KF_ERR_INVALID_ARGUMENT;
+  for (int l = 0; l < 3; ++l)
+    if (c->iterations[l] < 0 || c->iterations[l] > 1000) return KF_ERR_INVALID_ARGUMENT;
+  if (c->storage == KF_STORAGE_F16U16 && c->max_weight > 65535.0f) return KF_ERR_INVALID_ARGUMENT;
+  if (c->storage == KF_STORAGE_RG16I && c->max_weight > 32767.0f) return KF_ERR_INVALID_ARGUMENT;
+  // three mip levels of exact halves
+  if (in->width < 16 || in->height < 16 || (in->width % 4) || (in->height % 4)) return KF_ERR_INVALID_ARGUMENT;
+  if (in->width > 8192 || in->height > 8192) return KF_ERR_INVALID_ARGUMENT;
+  if (!(in->fx > 0) || !(in->fy > 0)) return KF_ERR_INVALID_ARGUMENT;
+  return KF_OK;
+}
+
+size_t value_bytes(int storage) { return storage == KF_STORAGE_F32F32 ? 4 : 2; }
+
+void free_mc(kf_session* s) {
+  cudaFree(s->d_mc_base);
+  s->d_mc_base = nullptr;
+  for (uint32_t* p : s->d_mc_levels) cudaFree(p);
+  s->d_mc_levels.clear();
+  cudaFree(s->d_mc_vertices);
+  s->d_mc_vertices = nullptr;
+  s->mc_vertex_cap = 0;
+  cudaFree(s->d_mc_scratch);
+  s->d_mc_scratch = nullptr;
+  s->mc_scratch_words = 0;
+  s->mc_valid = 0;
+  s->mc_triangles = 0;
+}
+
+void drop_graph(kf_session* s) {
+  for (int r = 0; r < kf_session::kRing; ++r) {
+    if (s->frame_exec[r]) cudaGraphExecDestroy(s->frame_exec[r]);
+    s->frame_exec[r] = nullptr;
+    s->ring_pending[r] = 0;
+  }
+}
+
+void free_all(kf_session* s) {
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graph(s);
+  free_mc(s);
+  cudaFree(s->d_vol);
+  cudaFree(s->d_depth_u16);
+  cudaFree(s->d_depth_f32_in);
+  for (int l = 0; l < 3; ++l) {
+    cudaFree(s->d_depth[l]);
+    cudaFree(s->d_vertex[l]);
+    cudaFree(s->d_normal[l]);
+    cudaFree(s->d_status[l]);
+  }
+  cudaFree(s->d_ref_vertex);
+  cudaFree(s->d_ref_normal);
+  cudaFree(s->d_sdf_rows);
+  cudaFree(s->d_partials);
+  cudaFree(s->d_state);
+  cudaFree(s->d_u32_scalar);
+  if (s->h_state) cudaFreeHost(s->h_state);
+  if (s->h_depth_pinned) cudaFreeHost(s->h_depth_pinned);
+  if (s->h_u32_scalar) cudaFreeHost(s->h_u32_scalar);
+  for (auto& e : s->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& row : s->ring_ev)
+    for (auto& e : row)
+      if (e) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// ---- host <-> device control block ------------------------------------------------------
+int check_device_error(kf_session* s) {
+  if (s->h_state->error) {
+    const int err = s->h_state->error;
+    s->h_state->error = 0;
+    cudaMemsetAsync(&s->d_state->error, 0, sizeof(int), s->stream);
+    cudaStreamSynchronize(s->stream);
+    return fail(s, KF_ERR_TIMEOUT, "device wait timed out (error " + std::to_string(err) + ")");
+  }
+  return KF_OK;
+}
+
+int pull_state(kf_session* s) {
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_state, s->d_state, sizeof(KfDevState), cudaMemcpyDeviceToHost, s->stream));
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return check_device_error(s);
+}
+
+// pose and result flags only (the per-frame result)
+int pull_state_head(kf_session* s) {
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_state, s->d_state, KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream));
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return check_device_error(s);
+}
+
+int push_state(kf_session* s) {
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_state, s->h_state, sizeof(KfDevState), cudaMemcpyHostToDevice, s->stream));
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return KF_OK;
+}
+
+void set_pose_fields(kf_session* s, const double* pose, bool reset_eig) {
+  std::memcpy(s->h_state->pose, pose, 16 * sizeof(double));
+  if (reset_eig) {
+    // resetPose (gFusion.cpp:275-287)
+    if (s->cfg.quirks & KF_Q19_EIG_TRANSLATION) {
+      std::memcpy(s->h_state->pose_eig, kIdentity, sizeof(kIdentity));
+      s->h_state->pose_eig[12] = pose[12];
+      s->h_state->pose_eig[13] = pose[13];
+      s->h_state->pose_eig[14] = pose[14];
+    } else {
+      std::memcpy(s->h_state->pose_eig, pose, 16 * sizeof(double));
+    }
+    for (int k = 0; k < 6; ++k) s->h_state->cum_twist[k] = 0;
+  }
+}
+
+int alloc_volume(kf_session* s) {
+  cudaFree(s->d_vol);
+  s->d_vol = nullptr;
+  s->vol_count = (size_t)s->cfg.nx * s->cfg.ny * s->cfg.nz;
+  s->vol_value_bytes = value_bytes(s->cfg.storage);
+  s->vol_bytes = s->vol_count * s->vol_value_bytes * 2;
+  char* p = nullptr;
+  int rc = dalloc(s, &p, s->vol_bytes);
+  if (rc) return rc;
+  s->d_vol = p;
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_vol, 0, s->vol_bytes, s->stream));
+  return KF_OK;
+}
+
+int record(kf_session* s, int i) {
+  if (!s->timing || s->capturing) return KF_OK;
+  KF_CUDA_TRY(s, cudaEventRecord(s->ev[i], s->stream));
+  return KF_OK;
+}
+
+// The device part of one frame of kinect.cpp:654-695 (input already in d_depth_u16),
+// with stage events ev[0..5]: start, pyramid, track, integrate, recover, raycast.
+int enqueue_frame(kf_session* s, cudaEvent_t* ev) {
+  int rc;
+  KF_CUDA_TRY(s, cudaEventRecord(ev[0], s->stream));
+  if ((rc = kf_launch_pyramid(s, s->d_depth_u16, nullptr))) return rc;
+  if ((rc = kf_launch_vertex_normal(s))) return rc;
+  KF_CUDA_TRY(s, cudaEventRecord(ev[1], s->stream));
+  if (s->cfg.tracking == KF_TRACK_SDF) {
+    if ((rc = kf_launch_sdf(s, 0, 0, 1))) return rc;
+    if ((rc = kf_launch_sdf_policy(s))) return rc;
+  } else {
+    if ((rc = kf_launch_icp(s, 1))) return rc;
+  }
+  KF_CUDA_TRY(s, cudaEventRecord(ev[2], s->stream));
+  if ((rc = kf_launch_integrate(s, 1))) return rc;
+  KF_CUDA_TRY(s, cudaEventRecord(ev[3], s->stream));
+  if ((rc = kf_launch_sdf(s, 1, 1, 0))) return rc;
+  KF_CUDA_TRY(s, cudaEventRecord(ev[4], s->stream));
+  if ((rc = kf_launch_raycast(s))) return rc;
+  KF_CUDA_TRY(s, cudaEventRecord(ev[5], s->stream));
+  return KF_OK;
+}
+
+int count_kernels(cudaGraph_t g) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return 0;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+  int k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
+// Read back the stage times of the frame held by a ring slot (waits for that frame only).
+int harvest(kf_session* s, int slot) {
+  if (!s->ring_pending[slot]) return KF_OK;
+  KF_CUDA_TRY(s, cudaEventSynchronize(s->ring_ev[slot][5]));
+  for (int i = 0; i < 5; ++i) {
+    float ms = 0.0f;
+    KF_CUDA_TRY(s, cudaEventElapsedTime(&ms, s->ring_ev[slot][i], s->ring_ev[slot][i + 1]));
+    s->stage_ms[i] = ms;
+    s->stage_acc[i] += ms;
+  }
+  s->stage_frames += 1;
+  s->ring_pending[slot] = 0;
+  return KF_OK;
+}
+
+int harvest_all(kf_session* s) {
+  // oldest first, so stage_ms ends as the newest frame
+  for (int k = 0; k < kf_session::kRing; ++k) {
+    const int slot = (int)((s->frames_run + k) % kf_session::kRing);
+    int rc = harvest(s, slot);
+    if (rc) return rc;
+  }
+  return KF_OK;
+}
+
+int run_frame(kf_session* s) {
+  const int slot = (int)(s->frames_run % kf_session::kRing);
+  if (!s->frame_exec[slot]) {
+    for (int i = 0; i < 6; ++i)
+      if (!s->ring_ev[slot][i]) KF_CUDA_TRY(s, cudaEventCreate(&s->ring_ev[slot][i]));
+    cudaGraph_t g = nullptr;
+    KF_CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    s->capturing = true;
+    int rc = enqueue_frame(s, s->ring_ev[slot]);
+    s->capturing = false;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(s, KF_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    s->frame_kernels = count_kernels(g);
+    e = cudaGraphInstantiate(&s->frame_exec[slot], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      s->frame_exec[slot] = nullptr;
+      return fail(s, KF_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    }
+  }
+  int rc = harvest(s, slot);  // the frame that used this slot kRing frames ago
+  if (rc) return rc;
+  KF_CUDA_TRY(s, cudaGraphLaunch(s->frame_exec[slot], s->stream));
+  s->ring_pending[slot] = 1;
+  s->frames_run += 1;
+  s->launches += (uint64_t)s->frame_kernels;
+  return KF_OK;
+}
+
+int finish_step(kf_session* s, int* tracked) {
+  if (!tracked) return KF_OK;
+  int rc = pull_state_head(s);
+  if (rc) return rc;
+  *tracked = s->h_state->tracked;
+  return KF_OK;
+}
+
+std::mutex g_occ_mu;
+std::map<std::pair<const void*, int>, int> g_occ;
+
+}  // namespace
+
+// SDF tracking in the frame step: TrackSDF's result drives the same policy flags as ICP.
+__global__ void kf_sdf_policy_kernel(KfDevState* st, int every) {
+  const int tracked = st->tracked;
+  every = every > 0 ? every : 1;
+  const int integ = (tracked && (st->counter % every) == 0) || st->reset_window;
+  st->do_integrate = integ;
+  if (integ && st->counter > 2) st->reset_window = 0;
+  st->need_recover = !tracked;
+  st->counter += 1;
+}
+
+int kf_launch_sdf_policy(kf_session* s) {
+  kf_sdf_policy_kernel<<<1, 1, 0, s->stream>>>(s->d_state, s->cfg.integrate_every);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  kf_note_launch(s);
+  return KF_OK;
+}
+
+int kf_occupancy_blocks(kf_session* s, const void* kernel, int threads, size_t smem) {
+  std::lock_guard<std::mutex> lk(g_occ_mu);
+  auto key = std::make_pair(kernel, s->device);
+  auto it = g_occ.find(key);
+  int per_sm;
+  if (it != g_occ.end()) {
+    per_sm = it->second;
+  } else {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (e != cudaSuccess || per_sm <= 0) {
+      s->last_error = std::string("occupancy: ") + cudaGetErrorString(e);
+      return 0;
+    }
+    g_occ[key] = per_sm;
+  }
+  // two co-resident blocks per SM: enough warps to hide the gather latency, few enough
+  // partial rows for the single-block FP64 reduction
+  const int blocks = std::min(per_sm, 2) * s->num_sms;
+  return std::min(blocks, KF_MAX_TRACK_BLOCKS);
+}
+
+// =========================================================================================
+extern "C" {
+
+int kf_abi_version(void) { return KF_ABI_VERSION; }
+
+const char* kf_status_string(int st) {
+  switch (st) {
+    case KF_OK: return "ok";
+    case KF_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case KF_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case KF_ERR_CUDA: return "CUDA error";
+    case KF_ERR_NO_DEVICE: return "no CUDA device";
+    case KF_ERR_TIMEOUT: return "device wait timed out";
+    case KF_ERR_STATE: return "call out of order";
+    case KF_ERR_IO: return "file error";
+    case KF_ERR_CAPACITY: return "capacity exceeded";
+    case KF_ERR_ADMISSION: return "admission refused";
+    default: return "unknown status";
+  }
+}
+
+int kf_config_default(kf_config* c) {
+  if (!c) return KF_ERR_INVALID_ARGUMENT;
+  std::memset(c, 0, sizeof(*c));
+  // gFusionConfig() (gFusion.h:56-69)
+  c->nx = c->ny = c->nz = 256;
+  c->dim_x = c->dim_y = c->dim_z = 1.0f;
+  c->mu = 0.05f;
+  c->max_weight = 100.0f;
+  c->near_plane = 0.1f;
+  c->far_plane = 3.0f;
+  c->dist_threshold = 0.05f;
+  c->normal_threshold = 0.8f;
+  c->iterations[0] = c->iterations[1] = c->iterations[2] = 5;
+  c->storage = KF_STORAGE_F32F32;
+  c->jtj = KF_JTJ_FP32;
+  c->tracking = KF_TRACK_ICP;
+  c->quirks = KF_QUIRKS_DEFAULT;
+  c->integrate_every = 1;
+  return KF_OK;
+}
+
+int kf_session_device_bytes(const kf_config* cfg, const kf_intrinsics* in, uint64_t* bytes) {
+  int rc = validate(cfg, in);
+  if (rc) return rc;
+  if (!bytes) return KF_ERR_INVALID_ARGUMENT;
+  const uint64_t vox = (uint64_t)cfg->nx * cfg->ny * cfg->nz;
+  const uint64_t px = (uint64_t)in->width * in->height;
+  uint64_t b = vox * value_bytes(cfg->storage) * 2;
+  b += px * (2 + 4);                       // staging
+  b += px * (4 + 16 + 16 + 4) * 2;         // three levels (sum < 4/3 of level 0)
+  b += px * 32;                            // raycast maps
+  b += px * 32;                            // sdf rows
+  b += (uint64_t)KF_MAX_TRACK_BLOCKS * 32 * 4 + sizeof(KfDevState);
+  *bytes = b;
+  return KF_OK;
+}
+
+int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out) {
+  if (!out) return KF_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int rc = validate(cfg, intr);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return KF_ERR_NO_DEVICE;
+  }
+  kf_session* s = new (std::nothrow) kf_session();
+  if (!s) return KF_ERR_OUT_OF_MEMORY;
+  s->cfg = *cfg;
+  if (s->cfg.integrate_every <= 0) s->cfg.integrate_every = 1;
+  s->intr = *intr;
+  cudaGetDevice(&s->device);
+  cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
+  auto bail = [&](int code) {
+    free_all(s);
+    delete s;
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(KF_ERR_CUDA);
+  for (auto& e : s->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bail(KF_ERR_CUDA);
+  s->timing = true;
+  for (int l = 0; l < 3; ++l) {
+    s->W[l] = intr->width >> l;
+    s->H[l] = intr->height >> l;
+  }
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  if ((rc = alloc_volume(s))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_depth_u16, px))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_depth_f32_in, px))) return bail(rc);
+  for (int l = 0; l < 3; ++l) {
+    const size_t n = (size_t)s->W[l] * s->H[l];
+    if ((rc = dalloc(s, &s->d_depth[l], n))) return bail(rc);
+    if ((rc = dalloc(s, &s->d_vertex[l], n))) return bail(rc);
+    if ((rc = dalloc(s, &s->d_normal[l], n))) return bail(rc);
+    if ((rc = dalloc(s, &s->d_status[l], n))) return bail(rc);
+    cudaMemsetAsync(s->d_depth[l], 0, n * 4, s->stream);
+    cudaMemsetAsync(s->d_vertex[l], 0, n * 16, s->stream);
+    cudaMemsetAsync(s->d_normal[l], 0, n * 16, s->stream);
+    cudaMemsetAsync(s->d_status[l], 0, n * 4, s->stream);
+  }
+  if ((rc = dalloc(s, &s->d_ref_vertex, px))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_ref_normal, px))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_sdf_rows, px * 8))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_partials, (size_t)KF_MAX_TRACK_BLOCKS * 32))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_state, 1))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_u32_scalar, 4))) return bail(rc);
+  cudaMemsetAsync(s->d_ref_vertex, 0, px * 16, s->stream);
+  cudaMemsetAsync(s->d_ref_normal, 0, px * 16, s->stream);
+  cudaMemsetAsync(s->d_sdf_rows, 0, px * 32, s->stream);
+  if (cudaMallocHost((void**)&s->h_state, sizeof(KfDevState)) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  if (cudaMallocHost((void**)&s->h_depth_pinned, px * 2) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  if (cudaMallocHost((void**)&s->h_u32_scalar, 16) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  std::memset(s->h_state, 0, sizeof(KfDevState));
+  std::memcpy(s->h_state->pose, kIdentity, sizeof(kIdentity));
+  std::memcpy(s->h_state->pose_eig, kIdentity, sizeof(kIdentity));
+  std::memcpy(s->h_state->old_pose, kIdentity, sizeof(kIdentity));
+  std::memcpy(s->h_state->raycast_pose, kIdentity, sizeof(kIdentity));
+  s->h_state->reset_window = 1;
+  if ((rc = push_state(s))) return bail(rc);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return bail(KF_ERR_CUDA);
+  *out = s;
+  return KF_OK;
+}
+
+int kf_destroy(kf_session* s) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  free_all(s);
+  delete s;
+  return KF_OK;
+}
+
+const char* kf_last_error(const kf_session* s) { return s ? s->last_error.c_str() : "null session"; }
+
+int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
+  if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
+  int rc;
+  if (delete_flag) {
+    KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    drop_graph(s);
+    if ((rc = alloc_volume(s))) return rc;
+  } else {
+    KF_CUDA_TRY(s, cudaMemsetAsync(s->d_vol, 0, s->vol_bytes, s->stream));
+  }
+  if ((rc = pull_state(s))) return rc;
+  s->h_state->lib_size = 0;  // poseLibrary.resize(0)
+  set_pose_fields(s, pose, true);
+  // the app's "Reset Volume" (kinect.cpp:446-477): reset = true, counter = 0, then a
+  // raycast of the empty volume, i.e. zero reference maps
+  s->h_state->reset_window = 1;
+  s->h_state->counter = 0;
+  std::memcpy(s->h_state->raycast_pose, pose, 16 * sizeof(double));
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_ref_vertex, 0, px * 16, s->stream));
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_ref_normal, 0, px * 16, s->stream));
+  free_mc(s);
+  return push_state(s);
+}
+
+int kf_reset_volume(kf_session* s) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_vol, 0, s->vol_bytes, s->stream));
+  return KF_OK;
+}
+
+int kf_reset_pose(kf_session* s, const double pose[16]) {
+  if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  set_pose_fields(s, pose, true);
+  return push_state(s);
+}
+
+int kf_set_pose(kf_session* s, const double pose[16]) {
+  if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  set_pose_fields(s, pose, false);
+  return push_state(s);
+}
+
+int kf_get_pose(kf_session* s, double pose[16]) {
+  if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  std::memcpy(pose, s->h_state->pose, 16 * sizeof(double));
+  return KF_OK;
+}
+
+int kf_set_config(kf_session* s, const kf_config* cfg) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  int rc = validate(cfg, &s->intr);
+  if (rc) return rc;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  const bool realloc = cfg->nx != s->cfg.nx || cfg->ny != s->cfg.ny || cfg->nz != s->cfg.nz ||
+                       cfg->storage != s->cfg.storage;
+  s->cfg = *cfg;
+  if (s->cfg.integrate_every <= 0) s->cfg.integrate_every = 1;
+  drop_graph(s);
+  if (realloc) {
+    free_mc(s);
+    if ((rc = alloc_volume(s))) return rc;
+  }
+  return KF_OK;
+}
+
+int kf_depth_to_vertex_f32(kf_session* s, const float* host_depth_mm) {
+  if (!s || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_f32_in, host_depth_mm, px * 4, cudaMemcpyHostToDevice, s->stream));
+  int rc = kf_launch_pyramid(s, nullptr, s->d_depth_f32_in);
+  if (rc) return rc;
+  return kf_launch_vertex(s);
+}
+
+int kf_depth_to_vertex_u16(kf_session* s, const uint16_t* host_depth_mm) {
+  if (!s || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->stream));
+  int rc = kf_launch_pyramid(s, s->d_depth_u16, nullptr);
+  if (rc) return rc;
+  return kf_launch_vertex(s);
+}
+
+int kf_depth_to_vertex_u16_device(kf_session* s, const uint16_t* device_depth_mm) {
+  if (!s || !device_depth_mm) return KF_ERR_INVALID_ARGUMENT;
+  int rc = kf_launch_pyramid(s, device_depth_mm, nullptr);
+  if (rc) return rc;
+  return kf_launch_vertex(s);
+}
+
+int kf_vertex_to_normal(kf_session* s) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  return kf_launch_normal(s);
+}
+
+int kf_track_icp(kf_session* s, int* tracked) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  int rc = record(s, 6);
+  if (!rc) rc = kf_launch_icp(s, 0);
+  if (!rc) rc = record(s, 7);
+  if (rc || !tracked) return rc;
+  if ((rc = pull_state_head(s))) return rc;
+  *tracked = s->h_state->tracked;
+  cudaEventElapsedTime(&s->stage_ms[1], s->ev[6], s->ev[7]);
+  return KF_OK;
+}
+
+int kf_track_sdf(kf_session* s, int* tracked) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  int rc = kf_launch_sdf(s, 0, 0, 0);
+  if (rc || !tracked) return rc;
+  if ((rc = pull_state(s))) return rc;
+  *tracked = s->h_state->tracked;
+  return KF_OK;
+}
+
+int kf_recover_pose(kf_session* s, int* found) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  int rc = kf_launch_sdf(s, 1, 0, 0);
+  if (rc || !found) return rc;
+  if ((rc = pull_state(s))) return rc;
+  *found = s->h_state->recover_found;
+  return KF_OK;
+}
+
+int kf_get_alignment_energy(kf_session* s, float* ae) {
+  if (!s || !ae) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  *ae = (float)s->h_state->ae;
+  return KF_OK;
+}
+
+int kf_get_reduction(kf_session* s, float sums[32]) {
+  if (!s || !sums) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  for (int k = 0; k < 32; ++k) sums[k] = (float)s->h_state->sums[k];
+  return KF_OK;
+}
+
+int kf_integrate(kf_session* s) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  int rc = record(s, 8);
+  if (!rc) rc = kf_launch_integrate(s, 0);
+  if (!rc) rc = record(s, 9);
+  return rc;
+}
+
+int kf_raycast(kf_session* s) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  int rc = record(s, 10);
+  if (!rc) rc = kf_launch_raycast(s);
+  if (!rc) rc = record(s, 11);
+  return rc;
+}
+
+int kf_frame_step_u16(kf_session* s, const uint16_t* host_depth_mm, int* tracked) {
+  if (!s || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->stream));
+  int rc = run_frame(s);
+  if (rc) return rc;
+  return finish_step(s, tracked);
+}
+
+int kf_frame_step_u16_device(kf_session* s, const uint16_t* device_depth_mm, int* tracked) {
+  if (!s || !device_depth_mm) return KF_ERR_INVALID_ARGUMENT;
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, device_depth_mm, px * 2, cudaMemcpyDeviceToDevice, s->stream));
+  int rc = run_frame(s);
+  if (rc) return rc;
+  return finish_step(s, tracked);
+}
+
+static int copy_out(kf_session* s, void* dst, const void* src, size_t bytes) {
+  KF_CUDA_TRY(s, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream));
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return KF_OK;
+}
+
+int kf_get_raycast(kf_session* s, float* v, float* n) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  int rc = KF_OK;
+  if (v) rc = copy_out(s, v, s->d_ref_vertex, px * 16);
+  if (!rc && n) rc = copy_out(s, n, s->d_ref_normal, px * 16);
+  return rc;
+}
+
+int kf_get_vertex_map(kf_session* s, int level, float* v) {
+  if (!s || !v || level < 0 || level > 2) return KF_ERR_INVALID_ARGUMENT;
+  return copy_out(s, v, s->d_vertex[level], (size_t)s->W[level] * s->H[level] * 16);
+}
+
+int kf_get_normal_map(kf_session* s, int level, float* n) {
+  if (!s || !n || level < 0 || level > 2) return KF_ERR_INVALID_ARGUMENT;
+  return copy_out(s, n, s->d_normal[level], (size_t)s->W[level] * s->H[level] * 16);
+}
+
+int kf_get_depth_map(kf_session* s, int level, float* d) {
+  if (!s || !d || level < 0 || level > 2) return KF_ERR_INVALID_ARGUMENT;
+  return copy_out(s, d, s->d_depth[level], (size_t)s->W[level] * s->H[level] * 4);
+}
+
+int kf_get_track_status(kf_session* s, int level, int32_t* st) {
+  if (!s || !st || level < 0 || level > 2) return KF_ERR_INVALID_ARGUMENT;
+  return copy_out(s, st, s->d_status[level], (size_t)s->W[level] * s->H[level] * 4);
+}
+
+int kf_get_volume(kf_session* s, kf_volume_view* v) {
+  if (!s || !v) return KF_ERR_INVALID_ARGUMENT;
+  v->device_ptr = s->d_vol;
+  v->nx = s->cfg.nx; v->ny = s->cfg.ny; v->nz = s->cfg.nz;
+  v->storage = s->cfg.storage;
+  v->value_bytes = (int64_t)s->vol_value_bytes;
+  v->weight_offset_bytes = (int64_t)(s->vol_count * s->vol_value_bytes);
+  v->row_pitch_bytes = (int64_t)s->cfg.nx * v->value_bytes;
+  v->slice_pitch_bytes = v->row_pitch_bytes * s->cfg.ny;
+  return KF_OK;
+}
+
+int kf_copy_volume_to_host(kf_session* s, void* dst, uint64_t bytes) {
+  if (!s || !dst || bytes != s->vol_bytes) return KF_ERR_INVALID_ARGUMENT;
+  return copy_out(s, dst, s->d_vol, bytes);
+}
+
+int kf_copy_volume_from_host(kf_session* s, const void* src, uint64_t bytes) {
+  if (!s || !src || bytes != s->vol_bytes) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_vol, src, bytes, cudaMemcpyHostToDevice, s->stream));
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return KF_OK;
+}
+
+int kf_get_cum_twist(kf_session* s, double t[6]) {
+  if (!s || !t) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  std::memcpy(t, s->h_state->cum_twist, 6 * sizeof(double));
+  return KF_OK;
+}
+
+int kf_get_pose_library_size(kf_session* s, int* n) {
+  if (!s || !n) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  *n = s->h_state->lib_size;
+  return KF_OK;
+}
+
+int kf_get_stage_times(kf_session* s, float ms[6]) {
+  if (!s || !ms) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  int rc = harvest_all(s);
+  if (rc) return rc;
+  for (int i = 0; i < 6; ++i) ms[i] = s->stage_ms[i];
+  return KF_OK;
+}
+
+int kf_get_stage_stats(kf_session* s, double mean_ms[6], uint64_t* frames) {
+  if (!s || !mean_ms || !frames) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  int rc = harvest_all(s);
+  if (rc) return rc;
+  *frames = s->stage_frames;
+  for (int i = 0; i < 6; ++i) mean_ms[i] = s->stage_frames ? s->stage_acc[i] / (double)s->stage_frames : 0.0;
+  return KF_OK;
+}
+
+int kf_reset_stage_stats(kf_session* s) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  int rc = harvest_all(s);
+  if (rc) return rc;
+  for (int i = 0; i < 6; ++i) s->stage_acc[i] = 0.0;
+  s->stage_frames = 0;
+  return KF_OK;
+}
+
+int kf_get_launch_count(kf_session* s, uint64_t* launches) {
+  if (!s || !launches) return KF_ERR_INVALID_ARGUMENT;
+  *launches = s->launches;
+  return KF_OK;
+}
+
+int kf_get_stream(kf_session* s, void** stream) {
+  if (!s || !stream) return KF_ERR_INVALID_ARGUMENT;
+  *stream = (void*)s->stream;
+  return KF_OK;
+}
+
+}  // extern "C"

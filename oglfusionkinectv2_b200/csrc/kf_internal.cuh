@@ -1,0 +1,418 @@
+// kf_internal.cuh — shared internals of the B200 KinectFusion core (not part of the ABI).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/kf.h"
+
+#define KF_MAX_LIBRARY 64         // pose library entries kept on the device
+#define KF_TRACK_THREADS 256      // threads per block of the persistent tracking kernels
+#define KF_MAX_TRACK_BLOCKS 1024  // upper bound of the persistent grid
+
+// Device-side error word values (KfDevState::error).
+#define KF_DEV_ERR_TIMEOUT 1
+
+// Spin-wait budget of the software grid barrier, in SM clock cycles (~0.5 s at 1.9 GHz).
+#define KF_BARRIER_SPIN_CYCLES (1000000000LL)
+
+// Device control block: everything the per-frame step keeps resident between kernels.
+// Poses are camera-to-world, column-major, FP64.
+struct KfDevState {
+  // ---- frame result: the bytes the host reads after every frame step ----
+  double pose[16];      // m_pose
+  int tracked;          // result of the last Track()/TrackSDF()
+  int error;            // KF_DEV_ERR_* (sticky until the host clears it)
+  int recover_found;    // result of the last recoverPose()
+  int counter;          // kinect.cpp frame counter
+  // ---- the rest of the resident state ----
+  double pose_eig[16];  // m_pose_eig (the SDF tracker's own pose chain)
+  double old_pose[16];  // pose at the start of the last tracking call
+  double raycast_pose[16];  // pose of the last raycast (projective association, Q4 clear)
+  double cum_twist[6];  // m_cumTwist
+  double sums[32];      // last reduction row (FP64 sum of the per-block FP32 partials)
+  double ae;            // alignment energy of the last iteration
+  int lib_size;
+  int need_recover;     // frame policy: tracking failed this frame
+  int do_integrate;     // frame policy: integrate this frame
+  int reset_window;     // kinect.cpp `reset` flag
+  int iterations_run;   // ICP/SDF iterations executed by the last tracking call
+  unsigned barrier_count;
+  unsigned barrier_gen;
+  int pad0_;
+  // hand-over between iterations of the persistent tracking kernels
+  double iter_pose[16]; // pose after the last solve (ICP) / camera-to-world (SDF)
+  double iter_result[6];// SDF twist accumulator
+  int iter_conv;        // convergence flag of the last solve
+  int pad_[3];
+  double lib_pose[KF_MAX_LIBRARY][16];  // pose library
+};
+// Bytes of KfDevState the host reads after a frame step (pose and result flags).
+#define KF_STATE_RESULT_BYTES (offsetof(KfDevState, pose_eig))
+
+struct kf_session {
+  kf_config cfg{};
+  kf_intrinsics intr{};
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+
+  // volume: value plane then weight plane
+  void* d_vol = nullptr;
+  size_t vol_count = 0;
+  size_t vol_value_bytes = 0;
+  size_t vol_bytes = 0;
+
+  // image pyramid
+  int W[3] = {0, 0, 0}, H[3] = {0, 0, 0};
+  uint16_t* d_depth_u16 = nullptr;  // upload staging (device)
+  float* d_depth_f32_in = nullptr;  // float upload staging (device)
+  float* d_depth[3] = {nullptr, nullptr, nullptr};
+  float4* d_vertex[3] = {nullptr, nullptr, nullptr};
+  float4* d_normal[3] = {nullptr, nullptr, nullptr};
+  int32_t* d_status[3] = {nullptr, nullptr, nullptr};
+  float4* d_ref_vertex = nullptr;
+  float4* d_ref_normal = nullptr;
+  float* d_sdf_rows = nullptr;  // persistent trackSDF rows, 8 floats per level-0 pixel
+  float* d_partials = nullptr;  // [2][KF_MAX_TRACK_BLOCKS][32]
+
+  KfDevState* d_state = nullptr;
+  KfDevState* h_state = nullptr;  // pinned mirror
+  uint16_t* h_depth_pinned = nullptr;
+
+  int track_blocks = 0;  // persistent grid of the tracking kernels
+
+  // frame-step CUDA graphs: a ring of instances, each with its own stage events, so the
+  // stage times of every frame can be read back without stalling the stream
+  static const int kRing = 4;
+  cudaGraphExec_t frame_exec[kRing] = {};
+  cudaEvent_t ring_ev[kRing][6] = {};
+  int ring_pending[kRing] = {};  // slot holds an unread frame
+  int frame_kernels = 0;         // kernels in one frame graph
+  uint64_t frames_run = 0;
+  double stage_acc[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t stage_frames = 0;
+  uint64_t launches = 0;         // kernels launched by this session
+
+  // stage timing of the individual entry points
+  cudaEvent_t ev[12] = {};
+  float stage_ms[6] = {0, 0, 0, 0, 0, 0};
+  bool timing = false;
+  bool capturing = false;
+
+  // marching cubes
+  uint32_t* d_mc_base = nullptr;  // nx*ny*nz cubes: numTri | cubeIndex << 16
+  std::vector<uint32_t*> d_mc_levels;  // level k >= 1, (P >> k)^3
+  int mc_P = 0, mc_top = 0;
+  float4* d_mc_vertices = nullptr;
+  size_t mc_vertex_cap = 0;
+  uint32_t mc_triangles = 0;
+  int mc_valid = 0;
+  uint32_t* d_mc_scratch = nullptr;  // scan path: verts, offsets, cube index
+  size_t mc_scratch_words = 0;
+  uint32_t* d_u32_scalar = nullptr;  // one device word for totals
+  uint32_t* h_u32_scalar = nullptr;  // pinned
+};
+
+// ---------------------------------------------------------------------------------------
+// error helpers
+#define KF_CUDA_TRY(s, expr)                                                          \
+  do {                                                                                \
+    cudaError_t e_ = (expr);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      (s)->last_error = std::string(#expr) + ": " + cudaGetErrorString(e_);          \
+      return KF_ERR_CUDA;                                                             \
+    }                                                                                 \
+  } while (0)
+
+// ---------------------------------------------------------------------------------------
+// storage policy: value/weight planes
+template <int S>
+struct Vox;
+
+template <>
+struct Vox<KF_STORAGE_F32F32> {
+  typedef float V;
+  typedef float Wt;
+  static constexpr float kRawToF = 1.0f;
+  __device__ static __forceinline__ float raw(const V* f, size_t i) { return __ldg(f + i); }
+  __device__ static __forceinline__ float raw_nc(const V* f, size_t i) { return f[i]; }
+  __device__ static __forceinline__ float weight(const Wt* w, size_t i) { return w[i]; }
+  __device__ static __forceinline__ V encode_value(float F) { return F; }
+  __device__ static __forceinline__ Wt encode_weight(float w) { return w; }
+};
+
+template <>
+struct Vox<KF_STORAGE_F16U16> {
+  typedef __half V;
+  typedef uint16_t Wt;
+  static constexpr float kRawToF = 1.0f;
+  __device__ static __forceinline__ float raw(const V* f, size_t i) { return __half2float(__ldg(f + i)); }
+  __device__ static __forceinline__ float raw_nc(const V* f, size_t i) { return __half2float(f[i]); }
+  __device__ static __forceinline__ float weight(const Wt* w, size_t i) { return (float)w[i]; }
+  __device__ static __forceinline__ V encode_value(float F) { return __float2half_rn(F); }
+  __device__ static __forceinline__ Wt encode_weight(float w) {
+    return (uint16_t)fminf(fmaxf(w, 0.0f), 65535.0f);
+  }
+};
+
+template <>
+struct Vox<KF_STORAGE_RG16I> {
+  typedef int16_t V;
+  typedef int16_t Wt;
+  // vs() of integrate.cs:42 / raycast.cs:81: float(data.x) * 0.00003051944088f
+  static constexpr float kRawToF = 0.00003051944088f;
+  __device__ static __forceinline__ float raw(const V* f, size_t i) { return (float)__ldg(f + i); }
+  __device__ static __forceinline__ float raw_nc(const V* f, size_t i) { return (float)f[i]; }
+  __device__ static __forceinline__ float weight(const Wt* w, size_t i) { return (float)w[i]; }
+  // set() of integrate.cs:45-50: int(F * 32766), int(w)
+  __device__ static __forceinline__ V encode_value(float F) { return (int16_t)(int)(F * 32766.0f); }
+  __device__ static __forceinline__ Wt encode_weight(float w) { return (int16_t)(int)w; }
+};
+
+// ---------------------------------------------------------------------------------------
+// FP64 pose math (column-major 4x4, glm layout), host and device
+__host__ __device__ inline void kf_mat4_mul(const double* a, const double* b, double* out) {
+  double r[16];
+  for (int c = 0; c < 4; ++c)
+    for (int rr = 0; rr < 4; ++rr) {
+      double s = 0;
+      for (int k = 0; k < 4; ++k) s += a[k * 4 + rr] * b[c * 4 + k];
+      r[c * 4 + rr] = s;
+    }
+  for (int i = 0; i < 16; ++i) out[i] = r[i];
+}
+
+// Inverse of a rigid transform [R t; 0 1]: [R^T, -R^T t].
+__host__ __device__ inline void kf_rigid_inverse(const double* T, double* out) {
+  double r[16];
+  for (int c = 0; c < 3; ++c)
+    for (int rr = 0; rr < 3; ++rr) r[c * 4 + rr] = T[rr * 4 + c];
+  for (int rr = 0; rr < 3; ++rr)
+    r[12 + rr] = -(r[rr] * T[12] + r[4 + rr] * T[13] + r[8 + rr] * T[14]);
+  r[3] = r[7] = r[11] = 0;
+  r[15] = 1;
+  for (int i = 0; i < 16; ++i) out[i] = r[i];
+}
+
+// glm::eulerAngleXYZ(t1,t2,t3) = Rx(t1) * Ry(t2) * Rz(t3) (used at gFusion.cpp:700),
+// written out from the three elementary rotations; column-major 3x3.
+__host__ __device__ inline void kf_euler_xyz(double a, double b, double c, double* R) {
+  double sa, ca, sb, cb, sc, cc;
+  sincos(a, &sa, &ca);
+  sincos(b, &sb, &cb);
+  sincos(c, &sc, &cc);
+  // column 0
+  R[0] = cb * cc;
+  R[1] = ca * sc + sa * sb * cc;
+  R[2] = sa * sc - ca * sb * cc;
+  // column 1
+  R[3] = -cb * sc;
+  R[4] = ca * cc - sa * sb * sc;
+  R[5] = sa * cc + ca * sb * sc;
+  // column 2
+  R[6] = sb;
+  R[7] = -sa * cb;
+  R[8] = ca * cb;
+}
+
+// exp of Twist(xi) (gFusion.cpp:811-833): closed-form SE(3) exponential, xi = (w, v).
+__host__ __device__ inline void kf_se3_exp(const double* xi, double* T) {
+  const double w0 = xi[0], w1 = xi[1], w2 = xi[2];
+  const double th2 = w0 * w0 + w1 * w1 + w2 * w2;
+  const double th = sqrt(th2);
+  double A, B, C;
+  if (th < 1e-6) {
+    A = 1 - th2 / 6 + th2 * th2 / 120;
+    B = 0.5 - th2 / 24 + th2 * th2 / 720;
+    C = 1.0 / 6 - th2 / 120 + th2 * th2 / 5040;
+  } else {
+    double s, c;
+    sincos(th, &s, &c);
+    A = s / th;
+    B = (1 - c) / th2;
+    C = (th - s) / (th2 * th);
+  }
+  // [w]x column-major
+  const double W[9] = {0, w2, -w1, -w2, 0, w0, w1, -w0, 0};
+  double W2[9];
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += W[k * 3 + r] * W[c * 3 + k];
+      W2[c * 3 + r] = s;
+    }
+  double R[9], V[9];
+  for (int i = 0; i < 9; ++i) {
+    double I = (i % 4 == 0) ? 1.0 : 0.0;
+    R[i] = I + A * W[i] + B * W2[i];
+    V[i] = I + B * W[i] + C * W2[i];
+  }
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) T[c * 4 + r] = R[c * 3 + r];
+  for (int r = 0; r < 3; ++r) T[12 + r] = V[r] * xi[3] + V[3 + r] * xi[4] + V[6 + r] * xi[5];
+  T[3] = T[7] = T[11] = 0;
+  T[15] = 1;
+}
+
+// FP64 Cholesky solve of the 6x6 SPD normal equations.  Returns 0 and x = 0 when a pivot
+// is not positive (rank-deficient C, where the reference's JacobiSVD would return the
+// minimum-norm solution; an all-zero system gives x = 0 in both).
+__host__ __device__ inline int kf_cholesky6(const double* C, const double* b, double* x) {
+  double L[36];
+  for (int i = 0; i < 36; ++i) L[i] = 0;
+  double dmax = 0;
+  for (int i = 0; i < 6; ++i) dmax = fmax(dmax, fabs(C[i * 7]));
+  const double eps = 1e-13 * dmax;
+  for (int j = 0; j < 6; ++j) {
+    double d = C[j * 7];
+    for (int k = 0; k < j; ++k) d -= L[j * 6 + k] * L[j * 6 + k];
+    if (!(d > eps)) {
+      for (int i = 0; i < 6; ++i) x[i] = 0;
+      return 0;
+    }
+    double ljj = sqrt(d);
+    L[j * 7] = ljj;
+    for (int i = j + 1; i < 6; ++i) {
+      double v = C[i * 6 + j];
+      for (int k = 0; k < j; ++k) v -= L[i * 6 + k] * L[j * 6 + k];
+      L[i * 6 + j] = v / ljj;
+    }
+  }
+  double y[6];
+  for (int i = 0; i < 6; ++i) {
+    double v = b[i];
+    for (int k = 0; k < i; ++k) v -= L[i * 6 + k] * y[k];
+    y[i] = v / L[i * 7];
+  }
+  for (int i = 5; i >= 0; --i) {
+    double v = y[i];
+    for (int k = i + 1; k < 6; ++k) v -= L[k * 6 + i] * x[k];
+    x[i] = v / L[i * 7];
+  }
+  return 1;
+}
+
+// LDL^T solve (C.ldlt().solve(b), gFusion.cpp:902), unpivoted; NaN in, NaN out.
+__host__ __device__ inline void kf_ldlt6(const double* C, const double* b, double* x) {
+  double L[36], D[6];
+  for (int i = 0; i < 36; ++i) L[i] = 0;
+  for (int j = 0; j < 6; ++j) {
+    double d = C[j * 7];
+    for (int k = 0; k < j; ++k) d -= L[j * 6 + k] * L[j * 6 + k] * D[k];
+    D[j] = d;
+    L[j * 7] = 1;
+    for (int i = j + 1; i < 6; ++i) {
+      double v = C[i * 6 + j];
+      for (int k = 0; k < j; ++k) v -= L[i * 6 + k] * L[j * 6 + k] * D[k];
+      L[i * 6 + j] = v / d;
+    }
+  }
+  double y[6];
+  for (int i = 0; i < 6; ++i) {
+    double v = b[i];
+    for (int k = 0; k < i; ++k) v -= L[i * 6 + k] * y[k];
+    y[i] = v;
+  }
+  for (int i = 0; i < 6; ++i) y[i] /= D[i];
+  for (int i = 5; i >= 0; --i) {
+    double v = y[i];
+    for (int k = i + 1; k < 6; ++k) v -= L[k * 6 + i] * x[k];
+    x[i] = v;
+  }
+}
+
+// makeJTJ (gFusion.h:472-487): symmetric 6x6 from the 21 upper-triangular sums.
+__host__ __device__ inline void kf_make_jtj(const double* v21, double* C) {
+  int k = 0;
+  for (int i = 0; i < 6; ++i)
+    for (int j = i; j < 6; ++j) {
+      C[i * 6 + j] = v21[k];
+      C[j * 6 + i] = v21[k];
+      ++k;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Grid hand-over for the persistent (cooperatively launched) tracking kernels.
+// kf_grid_arrive: every block calls it after writing its partial sums; it returns true
+// in exactly one block (the last to arrive), which then reduces, solves and calls
+// kf_grid_release.  The other blocks wait in kf_grid_wait.  Every wait is bounded: after
+// KF_BARRIER_SPIN_CYCLES the block records KF_DEV_ERR_TIMEOUT in st->error and stops;
+// callers leave their loops when kf_grid_wait returns false.
+__device__ inline bool kf_grid_arrive(KfDevState* st, unsigned nblocks, unsigned* s_gen,
+                                      int* s_last) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *s_gen = *(volatile unsigned*)&st->barrier_gen;
+    __threadfence();
+    unsigned arrived = atomicAdd(&st->barrier_count, 1u) + 1u;
+    *s_last = (arrived == nblocks);
+    __threadfence();
+  }
+  __syncthreads();
+  return *s_last != 0;
+}
+
+__device__ inline void kf_grid_release(KfDevState* st) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st->barrier_count = 0;
+    __threadfence();
+    atomicAdd(&st->barrier_gen, 1u);
+  }
+}
+
+__device__ inline bool kf_grid_wait(KfDevState* st, const unsigned* s_gen, int* s_flag) {
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = &st->barrier_gen;
+    int ok = 1;
+    long long t0 = clock64();
+    while (*vgen == *s_gen) {
+      if (*(volatile int*)&st->error) { ok = 0; break; }
+      if (clock64() - t0 > KF_BARRIER_SPIN_CYCLES) {
+        atomicExch(&st->error, KF_DEV_ERR_TIMEOUT);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    if (*(volatile int*)&st->error) ok = 0;
+    *s_flag = ok;
+  }
+  __syncthreads();
+  return *s_flag != 0;
+}
+
+// Count kernels launched outside graph capture (captured graphs are counted per replay).
+inline void kf_note_launch(kf_session* s, int n = 1) {
+  if (!s->capturing) s->launches += (uint64_t)n;
+}
+
+// ---------------------------------------------------------------------------------------
+// launchers (one per .cu file)
+int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32);
+int kf_launch_vertex(kf_session* s);
+int kf_launch_normal(kf_session* s);
+int kf_launch_vertex_normal(kf_session* s);
+int kf_launch_icp(kf_session* s, int frame_policy);
+int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy);
+int kf_launch_sdf_policy(kf_session* s);
+int kf_launch_integrate(kf_session* s, int gated);
+int kf_launch_raycast(kf_session* s);
+int kf_mc_run(kf_session* s, float iso, int method, uint32_t* n_tri);
+int kf_scan_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* d_total,
+                cudaStream_t stream, uint32_t* d_scratch, size_t scratch_words);
+size_t kf_scan_scratch_words(uint64_t n);
+int kf_occupancy_blocks(kf_session* s, const void* kernel, int threads, size_t smem);

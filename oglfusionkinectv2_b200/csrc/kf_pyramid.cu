@@ -1,0 +1,179 @@
+// kf_pyramid.cu — depth ingest, mip pyramid, vertex and normal maps.
+//
+// Reference: gFusion::depthToVertex (src/gFusion.cpp:496-526) with glGenerateMipmap at
+// :508 and shaders/depthToVert.cs:33-72; gFusion::vertexToNormal (:528-547) with
+// shaders/vertToNorm.cs:9-57.
+//
+// B200 layout: one kernel turns the uint16 (or float) frame into the three float depth
+// levels (2x2 box means, zeros included, level 2 built from level 1 in shared memory);
+// a second kernel covers the pixels of all three levels in one grid and writes vertex
+// and/or normal float4 maps.  Bytes are tiny (~11 MB per frame), so both are
+// latency-bound; fusing the three levels into one launch each is what matters.
+#include "kf_internal.cuh"
+
+namespace {
+
+struct PyrArgs {
+  const uint16_t* in_u16;
+  const float* in_f32;
+  float* depth[3];
+  int W[3], H[3];
+};
+
+// One thread per level-1 pixel; a 32x8 block also produces a 16x4 level-2 tile.
+__global__ void __launch_bounds__(256) depth_mip_kernel(PyrArgs a) {
+  __shared__ float s_l1[8][33];
+  const int x1 = blockIdx.x * 32 + threadIdx.x;
+  const int y1 = blockIdx.y * 8 + threadIdx.y;
+  float m = 0.0f;
+  if (x1 < a.W[1] && y1 < a.H[1]) {
+    const int W0 = a.W[0];
+    const size_t i0 = (size_t)(2 * y1) * W0 + 2 * x1;
+    float d00, d01, d10, d11;
+    if (a.in_u16) {
+      ushort2 r0 = *reinterpret_cast<const ushort2*>(a.in_u16 + i0);
+      ushort2 r1 = *reinterpret_cast<const ushort2*>(a.in_u16 + i0 + W0);
+      d00 = r0.x; d01 = r0.y; d10 = r1.x; d11 = r1.y;
+    } else {
+      float2 r0 = *reinterpret_cast<const float2*>(a.in_f32 + i0);
+      float2 r1 = *reinterpret_cast<const float2*>(a.in_f32 + i0 + W0);
+      d00 = r0.x; d01 = r0.y; d10 = r1.x; d11 = r1.y;
+    }
+    *reinterpret_cast<float2*>(a.depth[0] + i0) = make_float2(d00, d01);
+    *reinterpret_cast<float2*>(a.depth[0] + i0 + W0) = make_float2(d10, d11);
+    m = 0.25f * ((d00 + d01) + (d10 + d11));
+    a.depth[1][(size_t)y1 * a.W[1] + x1] = m;
+  }
+  s_l1[threadIdx.y][threadIdx.x] = m;
+  __syncthreads();
+  if (threadIdx.x < 16 && threadIdx.y < 4) {
+    const int x2 = blockIdx.x * 16 + threadIdx.x;
+    const int y2 = blockIdx.y * 4 + threadIdx.y;
+    if (x2 < a.W[2] && y2 < a.H[2]) {
+      const int tx = 2 * threadIdx.x, ty = 2 * threadIdx.y;
+      float v = 0.25f * ((s_l1[ty][tx] + s_l1[ty][tx + 1]) + (s_l1[ty + 1][tx] + s_l1[ty + 1][tx + 1]));
+      a.depth[2][(size_t)y2 * a.W[2] + x2] = v;
+    }
+  }
+}
+
+struct VNArgs {
+  const float* depth[3];
+  float4* vertex[3];
+  float4* normal[3];
+  int W[3], H[3];
+  int start[4];             // pixel offset of each level in the flat grid
+  float ifx[3], ify[3];     // invK[0][0], invK[1][1] per level (1/fx_l, 1/fy_l)
+  float mcx[3], mcy[3];     // invK[2][0], invK[2][1] per level (-cx_l/fx_l, -cy_l/fy_l)
+  int mode;                 // 1 vertex, 2 normal from stored vertex, 3 both from depth
+  int down_from_left;       // Q3
+};
+
+// (depth / 1000) * rotate(invK, (u, v, 1))  (depthToVert.cs:56)
+__device__ __forceinline__ float3 vertex_at(const VNArgs& a, int l, int x, int y) {
+  const float d = __ldg(a.depth[l] + (size_t)y * a.W[l] + x) / 1000.0f;
+  return make_float3(d * ((float)x * a.ifx[l] + a.mcx[l]), d * ((float)y * a.ify[l] + a.mcy[l]), d);
+}
+
+__device__ __forceinline__ float3 neighbour(const VNArgs& a, int l, int x, int y, bool from_depth) {
+  // imageLoad returns 0 outside the image; pix.x - 1 at x == 0 wraps to an invalid index
+  if (x < 0 || y < 0 || x >= a.W[l] || y >= a.H[l]) return make_float3(0.f, 0.f, 0.f);
+  if (from_depth) return vertex_at(a, l, x, y);
+  const float4 v = a.vertex[l][(size_t)y * a.W[l] + x];
+  return make_float3(v.x, v.y, v.z);
+}
+
+__global__ void __launch_bounds__(256) vertex_normal_kernel(VNArgs a) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= a.start[3]) return;
+  const int l = gid < a.start[1] ? 0 : (gid < a.start[2] ? 1 : 2);
+  const int local = gid - a.start[l];
+  const int x = local % a.W[l], y = local / a.W[l];
+  const size_t i = (size_t)local;
+  if (a.mode & 1) {
+    const float3 v = vertex_at(a, l, x, y);
+    a.vertex[l][i] = make_float4(v.x, v.y, v.z, 0.0f);
+  }
+  if (a.mode & 2) {
+    const bool fd = (a.mode == 3);
+    // vertToNorm.cs:23-26: left/right/up clamp on the high side only; "down" takes column
+    // x-1 in the reference (Q3)
+    const float3 lf = neighbour(a, l, x - 1, y, fd);
+    const float3 rt = neighbour(a, l, min(x + 1, a.W[l] - 1), y, fd);
+    const float3 up = neighbour(a, l, x, y - 1, fd);
+    const float3 dn = neighbour(a, l, a.down_from_left ? x - 1 : x, min(y + 1, a.H[l] - 1), fd);
+    float4 n;
+    if (lf.z == 0.f || rt.z == 0.f || up.z == 0.f || dn.z == 0.f) {
+      n = make_float4(2.f, 0.f, 0.f, 0.f);
+    } else {
+      const float3 dx = make_float3(rt.x - lf.x, rt.y - lf.y, rt.z - lf.z);
+      const float3 dy = make_float3(dn.x - up.x, dn.y - up.y, dn.z - up.z);
+      // normalize(cross(dyv, dxv))
+      const float cx = dy.y * dx.z - dy.z * dx.y;
+      const float cy = dy.z * dx.x - dy.x * dx.z;
+      const float cz = dy.x * dx.y - dy.y * dx.x;
+      const float inv = 1.0f / sqrtf(cx * cx + cy * cy + cz * cz);
+      n = make_float4(cx * inv, cy * inv, cz * inv, 1.0f);
+    }
+    a.normal[l][i] = n;
+  }
+}
+
+VNArgs make_vn_args(kf_session* s, int mode) {
+  VNArgs a;
+  int acc = 0;
+  for (int l = 0; l < 3; ++l) {
+    a.depth[l] = s->d_depth[l];
+    a.vertex[l] = s->d_vertex[l];
+    a.normal[l] = s->d_normal[l];
+    a.W[l] = s->W[l];
+    a.H[l] = s->H[l];
+    a.start[l] = acc;
+    acc += s->W[l] * s->H[l];
+    // getInverseCameraMatrix(m_camPamsDepth / float(1 << l)) in float (gFusion.cpp:517)
+    const float sc = (float)(1 << l);
+    const float fx = s->intr.fx / sc, fy = s->intr.fy / sc;
+    const float cx = s->intr.cx / sc, cy = s->intr.cy / sc;
+    a.ifx[l] = 1.0f / fx;
+    a.ify[l] = 1.0f / fy;
+    a.mcx[l] = -cx / fx;
+    a.mcy[l] = -cy / fy;
+  }
+  a.start[3] = acc;
+  a.mode = mode;
+  a.down_from_left = (s->cfg.quirks & KF_Q3_DOWN_FROM_LEFT) ? 1 : 0;
+  return a;
+}
+
+}  // namespace
+
+int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32) {
+  PyrArgs a;
+  a.in_u16 = d_u16;
+  a.in_f32 = d_u16 ? nullptr : d_f32;
+  for (int l = 0; l < 3; ++l) {
+    a.depth[l] = s->d_depth[l];
+    a.W[l] = s->W[l];
+    a.H[l] = s->H[l];
+  }
+  dim3 block(32, 8);
+  dim3 grid((s->W[1] + 31) / 32, (s->H[1] + 7) / 8);
+  depth_mip_kernel<<<grid, block, 0, s->stream>>>(a);
+  kf_note_launch(s);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  return KF_OK;
+}
+
+static int launch_vn(kf_session* s, int mode) {
+  VNArgs a = make_vn_args(s, mode);
+  const int threads = 256;
+  const int blocks = (a.start[3] + threads - 1) / threads;
+  vertex_normal_kernel<<<blocks, threads, 0, s->stream>>>(a);
+  kf_note_launch(s);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  return KF_OK;
+}
+
+int kf_launch_vertex(kf_session* s) { return launch_vn(s, 1); }
+int kf_launch_normal(kf_session* s) { return launch_vn(s, 2); }
+int kf_launch_vertex_normal(kf_session* s) { return launch_vn(s, 3); }

@@ -1,0 +1,371 @@
+"""Python mirror of the reference's gFusion and MCubes classes over the C ABI.
+
+Reference: class gFusion (include/gFusion.h:124-624) and class MCubes
+(include/mcubes.h:48-168).  Method names follow the reference so that code written
+against it reads the same; GL texture/buffer names become numpy arrays copied from the
+device.  Poses are 4x4 camera-to-world matrices in ordinary row-major numpy layout;
+they cross the ABI column-major (glm layout).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _pose_to_c(pose) -> C.Array:
+    m = np.asarray(pose, dtype=np.float64).reshape(4, 4)
+    return (C.c_double * 16)(*m.flatten(order="F"))
+
+
+def _pose_from_c(arr) -> np.ndarray:
+    return np.array(list(arr), dtype=np.float64).reshape(4, 4, order="F")
+
+
+@dataclass
+class GFusionConfig:
+    """gFusionConfig (gFusion.h:42-82) plus the storage / precision / quirk policy."""
+    volumeSize: tuple = (256, 256, 256)
+    volumeDimensions: tuple = (1.0, 1.0, 1.0)
+    mu: float = 0.05
+    maxWeight: float = 100.0
+    nearPlane: float = 0.1
+    farPlane: float = 3.0
+    dist_threshold: float = 0.05
+    normal_threshold: float = 0.8
+    iterations: tuple = (5, 5, 5)  # index 0 = finest level
+    storage: int = L.KF_STORAGE_F32F32
+    jtj: int = L.KF_JTJ_FP32
+    tracking: int = L.KF_TRACK_ICP
+    quirks: int = L.KF_QUIRKS_DEFAULT
+    integrate_every: int = 1
+
+    def stepSize(self) -> float:
+        """gFusionConfig::stepSize (gFusion.h:72-81)."""
+        return min(self.volumeDimensions) / max(self.volumeSize)
+
+    def to_c(self) -> L.kf_config:
+        c = L.kf_config()
+        c.nx, c.ny, c.nz = (int(v) for v in self.volumeSize)
+        c.dim_x, c.dim_y, c.dim_z = (float(v) for v in self.volumeDimensions)
+        c.mu = self.mu
+        c.max_weight = self.maxWeight
+        c.near_plane = self.nearPlane
+        c.far_plane = self.farPlane
+        c.dist_threshold = self.dist_threshold
+        c.normal_threshold = self.normal_threshold
+        for i in range(3):
+            c.iterations[i] = int(self.iterations[i])
+        c.storage = self.storage
+        c.jtj = self.jtj
+        c.tracking = self.tracking
+        c.quirks = self.quirks
+        c.integrate_every = self.integrate_every
+        return c
+
+
+@dataclass
+class Intrinsics:
+    fx: float = 365.0
+    fy: float = 365.0
+    cx: float = 256.0
+    cy: float = 212.0
+    width: int = 512
+    height: int = 424
+
+    def to_c(self) -> L.kf_intrinsics:
+        return L.kf_intrinsics(self.fx, self.fy, self.cx, self.cy, self.width, self.height)
+
+
+def volume_bytes(cfg: GFusionConfig) -> int:
+    n = int(np.prod(cfg.volumeSize))
+    return n * (4 if cfg.storage == L.KF_STORAGE_F32F32 else 2) * 2
+
+
+def decode_volume(raw: np.ndarray, cfg: GFusionConfig):
+    """Split a raw two-plane volume into (tsdf float32, weight float32) arrays [z, y, x]."""
+    nx, ny, nz = cfg.volumeSize
+    n = nx * ny * nz
+    if cfg.storage == L.KF_STORAGE_F32F32:
+        v = raw.view(np.float32)
+        F, W = v[:n], v[n:]
+    elif cfg.storage == L.KF_STORAGE_F16U16:
+        F = raw[:2 * n].view(np.float16).astype(np.float32)
+        W = raw[2 * n:].view(np.uint16).astype(np.float32)
+    else:
+        F = raw[:2 * n].view(np.int16).astype(np.float32) * np.float32(0.00003051944088)
+        W = raw[2 * n:].view(np.int16).astype(np.float32)
+    return F.reshape(nz, ny, nx), W.reshape(nz, ny, nx)
+
+
+class GFusion:
+    """B200 KinectFusion session with the gFusion method surface."""
+
+    def __init__(self, config: GFusionConfig | None = None, intrinsics: Intrinsics | None = None):
+        self.lib = L.load()
+        self.configuration = config or GFusionConfig()
+        self.intrinsics = intrinsics or Intrinsics()
+        self._cc = self.configuration.to_c()
+        self._ci = self.intrinsics.to_c()
+        h = C.c_void_p()
+        L.check(self.lib.kf_create(C.byref(self._cc), C.byref(self._ci), C.byref(h)), "kf_create")
+        self._h = h
+
+    # ---- lifecycle --------------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.kf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int, what: str) -> None:
+        if st != L.KF_OK:
+            msg = self.lib.kf_last_error(self._h)
+            raise L.KfError(st, what + (": " + msg.decode() if msg else ""))
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def setConfig(self, config: GFusionConfig) -> None:
+        self.configuration = config
+        self._cc = config.to_c()
+        self._check(self.lib.kf_set_config(self._h, C.byref(self._cc)), "kf_set_config")
+
+    # ---- pose / reset -----------------------------------------------------------------
+    def Reset(self, pose, deleteFlag: bool = False) -> None:
+        self._check(self.lib.kf_reset(self._h, _pose_to_c(pose), int(deleteFlag)), "kf_reset")
+
+    def resetVolume(self) -> None:
+        self._check(self.lib.kf_reset_volume(self._h), "kf_reset_volume")
+
+    def resetPose(self, pose) -> None:
+        self._check(self.lib.kf_reset_pose(self._h, _pose_to_c(pose)), "kf_reset_pose")
+
+    def setPose(self, pose) -> None:
+        self._check(self.lib.kf_set_pose(self._h, _pose_to_c(pose)), "kf_set_pose")
+
+    def getPose(self) -> np.ndarray:
+        a = (C.c_double * 16)()
+        self._check(self.lib.kf_get_pose(self._h, a), "kf_get_pose")
+        return _pose_from_c(a)
+
+    def getTransPose(self) -> np.ndarray:
+        return self.getPose()[:3, 3].copy()
+
+    def getCumTwist(self) -> np.ndarray:
+        a = (C.c_double * 6)()
+        self._check(self.lib.kf_get_cum_twist(self._h, a), "kf_get_cum_twist")
+        return np.array(list(a))
+
+    # ---- per-frame operations -----------------------------------------------------------
+    def depthToVertex(self, depth) -> None:
+        d = np.ascontiguousarray(depth)
+        if d.shape != (self.intrinsics.height, self.intrinsics.width):
+            raise ValueError(f"depth shape {d.shape}")
+        if d.dtype == np.uint16:
+            st = self.lib.kf_depth_to_vertex_u16(self._h, d.ctypes.data)
+        else:
+            d = np.ascontiguousarray(d, dtype=np.float32)
+            st = self.lib.kf_depth_to_vertex_f32(self._h, d.ctypes.data)
+        self._check(st, "kf_depth_to_vertex")
+
+    def vertexToNormal(self) -> None:
+        self._check(self.lib.kf_vertex_to_normal(self._h), "kf_vertex_to_normal")
+
+    def Track(self) -> bool:
+        t = C.c_int()
+        self._check(self.lib.kf_track_icp(self._h, C.byref(t)), "kf_track_icp")
+        return bool(t.value)
+
+    def TrackSDF(self) -> bool:
+        t = C.c_int()
+        self._check(self.lib.kf_track_sdf(self._h, C.byref(t)), "kf_track_sdf")
+        return bool(t.value)
+
+    def recoverPose(self) -> bool:
+        t = C.c_int()
+        self._check(self.lib.kf_recover_pose(self._h, C.byref(t)), "kf_recover_pose")
+        return bool(t.value)
+
+    def integrate(self) -> None:
+        self._check(self.lib.kf_integrate(self._h), "kf_integrate")
+
+    def raycast(self) -> None:
+        self._check(self.lib.kf_raycast(self._h), "kf_raycast")
+
+    def frameStep(self, depth_u16) -> bool:
+        """One iteration of the kinect.cpp:654-695 loop body."""
+        d = np.ascontiguousarray(depth_u16, dtype=np.uint16)
+        t = C.c_int()
+        self._check(self.lib.kf_frame_step_u16(self._h, d.ctypes.data, C.byref(t)), "kf_frame_step_u16")
+        return bool(t.value)
+
+    def frameStepDevice(self, device_ptr: int, sync: bool = True):
+        t = C.c_int()
+        st = self.lib.kf_frame_step_u16_device(self._h, C.c_void_p(device_ptr),
+                                               C.byref(t) if sync else None)
+        self._check(st, "kf_frame_step_u16_device")
+        return bool(t.value) if sync else None
+
+    # ---- accessors ----------------------------------------------------------------------
+    def _map(self, fn, level: int, comps: int, dtype=np.float32) -> np.ndarray:
+        w, h = self.intrinsics.width >> level, self.intrinsics.height >> level
+        out = np.empty((h, w, comps) if comps > 1 else (h, w), dtype=dtype)
+        self._check(fn(self._h, level, out.ctypes.data), fn.__name__)
+        return out
+
+    def getVerts(self) -> np.ndarray:
+        """Raycast vertex map (m_textureReferenceVertex), H x W x 4."""
+        v = np.empty((self.intrinsics.height, self.intrinsics.width, 4), np.float32)
+        self._check(self.lib.kf_get_raycast(self._h, v.ctypes.data, None), "kf_get_raycast")
+        return v
+
+    def getNorms(self) -> np.ndarray:
+        n = np.empty((self.intrinsics.height, self.intrinsics.width, 4), np.float32)
+        self._check(self.lib.kf_get_raycast(self._h, None, n.ctypes.data), "kf_get_raycast")
+        return n
+
+    def getVertexMap(self, level: int = 0) -> np.ndarray:
+        return self._map(self.lib.kf_get_vertex_map, level, 4)
+
+    def getNormalMap(self, level: int = 0) -> np.ndarray:
+        return self._map(self.lib.kf_get_normal_map, level, 4)
+
+    def getDepthImage(self, level: int = 0) -> np.ndarray:
+        return self._map(self.lib.kf_get_depth_map, level, 1)
+
+    def getTrackStatus(self, level: int = 0) -> np.ndarray:
+        return self._map(self.lib.kf_get_track_status, level, 1, np.int32)
+
+    def getVolumeRaw(self) -> np.ndarray:
+        raw = np.empty(volume_bytes(self.configuration), np.uint8)
+        self._check(self.lib.kf_copy_volume_to_host(self._h, raw.ctypes.data, raw.nbytes),
+                    "kf_copy_volume_to_host")
+        return raw
+
+    def setVolumeRaw(self, raw: np.ndarray) -> None:
+        raw = np.ascontiguousarray(raw, dtype=np.uint8)
+        self._check(self.lib.kf_copy_volume_from_host(self._h, raw.ctypes.data, raw.nbytes),
+                    "kf_copy_volume_from_host")
+
+    def getVolume(self):
+        """(tsdf, weight) float32 arrays indexed [z, y, x]."""
+        return decode_volume(self.getVolumeRaw(), self.configuration)
+
+    def getVolumeView(self) -> L.kf_volume_view:
+        v = L.kf_volume_view()
+        self._check(self.lib.kf_get_volume(self._h, C.byref(v)), "kf_get_volume")
+        return v
+
+    def alignmentEnergy(self) -> float:
+        f = C.c_float()
+        self._check(self.lib.kf_get_alignment_energy(self._h, C.byref(f)), "kf_get_alignment_energy")
+        return f.value
+
+    def getReduction(self) -> np.ndarray:
+        a = (C.c_float * 32)()
+        self._check(self.lib.kf_get_reduction(self._h, a), "kf_get_reduction")
+        return np.array(list(a), dtype=np.float32)
+
+    def poseLibrarySize(self) -> int:
+        n = C.c_int()
+        self._check(self.lib.kf_get_pose_library_size(self._h, C.byref(n)), "kf_get_pose_library_size")
+        return n.value
+
+    def getTimes(self) -> np.ndarray:
+        """Device ms of the last pyramid, track, integrate, recover, raycast stages."""
+        a = (C.c_float * 6)()
+        self._check(self.lib.kf_get_stage_times(self._h, a), "kf_get_stage_times")
+        return np.array(list(a), dtype=np.float32)
+
+    def stageStats(self):
+        """(mean device ms per stage [pyramid, track, integrate, recover, raycast, mc],
+        frames) over every frame step since resetStageStats()."""
+        a = (C.c_double * 6)()
+        n = C.c_uint64()
+        self._check(self.lib.kf_get_stage_stats(self._h, a, C.byref(n)), "kf_get_stage_stats")
+        return np.array(list(a)), n.value
+
+    def resetStageStats(self) -> None:
+        self._check(self.lib.kf_reset_stage_stats(self._h), "kf_reset_stage_stats")
+
+    def launchCount(self) -> int:
+        n = C.c_uint64()
+        self._check(self.lib.kf_get_launch_count(self._h, C.byref(n)), "kf_get_launch_count")
+        return n.value
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._check(self.lib.kf_get_stream(self._h, C.byref(p)), "kf_get_stream")
+        return p.value or 0
+
+
+class MCubes:
+    """Marching-cubes extraction of a GFusion volume (mcubes.h:48-168)."""
+
+    def __init__(self, fusion: GFusion | None = None):
+        self.fusion = fusion
+        self.isoLevel = 0.0
+        self.nTriangles = 0
+
+    def setVolumeTexture(self, fusion: GFusion) -> None:
+        self.fusion = fusion
+
+    def setIsolevel(self, iso: float) -> None:
+        self.isoLevel = float(iso)
+
+    def generateMarchingCubes(self, method: int = L.KF_MC_HISTOPYRAMID) -> int:
+        n = C.c_uint32()
+        f = self.fusion
+        f._check(f.lib.kf_mc_extract(f._h, self.isoLevel, method, C.byref(n)), "kf_mc_extract")
+        self.nTriangles = n.value
+        return n.value
+
+    def getNumberTriangles(self) -> int:
+        """Vertex count, as the reference's getNumberTriangles() (returns m_totalSum)."""
+        return 3 * self.nTriangles
+
+    def getVertices(self) -> np.ndarray:
+        f = self.fusion
+        out = np.empty((3 * self.nTriangles, 4), np.float32)
+        f._check(f.lib.kf_mc_copy_vertices(f._h, out.ctypes.data, out.shape[0]), "kf_mc_copy_vertices")
+        return out
+
+    def getBaseLevel(self) -> np.ndarray:
+        f = self.fusion
+        nx, ny, nz = f.configuration.volumeSize
+        out = np.empty(nx * ny * nz, np.uint32)
+        f._check(f.lib.kf_mc_copy_base_level(f._h, out.ctypes.data, out.size), "kf_mc_copy_base_level")
+        return out.reshape(nz, ny, nx)
+
+    def exportMesh(self, path: str) -> None:
+        f = self.fusion
+        f._check(f.lib.kf_mc_export_stl(f._h, path.encode()), "kf_mc_export_stl")
+
+    def exportPointCloud(self, path: str) -> None:
+        f = self.fusion
+        f._check(f.lib.kf_mc_export_ply(f._h, path.encode()), "kf_mc_export_ply")
+
+
+def prefix_sum_device(d_in: int, d_out: int, n: int, stream: int = 0) -> int:
+    """Exclusive scan of n uint32 device values; returns the total."""
+    lib = L.load()
+    tot = C.c_uint32()
+    L.check(lib.kf_prefix_sum_u32(C.c_void_p(d_in), C.c_void_p(d_out), n, C.byref(tot),
+                                  C.c_void_p(stream)), "kf_prefix_sum_u32")
+    return tot.value

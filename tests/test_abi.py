@@ -1,0 +1,73 @@
+"""The C-ABI library loads and exports every symbol include/kf.h declares (CPU only)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from oglfusionkinectv2_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "kf.h")).read()
+    return sorted(set(re.findall(r"^KF_API\s+[\w\s\*]+?\b(kf_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_the_api():
+    names = declared_symbols()
+    assert len(names) >= 40
+    assert set(names) == set(L.SIGNATURES), set(names) ^ set(L.SIGNATURES)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(L.LIB_PATH)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+    L.load()  # binds every signature
+
+
+def test_host_only_entry_points():
+    lib = L.load()
+    assert lib.kf_abi_version() == 1
+    c = L.kf_config()
+    assert lib.kf_config_default(C.byref(c)) == L.KF_OK
+    # gFusionConfig() defaults (gFusion.h:56-69)
+    assert (c.nx, c.mu, c.max_weight, c.near_plane, c.far_plane) == (256, pytest.approx(0.05), 100.0,
+                                                                     pytest.approx(0.1), 3.0)
+    assert list(c.iterations) == [5, 5, 5] and c.quirks == L.KF_QUIRKS_DEFAULT
+    assert lib.kf_status_string(L.KF_ERR_TIMEOUT) == b"device wait timed out"
+    b = C.c_uint64()
+    i = L.kf_intrinsics(365, 365, 256, 212, 512, 424)
+    assert lib.kf_session_device_bytes(C.byref(c), C.byref(i), C.byref(b)) == L.KF_OK
+    assert b.value > 256 ** 3 * 8
+    bad = L.kf_config.from_buffer_copy(c)
+    bad.mu = 0
+    assert lib.kf_session_device_bytes(C.byref(bad), C.byref(i), C.byref(b)) == L.KF_ERR_INVALID_ARGUMENT
+
+
+def test_quirk_presets_match_header():
+    text = open(os.path.join(ROOT, "include", "kf.h")).read()
+    for name in ["KF_Q1_LAST_GROUP_ONLY", "KF_Q3_DOWN_FROM_LEFT", "KF_Q4_SAME_PIXEL", "KF_Q6_SDF_D2_TWICE",
+                 "KF_Q7_SDF_LAST_COLUMN", "KF_Q8_NARROW_BAND", "KF_Q13_MC_FIRST_SEVEN",
+                 "KF_Q15_MC_BORDER_SKIP", "KF_Q18_STL_COUNT_X4", "KF_Q19_EIG_TRANSLATION",
+                 "KF_Q23_SDF_XY_OFFSET"]:
+        m = re.search(r"#define " + name + r" \(1u << (\d+)\)", text)
+        assert m and getattr(L, name) == 1 << int(m.group(1)), name
+
+
+def test_create_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    lib = L.load()
+    c = L.kf_config()
+    lib.kf_config_default(C.byref(c))
+    c.nx = c.ny = c.nz = 32
+    i = L.kf_intrinsics(365, 365, 256, 212, 512, 424)
+    h = C.c_void_p()
+    assert lib.kf_create(C.byref(c), C.byref(i), C.byref(h)) == L.KF_ERR_NO_DEVICE
+    from oglfusionkinectv2_b200 import GFusion
+    with pytest.raises(L.KfError):
+        GFusion()

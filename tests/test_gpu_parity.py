@@ -1,0 +1,222 @@
+"""GPU (CUDA, through the C ABI) vs FP64 oracle parity on identical inputs.
+
+Tolerances (north star): TSDF max-abs <= 1e-3 of the truncation (normalised units) on
+every voxel whose evaluation is unambiguous; per-frame pose <= 0.1 mm / 0.01 deg with
+teacher forcing; raycast vertex <= 0.5 mm; free-running ATE within 1 mm of the oracle.
+"""
+import numpy as np
+import pytest
+
+import kf_oracle as O
+from helpers import integrate_ambiguous, rot_deg, small_workload
+from oglfusionkinectv2_b200 import GFusion, synth, _lib as L
+
+pytestmark = pytest.mark.gpu
+
+STORAGES = [L.KF_STORAGE_F32F32, L.KF_STORAGE_F16U16, L.KF_STORAGE_RG16I]
+QUIRKS = {"tracking": L.KF_QUIRKS_TRACKING, "default": L.KF_QUIRKS_DEFAULT,
+          "reference": L.KF_QUIRKS_REFERENCE}
+
+
+def pair(w):
+    return GFusion(w.config, w.intrinsics), O.Oracle(w.config, w.intrinsics)
+
+
+def test_pyramid_parity():
+    w = small_workload(3)
+    g, o = pair(w)
+    f = w.frame(1)
+    for s in (g, o):
+        s.depthToVertex(f)
+        s.vertexToNormal()
+    for l in range(3):
+        np.testing.assert_allclose(g.getDepthImage(l), o.getDepthImage(l), rtol=1e-6)
+        Vg, Vo = g.getVertexMap(l), o.getVertexMap(l)
+        assert np.max(np.abs(Vg[..., :3] - Vo[..., :3])) < 2e-6
+        Ng, No = g.getNormalMap(l), o.getNormalMap(l)
+        np.testing.assert_array_equal(Ng[..., 0] == 2, No[..., 0] == 2)
+        valid = No[..., 0] != 2
+        err = np.linalg.norm(Ng[..., :3] - No[..., :3], axis=-1)[valid]
+        assert np.mean(err < 1e-4) > 0.9999 and err.max() < 1e-2
+    # float input path (the reference's depthToVertex(float*))
+    g.depthToVertex(f.astype(np.float32) + 0.25)
+    o.depthToVertex(f.astype(np.float32) + 0.25)
+    np.testing.assert_allclose(g.getDepthImage(0), o.getDepthImage(0), rtol=0)
+
+
+@pytest.mark.parametrize("storage", STORAGES)
+@pytest.mark.parametrize("quirks", ["tracking", "default"])
+def test_integrate_parity(storage, quirks):
+    w = small_workload(3, size=96, storage=storage, quirks=QUIRKS[quirks])
+    g, o = pair(w)
+    for s in (g, o):
+        s.Reset(w.poses[0])
+    for k in (0, 1):
+        f = w.frame(k)
+        oldF, oldW = o.getVolume()
+        if k:
+            g.setVolumeRaw(o.getVolumeRaw())  # identical input volume
+        for s in (g, o):
+            s.setPose(w.poses[k])
+            s.depthToVertex(f)
+            s.integrate()
+        Fg, Wg = g.getVolume()
+        Fo, Wo = o.getVolume()
+        bad = (np.abs(Fg - Fo) > 1e-3) | (Wg != Wo)
+        touched = (Wo > 0) | (Wg > 0)
+        idx = np.nonzero(bad)
+        amb = integrate_ambiguous(w.config, w.intrinsics, w.poses[k], f, oldF, oldW, idx)
+        assert touched.sum() > 1000
+        assert bad.sum() <= 1e-3 * touched.sum(), (bad.sum(), touched.sum())
+        assert amb.all(), f"{(~amb).sum()} unexplained voxel mismatches"
+
+
+@pytest.mark.parametrize("storage", STORAGES)
+def test_raycast_parity(storage):
+    w = small_workload(3, size=128, storage=storage)
+    g, o = pair(w)
+    o.Reset(w.poses[0])
+    for k in (0, 1):
+        o.setPose(w.poses[k])
+        o.depthToVertex(w.frame(k))
+        o.integrate()
+    g.setVolumeRaw(o.getVolumeRaw())
+    for s in (g, o):
+        s.setPose(w.poses[2])
+        s.raycast()
+    Vg, Ng = g.getVerts(), g.getNorms()
+    Vo, No = o.getVerts(), o.getNorms()
+    hg, ho = Vg[..., 3] > 0, Vo[..., 3] > 0
+    assert ho.mean() > 0.2
+    assert np.mean(hg == ho) > 0.999
+    both = hg & ho
+    err = np.linalg.norm(Vg[..., :3] - Vo[..., :3], axis=-1)[both]
+    assert np.mean(err <= 0.5e-3) > 0.999, np.percentile(err, [50, 99, 99.9])
+    nb = both & (No[..., 3] > 0) & (Ng[..., 3] > 0)
+    cosang = np.clip(np.einsum("ijk,ijk->ij", Ng[..., :3], No[..., :3])[nb], -1, 1)
+    assert np.mean(np.degrees(np.arccos(cosang)) < 1.0) > 0.99
+
+
+def _teacher_forced(w, k, track):
+    """Both sides track frame k from the pose of frame k-1 against identical reference
+    maps (the GPU raycast copied into the oracle) and an identical volume."""
+    g, o = pair(w)
+    o.Reset(w.poses[0])
+    for j in range(k):
+        o.setPose(w.poses[j])
+        o.depthToVertex(w.frame(j))
+        o.integrate()
+    g.Reset(w.poses[0])
+    g.setVolumeRaw(o.getVolumeRaw())
+    for s in (g, o):
+        s.setPose(w.poses[k - 1])
+        s.raycast()
+    o.setRaycast(g.getVerts().astype(np.float64), g.getNorms().astype(np.float64))
+    f = w.frame(k)
+    for s in (g, o):
+        s.depthToVertex(f)
+        s.vertexToNormal()
+    tg = getattr(g, track)()
+    to = getattr(o, track)()
+    return g, o, tg, to
+
+
+@pytest.mark.parametrize("jtj", [L.KF_JTJ_FP32, L.KF_JTJ_SPLIT_BF16])
+@pytest.mark.parametrize("quirks", ["tracking", "default", "reference"])
+def test_icp_teacher_forced(jtj, quirks):
+    w = small_workload(6, size=128, jtj=jtj, quirks=QUIRKS[quirks])
+    for k in (2, 4):
+        g, o, tg, to = _teacher_forced(w, k, "Track")
+        assert tg == to
+        Pg, Po = g.getPose(), o.getPose()
+        assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 1e-4
+        assert rot_deg(Pg, Po) <= 0.01
+        sg, so = g.getTrackStatus(0), o.getTrackStatus(0)
+        assert np.mean(sg == so) > 0.999
+        rg, ro = g.getReduction(), o.getReduction()
+        assert rg[28] == ro[28]
+        assert abs(g.alignmentEnergy() - o.alignmentEnergy()) <= 1e-3 * o.alignmentEnergy() + 1e-7
+
+
+@pytest.mark.parametrize("quirks", ["tracking", "default"])
+def test_sdf_teacher_forced(quirks):
+    w = small_workload(5, size=128, quirks=QUIRKS[quirks], tracking=L.KF_TRACK_SDF)
+    for k in (2, 3):
+        g, o, tg, to = _teacher_forced(w, k, "TrackSDF")
+        assert tg == to
+        Pg, Po = g.getPose(), o.getPose()
+        assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 1e-4
+        assert rot_deg(Pg, Po) <= 0.01
+
+
+@pytest.mark.parametrize("storage", [L.KF_STORAGE_F32F32, L.KF_STORAGE_F16U16])
+def test_frame_loop_ate_vs_oracle(storage):
+    """kinect.cpp:654-695 free-running on both sides: trajectories within 1 mm ATE."""
+    w = synth.plain_c1(30)
+    w.config.storage = storage
+    g, o = pair(w)
+    for s in (g, o):
+        s.Reset(w.poses[0])
+    pg, po = [], []
+    for k in range(w.n_frames):
+        f = w.frame(k)
+        tg, to = g.frameStep(f), o.frameStep(f)
+        assert tg == to, k
+        pg.append(g.getPose())
+        po.append(o.getPose())
+    assert synth.ate(pg, po) <= 1e-3
+    assert synth.ate(pg, w.poses) <= 5e-3  # and it actually tracks the ground truth
+
+
+def test_frame_step_graph_matches_step_by_step():
+    """The captured frame graph and the individual entry points compute the same frame."""
+    w = small_workload(4, size=64)
+    a, b = GFusion(w.config, w.intrinsics), GFusion(w.config, w.intrinsics)
+    for s in (a, b):
+        s.Reset(w.poses[0])
+    counter = 0
+    reset = True
+    for k in range(4):
+        f = w.frame(k)
+        ta = a.frameStep(f)
+        b.depthToVertex(f)
+        b.vertexToNormal()
+        tb = b.Track()
+        if tb or reset:
+            b.integrate()
+            if counter > 2:
+                reset = False
+        if not tb:
+            b.recoverPose()
+        counter += 1
+        b.raycast()
+        assert ta == tb
+        np.testing.assert_array_equal(a.getPose(), b.getPose())
+    np.testing.assert_array_equal(a.getVolumeRaw(), b.getVolumeRaw())
+    np.testing.assert_array_equal(a.getVerts(), b.getVerts())
+
+
+def test_pose_library_and_recover():
+    w = small_workload(8, size=64)
+    g, o = pair(w)
+    for s in (g, o):
+        s.Reset(w.poses[0])
+    for k in range(6):
+        f = w.frame(k)
+        assert g.frameStep(f) == o.frameStep(f)
+    assert g.poseLibrarySize() == o.poseLibrarySize() >= 1
+    # an empty frame cannot track (AE == 0): both recover from the library the same way
+    z = np.zeros((424, 512), np.uint16)
+    assert g.frameStep(z) is False and o.frameStep(z) is False
+    Pg, Po = g.getPose(), o.getPose()
+    assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 1e-4
+
+
+def test_errors_are_reported():
+    w = small_workload(1, size=32)
+    g = GFusion(w.config, w.intrinsics)
+    with pytest.raises(ValueError):
+        g.depthToVertex(np.zeros((10, 10), np.uint16))
+    with pytest.raises(L.KfError) as e:
+        g.setVolumeRaw(np.zeros(7, np.uint8))
+    assert e.value.status == L.KF_ERR_INVALID_ARGUMENT
