@@ -18,6 +18,7 @@ this host's cores for the same workload.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import subprocess
@@ -89,12 +90,16 @@ class ClockSampler:
             N.nvmlInit()
             self.N = N
             import torch
-            bus = torch.cuda.get_device_properties(device_index).pci_bus_id if hasattr(
-                torch.cuda.get_device_properties(device_index), "pci_bus_id") else None
-            if bus:
-                self._h = N.nvmlDeviceGetHandleByPciBusId(bus.encode() if isinstance(bus, str) else bus)
-            else:
-                self._h = N.nvmlDeviceGetHandleByIndex(int(os.environ.get("LOCAL_RANK", device_index)))
+            props = torch.cuda.get_device_properties(device_index)
+            uuid = getattr(props, "uuid", None)
+            self._h = None
+            if uuid is not None:
+                try:
+                    self._h = N.nvmlDeviceGetHandleByUUID(("GPU-" + str(uuid)).encode())
+                except Exception:
+                    self._h = None
+            if self._h is None:
+                self._h = N.nvmlDeviceGetHandleByIndex(0)
             self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self._h, N.NVML_CLOCK_SM)
         except Exception as e:  # NVML unavailable: report what we could not sample
             self.error = str(e)
@@ -209,7 +214,12 @@ def run_reference(args):
     return 0
 
 
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def main():
+    faulthandler.enable()
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
@@ -221,7 +231,9 @@ def main():
     n_frames = W + K + n_e2e + 1
     w = workload(args, n_frames)
     ncpu = os.cpu_count() or 1
+    log(f"rendering {n_frames} frames")
     frames = gen_frames(w, range(n_frames), max(1, min(16, ncpu // max(1, world))))
+    log("frames ready")
 
     import torch
     torch.cuda.set_device(local)
@@ -233,6 +245,7 @@ def main():
 
     g = GFusion(w.config, w.intrinsics)
     g.Reset(w.poses[0])
+    log("session created")
     mc = MCubes(g)
     stream = torch.cuda.ExternalStream(g.stream())
     stack = np.stack([frames[i] for i in range(n_frames)]).view(np.int16)
@@ -253,6 +266,7 @@ def main():
     for i in range(W):
         g.frameStepDevice(base + i * fbytes, sync=False)
     torch.cuda.synchronize()
+    log("warm-up done")
     if world > 1:
         dist.barrier()
     g.resetStageStats()
@@ -267,6 +281,7 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
     dev_ms = ev0.elapsed_time(ev1)
+    log(f"timed pass {dev_ms:.1f} ms")
     launches = g.launchCount() - launches0
     stage_mean, stage_frames = g.stageStats()
     tracked_ok = g.frameStepDevice(base + (W + K) * fbytes)  # a synchronised step: state readable
@@ -294,6 +309,7 @@ def main():
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         e2e_ms = e0.elapsed_time(e1)
+        log(f"e2e pass {e2e_ms:.1f} ms")
         e2e = {"ms": e2e_ms, "wall_s": wall}
 
     # max over ranks of the timed durations
@@ -337,6 +353,7 @@ def main():
                           "wall_frames_per_s": n_e2e / e2e["wall_s"]}
     g.close()
     if rank == 0 and not args.no_cpu_baseline and world == 1:
+        log("cpu baseline")
         out["cpu_baseline"] = cpu_baseline(args, w, frames)
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -180,26 +180,27 @@ int record(kf_session* s, int i) {
 }
 
 // The device part of one frame of kinect.cpp:654-695 (input already in d_depth_u16),
-// with stage events ev[0..5]: start, pyramid, track, integrate, recover, raycast.
+// with stage events ev[0..5]: start, pyramid, track, integrate, recover, raycast (event
+// record nodes in the captured graph, so they can be timed after every replay).
 int enqueue_frame(kf_session* s, cudaEvent_t* ev) {
   int rc;
-  KF_CUDA_TRY(s, cudaEventRecord(ev[0], s->stream));
+  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[0], s->stream, cudaEventRecordExternal));
   if ((rc = kf_launch_pyramid(s, s->d_depth_u16, nullptr))) return rc;
   if ((rc = kf_launch_vertex_normal(s))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecord(ev[1], s->stream));
+  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[1], s->stream, cudaEventRecordExternal));
   if (s->cfg.tracking == KF_TRACK_SDF) {
     if ((rc = kf_launch_sdf(s, 0, 0, 1))) return rc;
     if ((rc = kf_launch_sdf_policy(s))) return rc;
   } else {
     if ((rc = kf_launch_icp(s, 1))) return rc;
   }
-  KF_CUDA_TRY(s, cudaEventRecord(ev[2], s->stream));
+  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[2], s->stream, cudaEventRecordExternal));
   if ((rc = kf_launch_integrate(s, 1))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecord(ev[3], s->stream));
+  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[3], s->stream, cudaEventRecordExternal));
   if ((rc = kf_launch_sdf(s, 1, 1, 0))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecord(ev[4], s->stream));
+  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[4], s->stream, cudaEventRecordExternal));
   if ((rc = kf_launch_raycast(s))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecord(ev[5], s->stream));
+  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[5], s->stream, cudaEventRecordExternal));
   return KF_OK;
 }
 
@@ -446,6 +447,7 @@ int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out)
   std::memcpy(s->h_state->pose_eig, kIdentity, sizeof(kIdentity));
   std::memcpy(s->h_state->old_pose, kIdentity, sizeof(kIdentity));
   std::memcpy(s->h_state->raycast_pose, kIdentity, sizeof(kIdentity));
+  s->h_state->icp_center_cam[2] = 1.0;  // first ICP centre: 1 m in front of the camera
   s->h_state->reset_window = 1;
   if ((rc = push_state(s))) return bail(rc);
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return bail(KF_ERR_CUDA);

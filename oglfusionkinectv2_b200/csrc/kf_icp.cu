@@ -12,11 +12,19 @@
 // and releases the others.  No host round trip per iteration (the reference maps the
 // SSBO back every iteration, :1131-1134), no launch per iteration, deterministic sums.
 //
-// J^T J contraction: KF_JTJ_FP32 uses FMAs; KF_JTJ_SPLIT_BF16 stages each warp's 32
-// feature rows f = [J0..J5, e, 0] as bf16 hi + lo pairs and issues
-// mma.sync.m16n8k16 (A = [hi; lo]^T rows, B = hi then lo) so that the FP32 accumulator
-// holds sum (hi+lo)(hi+lo)^T: every bf16 x bf16 product is exact in FP32, the only
-// rounding is the 2^-16 split of each feature and the FP32 accumulation.
+// Conditioning: J = [n, p x n] with world p couples rotation and translation strongly
+// (lever arms of metres), so FP32 partial sums lose the small eigen-directions of J^T J.
+// The sums are therefore accumulated with the lever arm taken about a centre c (the
+// previous iteration's centroid of the valid points): J' = [n, (p - c) x n].  That is an
+// exact change of variables: J = M J' with M = [[I, 0], [[c]x, I]], so the world system
+// is C = M C' M^T, b = M b', and its solution is t = t' - w x c for the same w.  The
+// reported reduction row is the world form, as the reference's.
+//
+// J^T J contraction: KF_JTJ_FP32 uses FMAs; KF_JTJ_SPLIT_BF16 splits each feature of
+// f = [J'0..J'5, e, 0] into three bf16 terms (hi + mid + lo, 24 significant bits), stages
+// them feature-major per warp, and issues four mma.sync.m16n8k16 per 16 pixels
+// ([hi; mid] x hi, x mid, x lo, and [lo; 0] x hi) with FP32 accumulation: every bf16 x
+// bf16 product is exact in FP32 and only the lo*mid and lo*lo terms (~2^-24) are left out.
 #include "kf_internal.cuh"
 
 namespace {
@@ -42,7 +50,8 @@ struct IcpArgs {
 
 // ---- track.cs:53-133 for one pixel ------------------------------------------------------
 __device__ __forceinline__ int track_pixel(const IcpArgs& a, int l, int x, int y,
-                                           const float* T, const float* V, float* f) {
+                                           const float* T, const float* V, const float* c,
+                                           float* f, float* pw) {
   const size_t i = (size_t)y * a.W[l] + x;
   const float4 n = __ldg(&a.normal[l][i]);
   if (n.x == 2.0f) return -1;
@@ -75,10 +84,15 @@ __device__ __forceinline__ int track_pixel(const IcpArgs& a, int l, int x, int y
   f[0] = rn.x;
   f[1] = rn.y;
   f[2] = rn.z;
-  f[3] = pvy * rn.z - pvz * rn.y;  // cross(projectedVertex, referenceNormal)
-  f[4] = pvz * rn.x - pvx * rn.z;
-  f[5] = pvx * rn.y - pvy * rn.x;
+  // cross(projectedVertex - c, referenceNormal): the reference's p x n about centre c
+  const float qx = pvx - c[0], qy = pvy - c[1], qz = pvz - c[2];
+  f[3] = qy * rn.z - qz * rn.y;
+  f[4] = qz * rn.x - qx * rn.z;
+  f[5] = qx * rn.y - qy * rn.x;
   f[6] = rn.x * dx + rn.y * dy + rn.z * dz;  // dot(referenceNormal, diff)
+  pw[0] = pvx;
+  pw[1] = pvy;
+  pw[2] = pvz;
   return 1;
 }
 
@@ -113,13 +127,16 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
   __shared__ double s_pose[16];
   __shared__ double s_old[16];
   __shared__ double s_ray[16];
-  __shared__ float s_T[16], s_V[16];
+  __shared__ double s_cd[3];
+  __shared__ float s_T[16], s_V[16], s_c[3];
   __shared__ float s_warp[kWarps][64];
+  __shared__ float s_pw[kWarps][4];
   __shared__ double s_red[kWarps][32];
   __shared__ double s_sums[32];
   __shared__ unsigned s_gen;
   __shared__ int s_last, s_flag, s_conv;
   __shared__ __align__(16) __nv_bfloat16 s_hi[JTJ ? kWarps : 1][8][40];
+  __shared__ __align__(16) __nv_bfloat16 s_mid[JTJ ? kWarps : 1][8][40];
   __shared__ __align__(16) __nv_bfloat16 s_lo[JTJ ? kWarps : 1][8][40];
 
   KfDevState* st = a.st;
@@ -132,7 +149,15 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
     s_ray[tid] = st->raycast_pose[tid];
   }
   __syncthreads();
-  if (tid == 0) make_float_mats(a, s_pose, s_ray, s_T, s_V);
+  if (tid == 0) {
+    make_float_mats(a, s_pose, s_ray, s_T, s_V);
+    // first centre: last frame's centroid, carried in the camera frame
+    const double* cc = st->icp_center_cam;
+    for (int r = 0; r < 3; ++r) {
+      s_cd[r] = s_pose[r] * cc[0] + s_pose[4 + r] * cc[1] + s_pose[8 + r] * cc[2] + s_pose[12 + r];
+      s_c[r] = (float)s_cd[r];
+    }
+  }
   __syncthreads();
 
   bool ok = true;
@@ -141,26 +166,35 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
     const int Wl = a.W[level], Hl = a.H[level];
     const int P = Wl * Hl;
     for (int it = 0; it < a.iters[level]; ++it) {
-      float T[16], V[16];
+      float T[16], V[16], c[3];
 #pragma unroll
       for (int k = 0; k < 16; ++k) { T[k] = s_T[k]; V[k] = s_V[k]; }
+      c[0] = s_c[0]; c[1] = s_c[1]; c[2] = s_c[2];
 
       // ---------------- track + accumulate ----------------
       float acc[JTJ ? 4 : 28];
 #pragma unroll
       for (int k = 0; k < (JTJ ? 4 : 28); ++k) acc[k] = 0.0f;
+      float pacc[4] = {0.f, 0.f, 0.f, 0.f};  // valid count, sum of world points
       const int stride = nb * KF_TRACK_THREADS;
       for (int base = (blockIdx.x * kWarps + warp) * 32; base < P; base += stride) {
         const int i = base + lane;
         float f[7] = {0, 0, 0, 0, 0, 0, 0};
+        float pw[3] = {0, 0, 0};
         int status = 0;
         if (i < P) {
           const int y = i / Wl, x = i - y * Wl;
-          status = track_pixel(a, level, x, y, T, V, f);
+          status = track_pixel(a, level, x, y, T, V, c, f, pw);
           a.status[level][i] = status;
           if (a.q1 && (y & 7) != 7) status = 0;  // only work group 7 reaches the solver
         }
         const bool use = status == 1;
+        if (use) {
+          pacc[0] += 1.0f;
+          pacc[1] += pw[0];
+          pacc[2] += pw[1];
+          pacc[3] += pw[2];
+        }
         if constexpr (JTJ == 0) {
           if (use) {
             const float e = f[6];
@@ -171,16 +205,19 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
 #pragma unroll
             for (int r = 0; r < 6; ++r)
 #pragma unroll
-              for (int c = r; c < 6; ++c) acc[q++] += f[r] * f[c];
+              for (int cc = r; cc < 6; ++cc) acc[q++] += f[r] * f[cc];
           }
         } else {
-          // stage f = [J0..J5, e, 0] as hi/lo bf16, feature-major per warp
+          // stage f = [J'0..J'5, e, 0] as hi + mid + lo bf16, feature-major per warp
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
             const float v = (use && k < 7) ? f[k] : 0.0f;
             const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-            const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+            const float r1 = v - __bfloat162float(hi);
+            const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+            const __nv_bfloat16 lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
             s_hi[warp][k][lane] = hi;
+            s_mid[warp][k][lane] = mid;
             s_lo[warp][k][lane] = lo;
           }
           __syncwarp();
@@ -188,18 +225,30 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int c0 = 16 * h + 2 * t;
-            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&s_hi[warp][g][c0]);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&s_lo[warp][g][c0]);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&s_hi[warp][g][c0 + 8]);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&s_lo[warp][g][c0 + 8]);
-            mma_bf16_16816(acc, a0, a1, a2, a3, a0, a2);  // x B = hi
-            mma_bf16_16816(acc, a0, a1, a2, a3, a1, a3);  // x B = lo
+            const uint32_t h0 = *reinterpret_cast<const uint32_t*>(&s_hi[warp][g][c0]);
+            const uint32_t h1 = *reinterpret_cast<const uint32_t*>(&s_hi[warp][g][c0 + 8]);
+            const uint32_t m0 = *reinterpret_cast<const uint32_t*>(&s_mid[warp][g][c0]);
+            const uint32_t m1 = *reinterpret_cast<const uint32_t*>(&s_mid[warp][g][c0 + 8]);
+            const uint32_t l0 = *reinterpret_cast<const uint32_t*>(&s_lo[warp][g][c0]);
+            const uint32_t l1 = *reinterpret_cast<const uint32_t*>(&s_lo[warp][g][c0 + 8]);
+            // A = [hi; mid] (rows g, g+8); B columns = features of 16 pixels
+            mma_bf16_16816(acc, h0, m0, h1, m1, h0, h1);  // x hi
+            mma_bf16_16816(acc, h0, m0, h1, m1, m0, m1);  // x mid
+            mma_bf16_16816(acc, h0, m0, h1, m1, l0, l1);  // x lo
+            mma_bf16_16816(acc, l0, 0u, l1, 0u, h0, h1);  // [lo; 0] x hi
           }
           __syncwarp();
         }
       }
 
-      // ---------------- block partial ----------------
+      // ---------------- block partial: 28 sums + valid count + point sum --------------
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        float v = pacc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s_pw[warp][k] = v;
+      }
       if constexpr (JTJ == 0) {
 #pragma unroll
         for (int k = 0; k < 28; ++k) {
@@ -216,26 +265,32 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
           a.partials[(size_t)blockIdx.x * 32 + tid] = v;
         }
       } else {
-        // lane (g, t) holds M[g][2t], M[g][2t+1] as rows g (hi) + g+8 (lo) of the mma
+        // lane (g, t) holds M[g][2t], M[g][2t+1] as rows g + g+8 of the accumulator
         const int g = lane >> 2, t = lane & 3;
         s_warp[warp][g * 8 + 2 * t] = acc[0] + acc[2];
         s_warp[warp][g * 8 + 2 * t + 1] = acc[1] + acc[3];
         __syncthreads();
         if (tid < 28) {
-          int r, c;
-          if (tid == 0) { r = 6; c = 6; }
-          else if (tid < 7) { r = tid - 1; c = 6; }
+          int r, cc;
+          if (tid == 0) { r = 6; cc = 6; }
+          else if (tid < 7) { r = tid - 1; cc = 6; }
           else {
             int q = tid - 7;
             r = 0;
             while (q >= 6 - r) { q -= 6 - r; ++r; }
-            c = r + q;
+            cc = r + q;
           }
           float v = 0.0f;
 #pragma unroll
-          for (int w = 0; w < kWarps; ++w) v += s_warp[w][r * 8 + c];
+          for (int w = 0; w < kWarps; ++w) v += s_warp[w][r * 8 + cc];
           a.partials[(size_t)blockIdx.x * 32 + tid] = v;
         }
+      }
+      if (tid >= 28 && tid < 32) {
+        float v = 0.0f;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) v += s_pw[w][tid - 28];
+        a.partials[(size_t)blockIdx.x * 32 + tid] = v;
       }
 
       // ---------------- hand-over: last block reduces + solves ----------------
@@ -243,8 +298,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
         {
           const int k = tid & 31, r = tid >> 5;
           double v = 0.0;
-          if (k < 28)
-            for (unsigned b = r; b < nb; b += kWarps) v += (double)__ldcg(&a.partials[(size_t)b * 32 + k]);
+          for (unsigned b = r; b < nb; b += kWarps) v += (double)__ldcg(&a.partials[(size_t)b * 32 + k]);
           s_red[r][k] = v;
         }
         __syncthreads();
@@ -258,18 +312,24 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
         if (tid == 0) {
           // reduce.cs counts every pixel of the (group-7) rows in sums[28]
           const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
-          s_sums[28] = count;
-          s_sums[29] = s_sums[30] = s_sums[31] = 0.0;
-          double b[6], C[36], x[6];
-          for (int k = 0; k < 6; ++k) b[k] = s_sums[1 + k];
-          kf_make_jtj(&s_sums[7], C);
+          const double nvalid = s_sums[28];
+          const double cx = s_cd[0], cy = s_cd[1], cz = s_cd[2];
+          double bp[6], Cp[36], xp[6];
+          for (int k = 0; k < 6; ++k) bp[k] = s_sums[1 + k];
+          kf_make_jtj(&s_sums[7], Cp);
           const double ae = sqrt(s_sums[0] / count);  // getReduction :1167
-          kf_cholesky6(C, b, x);
+          kf_cholesky6(Cp, bp, xp);
+          // back to the reference's variables: w = w', t = t' - w x c
+          double x[6];
+          x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
+          x[0] = xp[0] - (x[4] * cz - x[5] * cy);
+          x[1] = xp[1] - (x[5] * cx - x[3] * cz);
+          x[2] = xp[2] - (x[3] * cy - x[4] * cx);
           // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2; pose = delta * pose
           double R[9], D[16], Pn[16];
           kf_euler_xyz(x[3], x[4], x[5], R);
-          for (int c = 0; c < 3; ++c)
-            for (int r = 0; r < 3; ++r) D[c * 4 + r] = R[c * 3 + r];
+          for (int cc = 0; cc < 3; ++cc)
+            for (int r = 0; r < 3; ++r) D[cc * 4 + r] = R[cc * 3 + r];
           D[3] = D[7] = D[11] = 0;
           D[12] = x[0]; D[13] = x[1]; D[14] = x[2]; D[15] = 1;
           kf_mat4_mul(D, s_pose, Pn);
@@ -278,7 +338,46 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
                                   x[4] * x[4] + x[5] * x[5]);
           st->iter_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
           st->ae = ae;
-          for (int k = 0; k < 32; ++k) st->sums[k] = s_sums[k];
+          // the world-form row of the reference: b = M b', C = M C' M^T
+          double Mx[36];
+          for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
+          // rows 3..5, columns 0..2 hold [c]x
+          Mx[3 * 6 + 1] = -cz; Mx[3 * 6 + 2] = cy;
+          Mx[4 * 6 + 0] = cz;  Mx[4 * 6 + 2] = -cx;
+          Mx[5 * 6 + 0] = -cy; Mx[5 * 6 + 1] = cx;
+          double bw[6], MC[36], Cw[36];
+          for (int r = 0; r < 6; ++r) {
+            double v = 0;
+            for (int k = 0; k < 6; ++k) v += Mx[r * 6 + k] * bp[k];
+            bw[r] = v;
+          }
+          for (int r = 0; r < 6; ++r)
+            for (int cc = 0; cc < 6; ++cc) {
+              double v = 0;
+              for (int k = 0; k < 6; ++k) v += Mx[r * 6 + k] * Cp[k * 6 + cc];
+              MC[r * 6 + cc] = v;
+            }
+          for (int r = 0; r < 6; ++r)
+            for (int cc = 0; cc < 6; ++cc) {
+              double v = 0;
+              for (int k = 0; k < 6; ++k) v += MC[r * 6 + k] * Mx[cc * 6 + k];
+              Cw[r * 6 + cc] = v;
+            }
+          st->sums[0] = s_sums[0];
+          for (int k = 0; k < 6; ++k) st->sums[1 + k] = bw[k];
+          int q = 7;
+          for (int r = 0; r < 6; ++r)
+            for (int cc = r; cc < 6; ++cc) st->sums[q++] = Cw[r * 6 + cc];
+          st->sums[28] = count;
+          st->sums[29] = st->sums[30] = st->sums[31] = 0.0;
+          // next centre: this iteration's centroid of the valid points
+          if (nvalid > 0) {
+            st->iter_center[0] = s_sums[29] / nvalid;
+            st->iter_center[1] = s_sums[30] / nvalid;
+            st->iter_center[2] = s_sums[31] / nvalid;
+          } else {
+            st->iter_center[0] = cx; st->iter_center[1] = cy; st->iter_center[2] = cz;
+          }
         }
         kf_grid_release(st);
       } else {
@@ -287,8 +386,12 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
       if (!ok) break;
       if (tid < 16) s_pose[tid] = __ldcg(&st->iter_pose[tid]);
       if (tid == 16) s_conv = __ldcg(&st->iter_conv);
+      if (tid >= 17 && tid < 20) s_cd[tid - 17] = __ldcg(&st->iter_center[tid - 17]);
       __syncthreads();
-      if (tid == 0) make_float_mats(a, s_pose, s_ray, s_T, s_V);
+      if (tid == 0) {
+        make_float_mats(a, s_pose, s_ray, s_T, s_V);
+        for (int r = 0; r < 3; ++r) s_c[r] = (float)s_cd[r];
+      }
       __syncthreads();
       ++iters_run;
       if (s_conv) break;  // result.norm() < 1e-5 && != 0 leaves this level (:707-708)
@@ -316,6 +419,11 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
       for (int k = 0; k < 16; ++k) st->lib_pose[st->lib_size][k] = s_pose[k];
       st->lib_size += 1;
     }
+    // keep the centroid for the next frame, in the camera frame of the tracked pose
+    double inv[16];
+    kf_rigid_inverse(s_pose, inv);
+    for (int r = 0; r < 3; ++r)
+      st->icp_center_cam[r] = inv[r] * s_cd[0] + inv[4 + r] * s_cd[1] + inv[8 + r] * s_cd[2] + inv[12 + r];
   }
   for (int k = 0; k < 16; ++k) st->old_pose[k] = s_old[k];
   st->tracked = tracked;

@@ -50,6 +50,8 @@ struct KfDevState {
   // hand-over between iterations of the persistent tracking kernels
   double iter_pose[16]; // pose after the last solve (ICP) / camera-to-world (SDF)
   double iter_result[6];// SDF twist accumulator
+  double iter_center[3];// ICP accumulation centre for the next iteration (world)
+  double icp_center_cam[3];  // ICP centre at the end of the last frame (camera frame)
   int iter_conv;        // convergence flag of the last solve
   int pad_[3];
   double lib_pose[KF_MAX_LIBRARY][16];  // pose library

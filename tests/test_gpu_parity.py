@@ -197,7 +197,9 @@ def test_frame_step_graph_matches_step_by_step():
 
 
 def test_pose_library_and_recover():
-    w = small_workload(8, size=64)
+    """Tracking failure (a frame 0.25 m away: every pixel fails the distance gate, AE == 0)
+    sends both sides through recoverPose (TrackSDF from the pose library)."""
+    w = small_workload(30, size=64)
     g, o = pair(w)
     for s in (g, o):
         s.Reset(w.poses[0])
@@ -205,11 +207,11 @@ def test_pose_library_and_recover():
         f = w.frame(k)
         assert g.frameStep(f) == o.frameStep(f)
     assert g.poseLibrarySize() == o.poseLibrarySize() >= 1
-    # an empty frame cannot track (AE == 0): both recover from the library the same way
-    z = np.zeros((424, 512), np.uint16)
-    assert g.frameStep(z) is False and o.frameStep(z) is False
+    far = w.frame(26)
+    tg, to = g.frameStep(far), o.frameStep(far)
+    assert tg is False and to is False
     Pg, Po = g.getPose(), o.getPose()
-    assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 1e-4
+    assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 5e-4
 
 
 def test_errors_are_reported():
