@@ -305,6 +305,7 @@ def main():
             st = lib.kf_frame_step_u16(g.handle, C.c_void_p(hp + i * fbytes), C.byref(t))
             if st:
                 raise L.KfError(st, "kf_frame_step_u16")
+            maybe_mc(i)
         e1.record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0

@@ -188,6 +188,8 @@ KF_API int kf_recover_pose(kf_session* s, int* found);
 /* Alignment energy and the 32-float reduction row of the last ICP / SDF iteration
  * (getReduction / getSDFReduction, gFusion.cpp:1127-1168, 1195-1232). */
 KF_API int kf_get_alignment_energy(kf_session* s, float* ae);
+/* Gauss-Newton iterations the last Track()/TrackSDF() executed (early exits included). */
+KF_API int kf_get_iterations_run(kf_session* s, int* iterations);
 KF_API int kf_get_reduction(kf_session* s, float sums[32]);
 
 /* ---- volume ------------------------------------------------------------------------- */

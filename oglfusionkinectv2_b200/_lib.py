@@ -110,6 +110,7 @@ SIGNATURES = {
     "kf_recover_pose": (_I, [_P, C.POINTER(_I)]),
     "kf_get_alignment_energy": (_I, [_P, _PF]),
     "kf_get_reduction": (_I, [_P, _PF]),
+    "kf_get_iterations_run": (_I, [_P, C.POINTER(_I)]),
     "kf_integrate": (_I, [_P]),
     "kf_raycast": (_I, [_P]),
     "kf_frame_step_u16": (_I, [_P, _P, C.POINTER(_I)]),

@@ -64,6 +64,8 @@ void free_mc(kf_session* s) {
   s->d_mc_base = nullptr;
   for (uint32_t* p : s->d_mc_levels) cudaFree(p);
   s->d_mc_levels.clear();
+  s->mc_P = 0;
+  s->mc_top = 0;
   cudaFree(s->d_mc_vertices);
   s->d_mc_vertices = nullptr;
   s->mc_vertex_cap = 0;
@@ -601,6 +603,14 @@ int kf_get_alignment_energy(kf_session* s, float* ae) {
   int rc = pull_state(s);
   if (rc) return rc;
   *ae = (float)s->h_state->ae;
+  return KF_OK;
+}
+
+int kf_get_iterations_run(kf_session* s, int* iterations) {
+  if (!s || !iterations) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  *iterations = s->h_state->iterations_run;
   return KF_OK;
 }
 

@@ -118,8 +118,8 @@ struct kf_session {
   size_t mc_vertex_cap = 0;
   uint32_t mc_triangles = 0;
   int mc_valid = 0;
-  uint32_t* d_mc_scratch = nullptr;  // scan path: verts, offsets, cube index
-  size_t mc_scratch_words = 0;
+  uint32_t* d_mc_scratch = nullptr;  // level table / scan path verts, offsets, scan scratch
+  size_t mc_scratch_words = 0;       // capacity of d_mc_scratch in bytes
   uint32_t* d_u32_scalar = nullptr;  // one device word for totals
   uint32_t* h_u32_scalar = nullptr;  // pinned
 };

@@ -277,6 +277,11 @@ class GFusion:
         self._check(self.lib.kf_get_alignment_energy(self._h, C.byref(f)), "kf_get_alignment_energy")
         return f.value
 
+    def iterationsRun(self) -> int:
+        n = C.c_int()
+        self._check(self.lib.kf_get_iterations_run(self._h, C.byref(n)), "kf_get_iterations_run")
+        return n.value
+
     def getReduction(self) -> np.ndarray:
         a = (C.c_float * 32)()
         self._check(self.lib.kf_get_reduction(self._h, a), "kf_get_reduction")

@@ -7,7 +7,7 @@ from oglfusionkinectv2_b200 import GFusionConfig, Intrinsics, synth, _lib as L
 
 
 def small_workload(n_frames=12, size=64, storage=L.KF_STORAGE_F32F32, quirks=None,
-                   jtj=L.KF_JTJ_FP32, tracking=L.KF_TRACK_ICP, seed=0xC0FFEE + 11):
+                   jtj=L.KF_JTJ_FP32, tracking=L.KF_TRACK_ICP, seed=0xC0FFEE + 1):
     """C1-like scene (plane + 3 spheres, 1.5 m cube) at a small volume size."""
     w = synth.plain_c1(n_frames, seed=seed)
     c = w.config

@@ -197,9 +197,10 @@ def test_frame_step_graph_matches_step_by_step():
 
 
 def test_pose_library_and_recover():
-    """Tracking failure (a frame 0.25 m away: every pixel fails the distance gate, AE == 0)
-    sends both sides through recoverPose (TrackSDF from the pose library)."""
-    w = small_workload(30, size=64)
+    """A frame whose every pixel fails the ICP distance gate (a flat wall at 4.2 m, outside
+    the volume) is not tracked (AE == 0); both sides then run recoverPose (TrackSDF from
+    each pose of the library) and end on the same pose."""
+    w = small_workload(8, size=64)
     g, o = pair(w)
     for s in (g, o):
         s.Reset(w.poses[0])
@@ -207,11 +208,12 @@ def test_pose_library_and_recover():
         f = w.frame(k)
         assert g.frameStep(f) == o.frameStep(f)
     assert g.poseLibrarySize() == o.poseLibrarySize() >= 1
-    far = w.frame(26)
-    tg, to = g.frameStep(far), o.frameStep(far)
+    wall = np.full((424, 512), 4200, np.uint16)
+    tg, to = g.frameStep(wall), o.frameStep(wall)
     assert tg is False and to is False
     Pg, Po = g.getPose(), o.getPose()
-    assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 5e-4
+    # the library holds each side's own tracked poses (within the 1 mm trajectory bound)
+    assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 1e-3
 
 
 def test_errors_are_reported():
