@@ -241,6 +241,24 @@ KF_API int kf_mc_export_ply(kf_session* s, const char* path);  /* exportPointClo
 KF_API int kf_prefix_sum_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* total,
                       void* cuda_stream);
 
+/* Allocation-free prefix sum.  No counterpart in the reference: it exists for callers that
+ * must not allocate device memory, such as a frame loop running under a fixed memory
+ * budget or inside a host framework that owns every device allocation, where the
+ * cudaMalloc of kf_prefix_sum_u32's scratch is not allowed.  Same result as
+ * kf_prefix_sum_u32; the scratch is a 262,220-byte array compiled into the library,
+ * which every GPU that loads the library keeps until the process exits.
+ *   - n may be at most 2^28 (268,435,456) elements; larger n returns KF_ERR_CAPACITY.
+ *   - The first call on a device looks up the array's device address (a host-side step,
+ *     done once per device with that device current); make that first call before any
+ *     stream capture on the device.
+ *   - All calls on a device share the one array: calls whose work overlaps on the GPU
+ *     (different streams, or host threads) race and corrupt each other's results.
+ *     Serialise them, e.g. on one stream.
+ *   - No cudaMalloc/cudaFree or allocating library call is made; if total is not NULL the
+ *     call copies it back and synchronises the stream. */
+KF_API int kf_prefix_sum_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, uint64_t n,
+                                     uint32_t* total, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -136,6 +136,7 @@ SIGNATURES = {
     "kf_mc_export_stl": (_I, [_P, C.c_char_p]),
     "kf_mc_export_ply": (_I, [_P, C.c_char_p]),
     "kf_prefix_sum_u32": (_I, [_P, _P, C.c_uint64, C.POINTER(C.c_uint32), _P]),
+    "kf_prefix_sum_u32_noalloc": (_I, [_P, _P, C.c_uint64, C.POINTER(C.c_uint32), _P]),
 }
 
 _lib = None

@@ -12,6 +12,8 @@
 // the 256 thread totals.  Tile totals go to a scratch array that is scanned by the same
 // code recursively (4096^2 = 16.7M elements per level), then added back.  There is no
 // inter-block waiting.
+#include <mutex>
+
 #include "kf_internal.cuh"
 
 namespace {
@@ -170,4 +172,67 @@ extern "C" int kf_prefix_sum_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t
   if (cudaStreamSynchronize(st) != cudaSuccess) rc = KF_ERR_CUDA;
   if (!rc && total) *total = h;
   return rc;
+}
+
+// ---- allocation-free variant -----------------------------------------------------------
+// Scratch for kf_prefix_sum_u32_noalloc: the tile totals of every scan level plus one
+// word for the grand total, for inputs of up to KF_NOALLOC_SCAN_MAX_ELEMENTS elements
+// (2^28 elements need 65,536 + 16 tile totals + 1 spare + 1 grand total = 65,554 words;
+// the array holds 65,555 words, 262,220 bytes).
+// Every GPU that loads this library holds the array until the process exits.
+#define KF_NOALLOC_SCAN_MAX_ELEMENTS (1ull << 28)
+#define KF_NOALLOC_SCAN_WORDS 65555
+static __device__ __align__(256) uint32_t g_noalloc_scan_scratch[KF_NOALLOC_SCAN_WORDS];
+
+namespace {
+std::mutex g_noalloc_mu;
+constexpr int kNoallocMaxDevices = 256;
+uint32_t* g_noalloc_ptr[kNoallocMaxDevices] = {};  // device address of the array, per device
+}  // namespace
+
+// In host code g_noalloc_scan_scratch only names the symbol; its device address is looked
+// up once per device (with that device current) and cached.
+static int noalloc_scratch(uint32_t** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
+    cudaGetLastError();
+    return KF_ERR_NO_DEVICE;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return KF_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<uint32_t*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return KF_OK;
+}
+
+extern "C" int kf_prefix_sum_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* total,
+                                         void* cuda_stream) {
+  if ((!d_in || !d_out) && n) return KF_ERR_INVALID_ARGUMENT;
+  if (n > KF_NOALLOC_SCAN_MAX_ELEMENTS) return KF_ERR_CAPACITY;
+  const size_t words = kf_scan_scratch_words(n);
+  if (words + 1 > KF_NOALLOC_SCAN_WORDS) return KF_ERR_CAPACITY;
+  uint32_t* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  // nothing in the scratch has to start at zero: every tile total and the grand total are
+  // written before they are read
+  uint32_t* d_total = scratch + words;
+  rc = kf_scan_u32(d_in, d_out, n, d_total, st, scratch, words);
+  if (rc || !total) return rc;
+  uint32_t h = 0;
+  if (cudaMemcpyAsync(&h, d_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaGetLastError();
+    return KF_ERR_CUDA;
+  }
+  *total = h;
+  return KF_OK;
 }
