@@ -134,7 +134,10 @@ typedef struct kf_intrinsics {
  * The volume is two planes: nx*ny*nz TSDF values (x fastest), then as many weights.
  * F32F32: float + float; F16U16: IEEE half + uint16; RG16I: int16 (TSDF*32766) + int16. */
 typedef struct kf_volume_view {
-  void* device_ptr;            /* value plane; valid until kf_reset(.., 1) or kf_destroy */
+  void* device_ptr;            /* value plane, for reading; valid until kf_reset(.., 1)  */
+                               /* or kf_destroy.  New contents go in through            */
+                               /* kf_copy_volume_from_host, which also refreshes the    */
+                               /* per-8^3-brick summary that kf_raycast skips by.       */
   int32_t nx, ny, nz;
   int32_t storage;             /* KF_STORAGE_*                                           */
   int64_t value_bytes;         /* bytes per value (and per weight): 4 or 2              */

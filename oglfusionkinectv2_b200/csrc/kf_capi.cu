@@ -41,6 +41,8 @@ int validate(const kf_config* c, const kf_intrinsics* in) {
   if (!c || !in) return KF_ERR_INVALID_ARGUMENT;
   if (c->nx < 4 || c->ny < 4 || c->nz < 4 || c->nx > 4096 || c->ny > 4096 || c->nz > 4096)
     return KF_ERR_INVALID_ARGUMENT;
+  // kernels index a volume plane with 32-bit offsets
+  if ((uint64_t)c->nx * (uint64_t)c->ny * (uint64_t)c->nz >= (1ull << 31)) return KF_ERR_INVALID_ARGUMENT;
   if (!(c->dim_x > 0) || !(c->dim_y > 0) || !(c->dim_z > 0) || !(c->mu > 0)) return KF_ERR_INVALID_ARGUMENT;
   if (!(c->max_weight > 0) || !(c->far_plane > c->near_plane)) return KF_ERR_INVALID_ARGUMENT;
   if (c->storage < KF_STORAGE_F32F32 || c->storage > KF_STORAGE_RG16I) return KF_ERR_INVALID_ARGUMENT;
@@ -89,6 +91,7 @@ void free_all(kf_session* s) {
   drop_graph(s);
   free_mc(s);
   cudaFree(s->d_vol);
+  cudaFree(s->d_bricks);
   cudaFree(s->d_depth_u16);
   cudaFree(s->d_depth_f32_in);
   for (int l = 0; l < 3; ++l) {
@@ -146,7 +149,7 @@ int push_state(kf_session* s) {
 }
 
 void set_pose_fields(kf_session* s, const double* pose, bool reset_eig) {
-  std::memcpy(s->h_state->pose, pose, 16 * sizeof(double));
+  kf_store_pose(s->h_state, pose);
   if (reset_eig) {
     // resetPose (gFusion.cpp:275-287)
     if (s->cfg.quirks & KF_Q19_EIG_TRANSLATION) {
@@ -164,6 +167,17 @@ void set_pose_fields(kf_session* s, const double* pose, bool reset_eig) {
 int alloc_volume(kf_session* s) {
   cudaFree(s->d_vol);
   s->d_vol = nullptr;
+  cudaFree(s->d_bricks);
+  s->d_bricks = nullptr;
+  s->bx = (s->cfg.nx + KF_BRICK - 1) / KF_BRICK;
+  s->by = (s->cfg.ny + KF_BRICK - 1) / KF_BRICK;
+  s->bz = (s->cfg.nz + KF_BRICK - 1) / KF_BRICK;
+  {
+    const size_t nb = (size_t)s->bx * s->by * s->bz;
+    int rc = dalloc(s, &s->d_bricks, nb);
+    if (rc) return rc;
+    KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, nb * 4, s->stream));
+  }
   s->vol_count = (size_t)s->cfg.nx * s->cfg.ny * s->cfg.nz;
   s->vol_value_bytes = value_bytes(s->cfg.storage);
   s->vol_bytes = s->vol_count * s->vol_value_bytes * 2;
@@ -378,6 +392,8 @@ int kf_session_device_bytes(const kf_config* cfg, const kf_intrinsics* in, uint6
   const uint64_t vox = (uint64_t)cfg->nx * cfg->ny * cfg->nz;
   const uint64_t px = (uint64_t)in->width * in->height;
   uint64_t b = vox * value_bytes(cfg->storage) * 2;
+  b += (uint64_t)((cfg->nx + KF_BRICK - 1) / KF_BRICK) * ((cfg->ny + KF_BRICK - 1) / KF_BRICK) *
+       ((cfg->nz + KF_BRICK - 1) / KF_BRICK) * 4;  // brick flags
   b += px * (2 + 4);                       // staging
   b += px * (4 + 16 + 16 + 4) * 2;         // three levels (sum < 4/3 of level 0)
   b += px * 32;                            // raycast maps
@@ -445,7 +461,7 @@ int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out)
   if (cudaMallocHost((void**)&s->h_depth_pinned, px * 2) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
   if (cudaMallocHost((void**)&s->h_u32_scalar, 16) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
   std::memset(s->h_state, 0, sizeof(KfDevState));
-  std::memcpy(s->h_state->pose, kIdentity, sizeof(kIdentity));
+  kf_store_pose(s->h_state, kIdentity);
   std::memcpy(s->h_state->pose_eig, kIdentity, sizeof(kIdentity));
   std::memcpy(s->h_state->old_pose, kIdentity, sizeof(kIdentity));
   std::memcpy(s->h_state->raycast_pose, kIdentity, sizeof(kIdentity));
@@ -475,6 +491,7 @@ int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
     if ((rc = alloc_volume(s))) return rc;
   } else {
     KF_CUDA_TRY(s, cudaMemsetAsync(s->d_vol, 0, s->vol_bytes, s->stream));
+    KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, (size_t)s->bx * s->by * s->bz * 4, s->stream));
   }
   if ((rc = pull_state(s))) return rc;
   s->h_state->lib_size = 0;  // poseLibrary.resize(0)
@@ -494,6 +511,7 @@ int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
 int kf_reset_volume(kf_session* s) {
   if (!s) return KF_ERR_INVALID_ARGUMENT;
   KF_CUDA_TRY(s, cudaMemsetAsync(s->d_vol, 0, s->vol_bytes, s->stream));
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, (size_t)s->bx * s->by * s->bz * 4, s->stream));
   return KF_OK;
 }
 
@@ -711,6 +729,8 @@ int kf_copy_volume_to_host(kf_session* s, void* dst, uint64_t bytes) {
 int kf_copy_volume_from_host(kf_session* s, const void* src, uint64_t bytes) {
   if (!s || !src || bytes != s->vol_bytes) return KF_ERR_INVALID_ARGUMENT;
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_vol, src, bytes, cudaMemcpyHostToDevice, s->stream));
+  int rc = kf_rebuild_bricks(s);
+  if (rc) return rc;
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return KF_OK;
 }

@@ -123,11 +123,12 @@ __device__ __forceinline__ void make_float_mats(const IcpArgs& a, const double* 
 constexpr int kWarps = KF_TRACK_THREADS / 32;
 
 template <int JTJ>
-__global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
+__global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
   __shared__ double s_pose[16];
   __shared__ double s_old[16];
   __shared__ double s_ray[16];
   __shared__ double s_cd[3];
+  __shared__ double s_D[16];
   __shared__ float s_T[16], s_V[16], s_c[3];
   __shared__ float s_warp[kWarps][64];
   __shared__ float s_pw[kWarps][4];
@@ -325,73 +326,70 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
           x[0] = xp[0] - (x[4] * cz - x[5] * cy);
           x[1] = xp[1] - (x[5] * cx - x[3] * cz);
           x[2] = xp[2] - (x[3] * cy - x[4] * cx);
-          // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2; pose = delta * pose
-          double R[9], D[16], Pn[16];
+          // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2 (gFusion.cpp:700-703)
+          double R[9];
           kf_euler_xyz(x[3], x[4], x[5], R);
           for (int cc = 0; cc < 3; ++cc)
-            for (int r = 0; r < 3; ++r) D[cc * 4 + r] = R[cc * 3 + r];
-          D[3] = D[7] = D[11] = 0;
-          D[12] = x[0]; D[13] = x[1]; D[14] = x[2]; D[15] = 1;
-          kf_mat4_mul(D, s_pose, Pn);
-          for (int k = 0; k < 16; ++k) st->iter_pose[k] = Pn[k];
+            for (int r = 0; r < 3; ++r) s_D[cc * 4 + r] = R[cc * 3 + r];
+          s_D[3] = s_D[7] = s_D[11] = 0;
+          s_D[12] = x[0]; s_D[13] = x[1]; s_D[14] = x[2]; s_D[15] = 1;
           const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] +
                                   x[4] * x[4] + x[5] * x[5]);
-          st->iter_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
+          s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
+          st->iter_conv = s_conv;
           st->ae = ae;
-          // the world-form row of the reference: b = M b', C = M C' M^T
-          double Mx[36];
-          for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
-          // rows 3..5, columns 0..2 hold [c]x
-          Mx[3 * 6 + 1] = -cz; Mx[3 * 6 + 2] = cy;
-          Mx[4 * 6 + 0] = cz;  Mx[4 * 6 + 2] = -cx;
-          Mx[5 * 6 + 0] = -cy; Mx[5 * 6 + 1] = cx;
-          double bw[6], MC[36], Cw[36];
-          for (int r = 0; r < 6; ++r) {
-            double v = 0;
-            for (int k = 0; k < 6; ++k) v += Mx[r * 6 + k] * bp[k];
-            bw[r] = v;
-          }
-          for (int r = 0; r < 6; ++r)
-            for (int cc = 0; cc < 6; ++cc) {
-              double v = 0;
-              for (int k = 0; k < 6; ++k) v += Mx[r * 6 + k] * Cp[k * 6 + cc];
-              MC[r * 6 + cc] = v;
-            }
-          for (int r = 0; r < 6; ++r)
-            for (int cc = 0; cc < 6; ++cc) {
-              double v = 0;
-              for (int k = 0; k < 6; ++k) v += MC[r * 6 + k] * Mx[cc * 6 + k];
-              Cw[r * 6 + cc] = v;
-            }
-          st->sums[0] = s_sums[0];
-          for (int k = 0; k < 6; ++k) st->sums[1 + k] = bw[k];
-          int q = 7;
-          for (int r = 0; r < 6; ++r)
-            for (int cc = r; cc < 6; ++cc) st->sums[q++] = Cw[r * 6 + cc];
-          st->sums[28] = count;
-          st->sums[29] = st->sums[30] = st->sums[31] = 0.0;
+          // the centred row; the tail turns the last one into the reference's world form
+          for (int k = 0; k < 28; ++k) st->iter_csums[k] = s_sums[k];
+          st->iter_csums[28] = count;
+          st->iter_ccenter[0] = cx; st->iter_ccenter[1] = cy; st->iter_ccenter[2] = cz;
           // next centre: this iteration's centroid of the valid points
           if (nvalid > 0) {
-            st->iter_center[0] = s_sums[29] / nvalid;
-            st->iter_center[1] = s_sums[30] / nvalid;
-            st->iter_center[2] = s_sums[31] / nvalid;
-          } else {
-            st->iter_center[0] = cx; st->iter_center[1] = cy; st->iter_center[2] = cz;
+            s_cd[0] = s_sums[29] / nvalid;
+            s_cd[1] = s_sums[30] / nvalid;
+            s_cd[2] = s_sums[31] / nvalid;
           }
+          for (int r = 0; r < 3; ++r) {
+            st->iter_center[r] = s_cd[r];
+            s_c[r] = (float)s_cd[r];
+            st->iter_cf[r] = s_c[r];
+          }
+        }
+        __syncthreads();
+        // pose = delta * pose, one element per thread
+        double pn = 0.0;
+        if (tid < 16) {
+          const int r = tid & 3, cc = tid >> 2;
+          for (int k = 0; k < 4; ++k) pn += s_D[k * 4 + r] * s_pose[cc * 4 + k];
+        }
+        __syncthreads();
+        if (tid < 16) {
+          s_pose[tid] = pn;
+          st->iter_pose[tid] = pn;
+          s_T[tid] = (float)pn;
+          st->iter_T[tid] = s_T[tid];
+        }
+        __syncthreads();
+        if (a.same_pixel && tid == 0) {
+          make_float_mats(a, s_pose, s_ray, s_T, s_V);
+          for (int k = 0; k < 16; ++k) st->iter_V[k] = s_V[k];
         }
         kf_grid_release(st);
       } else {
         ok = kf_grid_wait(st, &s_gen, &s_flag);
+        if (ok) {
+          if (tid < 16) {
+            s_pose[tid] = __ldcg(&st->iter_pose[tid]);
+            s_T[tid] = __ldcg(&st->iter_T[tid]);
+            if (a.same_pixel) s_V[tid] = __ldcg(&st->iter_V[tid]);
+          } else if (tid == 16) {
+            s_conv = __ldcg(&st->iter_conv);
+          } else if (tid < 20) {
+            s_cd[tid - 17] = __ldcg(&st->iter_center[tid - 17]);
+            s_c[tid - 17] = __ldcg(&st->iter_cf[tid - 17]);
+          }
+        }
       }
       if (!ok) break;
-      if (tid < 16) s_pose[tid] = __ldcg(&st->iter_pose[tid]);
-      if (tid == 16) s_conv = __ldcg(&st->iter_conv);
-      if (tid >= 17 && tid < 20) s_cd[tid - 17] = __ldcg(&st->iter_center[tid - 17]);
-      __syncthreads();
-      if (tid == 0) {
-        make_float_mats(a, s_pose, s_ray, s_T, s_V);
-        for (int r = 0; r < 3; ++r) s_c[r] = (float)s_cd[r];
-      }
       __syncthreads();
       ++iters_run;
       if (s_conv) break;  // result.norm() < 1e-5 && != 0 leaves this level (:707-708)
@@ -401,13 +399,48 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) icp_kernel(IcpArgs a) {
   // ---------------- Track() tail (:715-723) + frame policy, block 0 only -----------------
   if (blockIdx.x != 0 || tid != 0 || !ok) return;
   const double ae = iters_run ? __ldcg(&st->ae) : 0.0;
+  if (iters_run) {
+    // the last reduction row in the reference's world form: b = M b', C = M C' M^T,
+    // M = [[I, 0], [[c]x, I]]
+    double cs[29];
+    for (int k = 0; k < 29; ++k) cs[k] = __ldcg(&st->iter_csums[k]);
+    const double cx = __ldcg(&st->iter_ccenter[0]), cy = __ldcg(&st->iter_ccenter[1]),
+                 cz = __ldcg(&st->iter_ccenter[2]);
+    double Cp[36], Mx[36], MC[36];
+    kf_make_jtj(&cs[7], Cp);
+    for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
+    Mx[3 * 6 + 1] = -cz; Mx[3 * 6 + 2] = cy;
+    Mx[4 * 6 + 0] = cz;  Mx[4 * 6 + 2] = -cx;
+    Mx[5 * 6 + 0] = -cy; Mx[5 * 6 + 1] = cx;
+    st->sums[0] = cs[0];
+    for (int r = 0; r < 6; ++r) {
+      double v = 0;
+      for (int k = 0; k < 6; ++k) v += Mx[r * 6 + k] * cs[1 + k];
+      st->sums[1 + r] = v;
+    }
+    for (int r = 0; r < 6; ++r)
+      for (int cc = 0; cc < 6; ++cc) {
+        double v = 0;
+        for (int k = 0; k < 6; ++k) v += Mx[r * 6 + k] * Cp[k * 6 + cc];
+        MC[r * 6 + cc] = v;
+      }
+    int q = 7;
+    for (int r = 0; r < 6; ++r)
+      for (int cc = r; cc < 6; ++cc) {
+        double v = 0;
+        for (int k = 0; k < 6; ++k) v += MC[r * 6 + k] * Mx[cc * 6 + k];
+        st->sums[q++] = v;
+      }
+    st->sums[28] = cs[28];
+    st->sums[29] = st->sums[30] = st->sums[31] = 0.0;
+  }
   int tracked;
   if (ae > 0.5 || ae == 0.0) {
     tracked = 0;
-    for (int k = 0; k < 16; ++k) st->pose[k] = s_old[k];
+    kf_store_pose(st, s_old);
   } else {
     tracked = 1;
-    for (int k = 0; k < 16; ++k) st->pose[k] = s_pose[k];
+    kf_store_pose(st, s_pose);
     // updatePoseFinder (gFusion.cpp:1570-1594): add when 0.2 m from every library pose
     bool add = true;
     for (int e = 0; e < st->lib_size; ++e) {

@@ -8,14 +8,15 @@
 // below 0.2, clamped to [-0.1, 0.2] with w = min(w + 1, maxWeight); otherwise (and for
 // eta <= -mu) value and weight are zeroed (Q8).
 //
-// B200 design: threads own 32 consecutive x of one y (one warp = 64 B per plane per
-// z-step for 2-byte storage, fully used sectors).  Each column first intersects its line
-// with the camera frustum analytically (five half-spaces, solved in FP64 with a two-voxel
-// margin) so voxels that cannot project into the image are never visited; inside the
-// interval every voxel runs the reference's exact tests.  The weight plane is read only
-// where eta > -mu, and a voxel whose encoded value and weight do not change is not
-// written back (the reference writes it unchanged).  Result bits are the same as
-// without these shortcuts.
+// B200 design: a block owns 32 x 8 columns by 16 z (one warp = 32 consecutive x: 64 B
+// per plane per z-step for 2-byte storage, fully used sectors); splitting the z-march
+// over 16-voxel chunks gives the SMs enough independent warps to hide the depth-gather and
+// volume latencies.  A block whose voxel box lies outside one of the five frustum
+// half-spaces returns at once, so voxels that cannot project into the image cost nothing;
+// inside, every voxel runs the reference's tests.  Per voxel one reciprocal replaces the
+// shader's divisions by z (u = fx * x/z + cx + 0.5 is the reference's (fx x + cx z)/z + 0.5
+// up to rounding).  The weight plane is read only where eta > -mu, and a voxel whose
+// encoded value and weight do not change is not written back.
 #include "kf_internal.cuh"
 
 namespace {
@@ -28,10 +29,12 @@ struct IntArgs {
   const float* depth;
   int W, H;
   float fx, fy, cx, cy;
-  float mu, maxw;
+  float mu, inv_mu, maxw;
   int band;  // Q8
   const int* gate;
   const KfDevState* st;
+  uint32_t* bricks;
+  int bx, by, bz;
 };
 
 template <class T>
@@ -41,79 +44,75 @@ __device__ __forceinline__ uint32_t bits_of(const T& v) {
   return b;
 }
 
+constexpr int kZC = 16;  // voxels per thread along z
+
+// True when the box of voxel centres [b0, b1] (index space, inclusive) lies entirely on the
+// outside of one of the five half-spaces whose intersection is the set of voxels
+// integrate.cs can touch: z >= 1e-4, 0 <= u <= W-1, 0 <= v <= H-1 (u, v the +0.5-rounded
+// projection).  Conservative: a box that is not culled is tested voxel by voxel.
+__device__ bool box_outside_frustum(const IntArgs& a, const float* inv, const int* b0, const int* b1) {
+  const float vx = a.dimx / a.nx, vy = a.dimy / a.ny, vz = a.dimz / a.nz;
+  const float kx0 = a.cx + 0.5f, kx1 = a.cx + 0.5f - (float)(a.W - 1);
+  const float ky0 = a.cy + 0.5f, ky1 = a.cy + 0.5f - (float)(a.H - 1);
+  bool all_out[5] = {true, true, true, true, true};
+  for (int c = 0; c < 8; ++c) {
+    const float wx = ((c & 1 ? b1[0] : b0[0]) + 0.5f) * vx;
+    const float wy = ((c & 2 ? b1[1] : b0[1]) + 0.5f) * vy;
+    const float wz = ((c & 4 ? b1[2] : b0[2]) + 0.5f) * vz;
+    const float X = inv[0] * wx + inv[1] * wy + inv[2] * wz + inv[3];
+    const float Y = inv[4] * wx + inv[5] * wy + inv[6] * wz + inv[7];
+    const float Z = inv[8] * wx + inv[9] * wy + inv[10] * wz + inv[11];
+    all_out[0] &= Z - 1e-4f < 0.0f;
+    all_out[1] &= a.fx * X + kx0 * Z < 0.0f;
+    all_out[2] &= -(a.fx * X + kx1 * Z) < 0.0f;
+    all_out[3] &= a.fy * Y + ky0 * Z < 0.0f;
+    all_out[4] &= -(a.fy * Y + ky1 * Z) < 0.0f;
+  }
+  return all_out[0] || all_out[1] || all_out[2] || all_out[3] || all_out[4];
+}
+
+// The z-chunk [zb, zb + kZC) of column (x, y); returns which z-bricks received a negative
+// value (bit j = brick zb/8 - 1 + j, bit 0 for the dilation of a z % 8 == 0 voxel).
 template <int S>
-__global__ void __launch_bounds__(256) integrate_kernel(IntArgs a) {
+__device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const float* inv, int x, int y, int zb) {
   typedef typename Vox<S>::V V;
   typedef typename Vox<S>::Wt Wt;
-  __shared__ float s_inv[12];  // inverse(pose): 3 rows x (R | t), row-major
-  if (a.gate && *(volatile const int*)a.gate == 0) return;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    double P[16], I[16];
-    for (int k = 0; k < 16; ++k) P[k] = a.st->pose[k];
-    kf_rigid_inverse(P, I);
-    for (int r = 0; r < 3; ++r)
-      for (int c = 0; c < 4; ++c) s_inv[r * 4 + c] = (float)I[c * 4 + r];
-  }
-  __syncthreads();
-  const int x = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= a.nx || y >= a.ny) return;
+  uint32_t zneg = 0;
 
-  // getVolumePosition (integrate.cs:16-19) for z = 0, and delta = rotate(invTrack, (0,0,vz))
+  // getVolumePosition (integrate.cs:16-19) at z = zb, and delta = rotate(invTrack, (0,0,vz))
   const float cxw = (x + 0.5f) * a.dimx / a.nx;
   const float cyw = (y + 0.5f) * a.dimy / a.ny;
-  const float czw = 0.5f * a.dimz / a.nz;
+  const float czw = (zb + 0.5f) * a.dimz / a.nz;
   const float vz = a.dimz / a.nz;
   float p0[3], dz[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    p0[r] = fmaf(s_inv[r * 4 + 0], cxw, fmaf(s_inv[r * 4 + 1], cyw, fmaf(s_inv[r * 4 + 2], czw, s_inv[r * 4 + 3])));
-    dz[r] = s_inv[r * 4 + 2] * vz;
+    p0[r] = fmaf(inv[r * 4 + 0], cxw, fmaf(inv[r * 4 + 1], cyw, fmaf(inv[r * 4 + 2], czw, inv[r * 4 + 3])));
+    dz[r] = inv[r * 4 + 2] * vz;
   }
-
-  // frustum interval of this column: alpha + beta * z >= 0 for all five constraints
-  double lo = 0.0, hi = (double)(a.nz - 1);
-  auto clip = [&](double al, double be) {
-    const double eps = 1e-5 * (fabs(al) + fabs(be) * a.nz) + 1e-9;
-    al += eps;
-    if (be > 0) lo = fmax(lo, -al / be);
-    else if (be < 0) hi = fmin(hi, -al / be);
-    else if (al < 0) hi = -1.0;
-  };
-  {
-    const double X0 = p0[0], Y0 = p0[1], Z0 = p0[2], dX = dz[0], dY = dz[1], dZ = dz[2];
-    const double kx0 = (double)a.cx + 0.5, kx1 = (double)a.cx + 0.5 - (a.W - 1);
-    const double ky0 = (double)a.cy + 0.5, ky1 = (double)a.cy + 0.5 - (a.H - 1);
-    clip(Z0 - 1e-4, dZ);                                             // z >= 1e-4
-    clip(a.fx * X0 + kx0 * Z0, a.fx * dX + kx0 * dZ);                 // px >= 0
-    clip(-(a.fx * X0 + kx1 * Z0), -(a.fx * dX + kx1 * dZ));           // px <= W - 1
-    clip(a.fy * Y0 + ky0 * Z0, a.fy * dY + ky0 * dZ);                 // py >= 0
-    clip(-(a.fy * Y0 + ky1 * Z0), -(a.fy * dY + ky1 * dZ));           // py <= H - 1
-  }
-  if (!(hi >= lo - 2.0)) return;
-  const int z0 = max(0, (int)floor(lo) - 2);
-  const int z1 = min(a.nz - 1, (int)ceil(hi) + 2);
-
   V* vf = reinterpret_cast<V*>(a.vol);
   Wt* vw = reinterpret_cast<Wt*>(reinterpret_cast<char*>(a.vol) + a.count * sizeof(V));
-  const size_t slice = (size_t)a.nx * a.ny;
-  size_t idx = (size_t)x + (size_t)a.nx * y + (size_t)z0 * slice;
+  const uint32_t slice = (uint32_t)a.nx * (uint32_t)a.ny;
+  uint32_t idx = (uint32_t)x + (uint32_t)a.nx * (uint32_t)y + (uint32_t)zb * slice;
   const float fW1 = (float)(a.W - 1), fH1 = (float)(a.H - 1);
-  for (int z = z0; z <= z1; ++z, idx += slice) {
-    const float fz = (float)z;
-    const float px3 = fmaf(fz, dz[0], p0[0]);
-    const float py3 = fmaf(fz, dz[1], p0[1]);
-    const float pz3 = fmaf(fz, dz[2], p0[2]);
-    if (pz3 < 0.0001f) continue;
-    const float u = fmaf(a.fx, px3, a.cx * pz3) / pz3 + 0.5f;
-    const float v = fmaf(a.fy, py3, a.cy * pz3) / pz3 + 0.5f;
+  const float ku = a.cx + 0.5f, kv = a.cy + 0.5f;
+  const int zend = min(kZC, a.nz - zb);
+  for (int k = 0; k < zend; ++k, idx += slice) {
+    const float fk = (float)k;
+    const float pz = fmaf(fk, dz[2], p0[2]);
+    if (pz < 0.0001f) continue;
+    const float iz = 1.0f / pz;
+    const float rx = fmaf(fk, dz[0], p0[0]) * iz;  // pos.x / pos.z
+    const float ry = fmaf(fk, dz[1], p0[1]) * iz;
+    // cameraX.x / cameraX.z + 0.5 = fx * x/z + cx + 0.5 (K has no skew, :67)
+    const float u = fmaf(a.fx, rx, ku);
+    const float v = fmaf(a.fy, ry, kv);
     if (u < 0.0f || u > fW1 || v < 0.0f || v > fH1) continue;
-    const float d = __ldg(a.depth + (size_t)(int)v * a.W + (int)u) / 1000.0f;
+    const float d = __ldg(a.depth + (uint32_t)(int)v * (uint32_t)a.W + (uint32_t)(int)u) * 0.001f;
     if (d == 0.0f) continue;
-    const float rx = px3 / pz3, ry = py3 / pz3;
-    const float diff = (d - pz3) * sqrtf(1.0f + rx * rx + ry * ry);
+    const float diff = (d - pz) * sqrtf(fmaf(rx, rx, fmaf(ry, ry, 1.0f)));
     if (diff > -a.mu) {
-      const float sdf = fminf(1.0f, diff / a.mu);
+      const float sdf = fminf(1.0f, diff * a.inv_mu);
       const V oldv = vf[idx];
       const Wt oldw = vw[idx];
       const float F = Vox<S>::raw_nc(&oldv, 0) * Vox<S>::kRawToF;
@@ -135,9 +134,68 @@ __global__ void __launch_bounds__(256) integrate_kernel(IntArgs a) {
       const Wt ew = Vox<S>::encode_weight(nw);
       if (bits_of(ev) != bits_of(oldv)) vf[idx] = ev;
       if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
+      if (Vox<S>::raw_nc(&ev, 0) < 0.0f) {
+        const int z = zb + k;
+        zneg |= 1u << ((z >> 3) - (zb >> 3) + 1);
+        if ((z & 7) == 0) zneg |= 1u << ((z >> 3) - (zb >> 3));
+      }
     } else {
       vf[idx] = Vox<S>::encode_value(0.0f);
       vw[idx] = Vox<S>::encode_weight(0.0f);
+    }
+  }
+  return zneg;
+}
+
+template <int S>
+__global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a) {
+  __shared__ int s_cull;
+  // negative-value flags of the bricks this block may touch, dilated by one voxel towards
+  // -x/-y/-z: [z: bz0-1 .. bz0+1][y: by0-1 .. by0][x: bx0-1 .. bx0+3]
+  __shared__ uint32_t s_neg[3][2][5];
+  if (a.gate && *(volatile const int*)a.gate == 0) return;
+  float inv[12];  // inverse(m_pose), rows of [R^T | -R^T t] (integrate uses glm::inverse, :1242)
+#pragma unroll
+  for (int k = 0; k < 12; ++k) inv[k] = a.st->inv_rows[k];
+  const int xb = blockIdx.x * 32, yb = blockIdx.y * 8, zb = blockIdx.z * kZC;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    // one voxel of margin on every side absorbs the rounding of the per-voxel tests
+    const int b0[3] = {xb - 1, yb - 1, zb - 1};
+    const int b1[3] = {xb + 32, yb + 8, zb + kZC};
+    s_cull = box_outside_frustum(a, inv, b0, b1) ? 1 : 0;
+  }
+  {
+    const int t = threadIdx.y * 32 + threadIdx.x;
+    if (t < 30) (&s_neg[0][0][0])[t] = 0u;
+  }
+  __syncthreads();
+  if (s_cull) return;
+  const int x = xb + threadIdx.x;
+  const int y = yb + threadIdx.y;
+  uint32_t zneg = 0;  // bit j: a negative value was written in z-brick (zb/8 - 1 + j)
+  if (x < a.nx && y < a.ny) zneg = integrate_column<S>(a, inv, x, y, zb);
+  if (zneg) {
+    // this voxel column's own brick and, at brick-low faces, the brick below (dilation)
+    const int lx = (x >> 3) - (xb >> 3) + 1, ly = 1;
+    for (int j = 0; j < 3; ++j) {
+      if (!(zneg & (1u << j))) continue;
+      atomicOr(&s_neg[j][ly][lx], 1u);
+      if ((x & 7) == 0) atomicOr(&s_neg[j][ly][lx - 1], 1u);
+      if ((y & 7) == 0) {
+        atomicOr(&s_neg[j][ly - 1][lx], 1u);
+        if ((x & 7) == 0) atomicOr(&s_neg[j][ly - 1][lx - 1], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  {
+    const int t = threadIdx.y * 32 + threadIdx.x;
+    if (t < 30) {
+      const int j = t / 10, r = (t / 5) % 2, c = t % 5;
+      const int gx = (xb >> 3) - 1 + c, gy = (yb >> 3) - 1 + r, gz = (zb >> 3) - 1 + j;
+      if (s_neg[j][r][c] && gx >= 0 && gy >= 0 && gz >= 0 && gx < a.bx && gy < a.by && gz < a.bz)
+        atomicOr(&a.bricks[(uint32_t)gx + (uint32_t)a.bx * ((uint32_t)gy + (uint32_t)a.by * (uint32_t)gz)],
+                 KF_BRICK_NEG);
     }
   }
 }
@@ -154,12 +212,15 @@ int kf_launch_integrate(kf_session* s, int gated) {
   a.W = s->W[0]; a.H = s->H[0];
   a.fx = s->intr.fx; a.fy = s->intr.fy; a.cx = s->intr.cx; a.cy = s->intr.cy;
   a.mu = s->cfg.mu;
+  a.inv_mu = 1.0f / s->cfg.mu;
   a.maxw = s->cfg.max_weight;
   a.band = (s->cfg.quirks & KF_Q8_NARROW_BAND) ? 1 : 0;
   a.gate = gated ? &s->d_state->do_integrate : nullptr;
   a.st = s->d_state;
+  a.bricks = s->d_bricks;
+  a.bx = s->bx; a.by = s->by; a.bz = s->bz;
   dim3 block(32, 8);
-  dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8);
+  dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + kZC - 1) / kZC);
   switch (s->cfg.storage) {
     case KF_STORAGE_F32F32: integrate_kernel<KF_STORAGE_F32F32><<<grid, block, 0, s->stream>>>(a); break;
     case KF_STORAGE_F16U16: integrate_kernel<KF_STORAGE_F16U16><<<grid, block, 0, s->stream>>>(a); break;

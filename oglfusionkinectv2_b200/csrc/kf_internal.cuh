@@ -33,6 +33,9 @@ struct KfDevState {
   int recover_found;    // result of the last recoverPose()
   int counter;          // kinect.cpp frame counter
   // ---- the rest of the resident state ----
+  // derived FP32 forms of `pose`, kept in step with it by every writer (kf_store_pose)
+  float pose_rows[12];  // rows of [R | t]
+  float inv_rows[12];   // rows of [R^T | -R^T t]
   double pose_eig[16];  // m_pose_eig (the SDF tracker's own pose chain)
   double old_pose[16];  // pose at the start of the last tracking call
   double raycast_pose[16];  // pose of the last raycast (projective association, Q4 clear)
@@ -51,13 +54,20 @@ struct KfDevState {
   double iter_pose[16]; // pose after the last solve (ICP) / camera-to-world (SDF)
   double iter_result[6];// SDF twist accumulator
   double iter_center[3];// ICP accumulation centre for the next iteration (world)
+  double iter_csums[32];// centred reduction row of the last ICP iteration
+  double iter_ccenter[3];// centre that row was accumulated about
+  float iter_T[16];     // FP32 pose for the next iteration (published by the last block)
+  float iter_V[16];     // FP32 view = K * inverse(.) for the next iteration
+  float iter_cf[3];     // FP32 centre for the next iteration
+  int pad1_;
   double icp_center_cam[3];  // ICP centre at the end of the last frame (camera frame)
   int iter_conv;        // convergence flag of the last solve
   int pad_[3];
   double lib_pose[KF_MAX_LIBRARY][16];  // pose library
 };
 // Bytes of KfDevState the host reads after a frame step (pose and result flags).
-#define KF_STATE_RESULT_BYTES (offsetof(KfDevState, pose_eig))
+#define KF_STATE_RESULT_BYTES (offsetof(KfDevState, pose_rows))
+static_assert(KF_STATE_RESULT_BYTES == 144, "frame result head: pose, tracked, error, recover_found, counter");
 
 struct kf_session {
   kf_config cfg{};
@@ -66,6 +76,11 @@ struct kf_session {
   int num_sms = 0;
   cudaStream_t stream = nullptr;
   std::string last_error;
+
+  // per 8^3 brick: bit 0 set when the brick (dilated by one voxel towards +x, +y, +z) may
+  // hold a negative TSDF value; set by integrate, cleared by reset, rebuilt on upload
+  uint32_t* d_bricks = nullptr;
+  int bx = 0, by = 0, bz = 0;
 
   // volume: value plane then weight plane
   void* d_vol = nullptr;
@@ -265,6 +280,18 @@ __host__ __device__ inline void kf_se3_exp(const double* xi, double* T) {
   T[15] = 1;
 }
 
+// Write m_pose and its FP32 forms (used by integrate and raycast).
+__host__ __device__ inline void kf_store_pose(KfDevState* st, const double* P) {
+  for (int k = 0; k < 16; ++k) st->pose[k] = P[k];
+  double I[16];
+  kf_rigid_inverse(P, I);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 4; ++c) {
+      st->pose_rows[r * 4 + c] = (float)P[c * 4 + r];
+      st->inv_rows[r * 4 + c] = (float)I[c * 4 + r];
+    }
+}
+
 // FP64 Cholesky solve of the 6x6 SPD normal equations.  Returns 0 and x = 0 when a pivot
 // is not positive (rank-deficient C, where the reference's JacobiSVD would return the
 // minimum-norm solution; an all-zero system gives x = 0 in both).
@@ -413,6 +440,9 @@ int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy);
 int kf_launch_sdf_policy(kf_session* s);
 int kf_launch_integrate(kf_session* s, int gated);
 int kf_launch_raycast(kf_session* s);
+int kf_rebuild_bricks(kf_session* s);
+#define KF_BRICK 8
+#define KF_BRICK_NEG 1u
 int kf_mc_run(kf_session* s, float iso, int method, uint32_t* n_tri);
 int kf_scan_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* d_total,
                 cudaStream_t stream, uint32_t* d_scratch, size_t scratch_words);

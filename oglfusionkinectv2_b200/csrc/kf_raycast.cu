@@ -13,7 +13,10 @@
 // B200 design: one thread per pixel, 32x8 tiles so a warp's rays stay coherent and its
 // trilinear taps share L1 lines; the value plane alone is read (2 B per tap for the
 // 16-bit storages).  The march position is t0 + k * step (one rounding) rather than the
-// reference's repeated float addition.
+// reference's repeated float addition.  Once the march is in its fine-step phase it
+// skips every brick whose negative-value flag is clear (no sample there can be the first
+// negative one), keeping the sample positions tb + k * step and re-evaluating the sample
+// before a hit for the refinement, so the result is the unskipped march's.
 #include "kf_internal.cuh"
 
 namespace {
@@ -27,11 +30,13 @@ struct RayArgs {
   float step, large_step, nearp, farp;
   int max_steps;
   int W, H;
-  double fx, fy, cx, cy;
+  float ikx, iky, ikcx, ikcy;  // getInverseCameraMatrix: 1/fx, 1/fy, -cx/fx, -cy/fy (float)
   float4* out_v;
   float4* out_n;
   const KfDevState* st;
   KfDevState* st_out;
+  const uint32_t* bricks;
+  int bx, by, bz;
 };
 
 template <int S>
@@ -39,21 +44,25 @@ struct Sampler {
   typedef typename Vox<S>::V V;
   const V* f;
   int nx, ny, nz;
-  size_t sxy;
+  uint32_t sxy;
   __device__ __forceinline__ float tap(int x, int y, int z) const {
-    return Vox<S>::raw(f, (size_t)x + (size_t)nx * y + sxy * z);
+    return Vox<S>::raw(f, (uint32_t)x + (uint32_t)nx * (uint32_t)y + sxy * (uint32_t)z);
   }
-  // interpVol (raycast.cs:69-82) before the final * (1/32766)
+  // interpVol (raycast.cs:69-82) before the final * (1/32766); q in voxel coordinates
+  // (world * volSize / volDim - 0.5).  The 8 taps share one base offset.
   __device__ __forceinline__ float interp_raw(float qx, float qy, float qz) const {
     const float bx = floorf(qx), by = floorf(qy), bz = floorf(qz);
     const float fx = qx - bx, fy = qy - by, fz = qz - bz;
     const int ix = (int)bx, iy = (int)by, iz = (int)bz;
     const int lx = min(max(ix, 0), nx - 1), ly = min(max(iy, 0), ny - 1), lz = min(max(iz, 0), nz - 1);
     const int ux = max(min(ix + 1, nx - 1), 0), uy = max(min(iy + 1, ny - 1), 0), uz = max(min(iz + 1, nz - 1), 0);
-    const float c000 = tap(lx, ly, lz), c100 = tap(ux, ly, lz);
-    const float c010 = tap(lx, uy, lz), c110 = tap(ux, uy, lz);
-    const float c001 = tap(lx, ly, uz), c101 = tap(ux, ly, uz);
-    const float c011 = tap(lx, uy, uz), c111 = tap(ux, uy, uz);
+    const uint32_t b = (uint32_t)lx + (uint32_t)nx * (uint32_t)ly + sxy * (uint32_t)lz;
+    const uint32_t ox = (uint32_t)(ux - lx), oy = (uint32_t)(uy - ly) * (uint32_t)nx,
+                   oz = (uint32_t)(uz - lz) * sxy;
+    const float c000 = Vox<S>::raw(f, b), c100 = Vox<S>::raw(f, b + ox);
+    const float c010 = Vox<S>::raw(f, b + oy), c110 = Vox<S>::raw(f, b + ox + oy);
+    const float c001 = Vox<S>::raw(f, b + oz), c101 = Vox<S>::raw(f, b + ox + oz);
+    const float c011 = Vox<S>::raw(f, b + oy + oz), c111 = Vox<S>::raw(f, b + ox + oy + oz);
     return ((c000 * (1 - fx) + c100 * fx) * (1 - fy) + (c010 * (1 - fx) + c110 * fx) * fy) * (1 - fz) +
            ((c001 * (1 - fx) + c101 * fx) * (1 - fy) + (c011 * (1 - fx) + c111 * fx) * fy) * fz;
   }
@@ -62,21 +71,19 @@ struct Sampler {
 template <int S>
 __global__ void __launch_bounds__(256) raycast_kernel(RayArgs a) {
   __shared__ float s_view[12];  // rows of m_pose * invK: (R K^-1 | t)
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    double P[16], iK[16], Vw[16];
-    for (int k = 0; k < 16; ++k) { P[k] = a.st->pose[k]; iK[k] = 0.0; }
-    // getInverseCameraMatrix in float (gFusion.h:451-457)
-    iK[0] = (double)(1.0f / (float)a.fx);
-    iK[8] = (double)(-(float)a.cx / (float)a.fx);
-    iK[5] = (double)(1.0f / (float)a.fy);
-    iK[9] = (double)(-(float)a.cy / (float)a.fy);
-    iK[10] = 1.0; iK[15] = 1.0;
-    kf_mat4_mul(P, iK, Vw);
-    for (int r = 0; r < 3; ++r)
-      for (int c = 0; c < 4; ++c) s_view[r * 4 + c] = (float)Vw[c * 4 + r];
-    if (blockIdx.x == 0 && blockIdx.y == 0)
-      for (int k = 0; k < 16; ++k) a.st_out->raycast_pose[k] = P[k];
+  if (threadIdx.y == 0 && threadIdx.x < 12) {
+    // view = m_pose * invK (gFusion.cpp:1296) from the FP32 pose rows and float invK
+    const int r = threadIdx.x >> 2, c = threadIdx.x & 3;
+    const float* P = a.st->pose_rows;
+    float v;
+    if (c == 0) v = P[r * 4 + 0] * a.ikx;
+    else if (c == 1) v = P[r * 4 + 1] * a.iky;
+    else if (c == 2) v = fmaf(P[r * 4 + 0], a.ikcx, fmaf(P[r * 4 + 1], a.ikcy, P[r * 4 + 2]));
+    else v = P[r * 4 + 3];
+    s_view[r * 4 + c] = v;
   }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.y == 1 && threadIdx.x < 16)
+    a.st_out->raycast_pose[threadIdx.x] = a.st->pose[threadIdx.x];
   __syncthreads();
   const int x = blockIdx.x * 32 + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -85,7 +92,7 @@ __global__ void __launch_bounds__(256) raycast_kernel(RayArgs a) {
   Sampler<S> smp;
   smp.f = reinterpret_cast<const typename Vox<S>::V*>(a.vol);
   smp.nx = a.nx; smp.ny = a.ny; smp.nz = a.nz;
-  smp.sxy = (size_t)a.nx * a.ny;
+  smp.sxy = (uint32_t)a.nx * (uint32_t)a.ny;
 
   const float ox = s_view[3], oy = s_view[7], oz = s_view[11];
   const float fxp = (float)x, fyp = (float)y;
@@ -108,28 +115,76 @@ __global__ void __launch_bounds__(256) raycast_kernel(RayArgs a) {
   float hx = 0.f, hy = 0.f, hz = 0.f, ht = 0.f;
   if (tnear < tfar) {
     float t = tnear, stepsize = a.large_step;
+    // the ray in voxel coordinates: q(t) = (o + d t) * volSize / volDim - 0.5
+    const float q0x = fmaf(ox, a.sx, -0.5f), q0y = fmaf(oy, a.sy, -0.5f), q0z = fmaf(oz, a.sz, -0.5f);
+    const float dqx = dx * a.sx, dqy = dy * a.sy, dqz = dzv * a.sz;
     auto sample = [&](float tt) {
-      const float px = fmaf(dx, tt, ox), py = fmaf(dy, tt, oy), pz = fmaf(dzv, tt, oz);
-      return smp.interp_raw(px * a.sx - 0.5f, py * a.sy - 0.5f, pz * a.sz - 0.5f) * scale;
+      return smp.interp_raw(fmaf(tt, dqx, q0x), fmaf(tt, dqy, q0y), fmaf(tt, dqz, q0z)) * scale;
     };
     float f_t = sample(t), f_tt = 0.0f;
     if (f_t >= 0.0f) {
+      // 1 / ray slope in voxel coordinates, for the brick-exit distances
+      const float rdx = 1.0f / dqx, rdy = 1.0f / dqy, rdz = 1.0f / dqz;
       float tb = t;
       int k = 0;
+      bool fine = false;       // stepsize == step (the reference never switches back)
+      bool prev_known = true;  // f_t holds the sample just before t
       // bounded march: a NaN sample keeps largeStep, so cap the step count
       for (int n = 0; t < tfar && n < a.max_steps; ++n) {
+        if (fine) {
+          // empty-space skipping: a sample whose brick holds no negative value cannot be
+          // the first negative one; jump to the first sample past the brick.  The sample
+          // positions stay tb + k * step, as in the unskipped march.
+          const float qx = fmaf(t, dqx, q0x), qy = fmaf(t, dqy, q0y), qz = fmaf(t, dqz, q0z);
+          const int ix = min(max((int)floorf(qx), 0), a.nx - 1) >> 3;
+          const int iy = min(max((int)floorf(qy), 0), a.ny - 1) >> 3;
+          const int iz = min(max((int)floorf(qz), 0), a.nz - 1) >> 3;
+          if (!(__ldg(a.bricks + (uint32_t)ix + (uint32_t)a.bx * ((uint32_t)iy + (uint32_t)a.by * (uint32_t)iz)) &
+                KF_BRICK_NEG)) {
+            // the brick spans [8i, 8i + 8) in voxel coordinates; the border bricks extend
+            // outwards (taps are clamped there)
+            float te = tfar;
+            if (dqx > 0.0f && ix < a.bx - 1) te = fminf(te, (float)(8 * ix + 8) * rdx - q0x * rdx);
+            if (dqx < 0.0f && ix > 0) te = fminf(te, (float)(8 * ix) * rdx - q0x * rdx);
+            if (dqy > 0.0f && iy < a.by - 1) te = fminf(te, (float)(8 * iy + 8) * rdy - q0y * rdy);
+            if (dqy < 0.0f && iy > 0) te = fminf(te, (float)(8 * iy) * rdy - q0y * rdy);
+            if (dqz > 0.0f && iz < a.bz - 1) te = fminf(te, (float)(8 * iz + 8) * rdz - q0z * rdz);
+            if (dqz < 0.0f && iz > 0) te = fminf(te, (float)(8 * iz) * rdz - q0z * rdz);
+            const float kf = ceilf((te - tb) / stepsize);
+            int kn = kf < 2.0e9f ? (int)kf : k + 1;
+            if (kn > k + 1) {
+              // te carries rounding; the rounded sample positions are monotone in k on
+              // every axis, so if the last skipped sample is still in this brick, all of
+              // them are.  Otherwise advance by one sample.
+              const float tl = fmaf((float)(kn - 1), stepsize, tb);
+              const int jx = min(max((int)floorf(fmaf(tl, dqx, q0x)), 0), a.nx - 1) >> 3;
+              const int jy = min(max((int)floorf(fmaf(tl, dqy, q0y)), 0), a.ny - 1) >> 3;
+              const int jz = min(max((int)floorf(fmaf(tl, dqz, q0z)), 0), a.nz - 1) >> 3;
+              if (jx != ix || jy != iy || jz != iz) kn = k + 1;
+            } else {
+              kn = k + 1;
+            }
+            k = kn;
+            t = fmaf((float)k, stepsize, tb);
+            prev_known = false;
+            continue;
+          }
+        }
         f_tt = sample(t);
         if (f_tt < 0.0f) break;
-        if (f_tt < 0.8f && stepsize != a.step) {
+        if (f_tt < 0.8f && !fine) {
+          fine = true;
           stepsize = a.step;
           tb = t;
           k = 0;
         }
         f_t = f_tt;
+        prev_known = true;
         ++k;
         t = fmaf((float)k, stepsize, tb);
       }
       if (f_tt < 0.0f) {
+        if (!prev_known) f_t = sample(fmaf((float)(k - 1), stepsize, tb));
         t = t + stepsize * f_tt / (f_t - f_tt);
         hx = fmaf(dx, t, ox);
         hy = fmaf(dy, t, oy);
@@ -192,7 +247,45 @@ __global__ void __launch_bounds__(256) raycast_kernel(RayArgs a) {
   }
 }
 
+// Negative-value flag of every brick from the volume itself (after an upload).
+template <int S>
+__global__ void __launch_bounds__(256) rebuild_bricks_kernel(const void* vol, int nx, int ny, int nz, int bx, int by,
+                                                            int bz, uint32_t* bricks) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= (uint32_t)bx * by * bz) return;
+  const int ix = b % bx, iy = (b / bx) % by, iz = b / (bx * by);
+  const typename Vox<S>::V* f = reinterpret_cast<const typename Vox<S>::V*>(vol);
+  uint32_t flag = 0;
+  for (int z = 8 * iz; z <= min(8 * iz + 8, nz - 1) && !flag; ++z)
+    for (int y = 8 * iy; y <= min(8 * iy + 8, ny - 1) && !flag; ++y)
+      for (int x = 8 * ix; x <= min(8 * ix + 8, nx - 1); ++x)
+        if (Vox<S>::raw(f, (uint32_t)x + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z)) < 0.0f) {
+          flag = KF_BRICK_NEG;
+          break;
+        }
+  bricks[b] = flag;
+}
+
 }  // namespace
+
+int kf_rebuild_bricks(kf_session* s) {
+  const uint32_t nb = (uint32_t)s->bx * s->by * s->bz;
+  const int g = (int)((nb + 255) / 256);
+  switch (s->cfg.storage) {
+    case KF_STORAGE_F32F32:
+      rebuild_bricks_kernel<KF_STORAGE_F32F32><<<g, 256, 0, s->stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      break;
+    case KF_STORAGE_F16U16:
+      rebuild_bricks_kernel<KF_STORAGE_F16U16><<<g, 256, 0, s->stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      break;
+    default:
+      rebuild_bricks_kernel<KF_STORAGE_RG16I><<<g, 256, 0, s->stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      break;
+  }
+  KF_CUDA_TRY(s, cudaGetLastError());
+  kf_note_launch(s);
+  return KF_OK;
+}
 
 int kf_launch_raycast(kf_session* s) {
   RayArgs a;
@@ -214,11 +307,16 @@ int kf_launch_raycast(kf_session* s) {
     a.max_steps = (int)fmin(n, 1.0e8);
   }
   a.W = s->W[0]; a.H = s->H[0];
-  a.fx = s->intr.fx; a.fy = s->intr.fy; a.cx = s->intr.cx; a.cy = s->intr.cy;
+  a.ikx = 1.0f / s->intr.fx;
+  a.iky = 1.0f / s->intr.fy;
+  a.ikcx = -s->intr.cx / s->intr.fx;
+  a.ikcy = -s->intr.cy / s->intr.fy;
   a.out_v = s->d_ref_vertex;
   a.out_n = s->d_ref_normal;
   a.st = s->d_state;
   a.st_out = s->d_state;
+  a.bricks = s->d_bricks;
+  a.bx = s->bx; a.by = s->by; a.bz = s->bz;
   dim3 block(32, 8);
   dim3 grid((a.W + 31) / 32, (a.H + 7) / 8);
   switch (s->cfg.storage) {

@@ -247,12 +247,13 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
         double E[16], Pn[16];
         kf_se3_exp(res, E);
         kf_mat4_mul(E, s_prev, Pn);
-        for (int k = 0; k < 16; ++k) { st->pose_eig[k] = Pn[k]; st->pose[k] = Pn[k]; }
+        for (int k = 0; k < 16; ++k) st->pose_eig[k] = Pn[k];
+        kf_store_pose(st, Pn);
         for (int k = 0; k < 6; ++k) st->cum_twist[k] += res[k];
       } else {
         // m_pose = oldPose: the pose at entry, i.e. the library pose in recover mode
         if (a.recover)
-          for (int k = 0; k < 16; ++k) st->pose[k] = st->lib_pose[attempt][k];
+          kf_store_pose(st, st->lib_pose[attempt]);
       }
       if (!a.recover) st->tracked = tracked ? 1 : 0;  // recoverPose leaves `tracked` alone
       st->iterations_run = iters_run;

@@ -97,6 +97,33 @@ def test_raycast_parity(storage):
     assert np.mean(np.degrees(np.arccos(cosang)) < 1.0) > 0.99
 
 
+def test_raycast_brick_skip_is_exact():
+    """kf_raycast skips 8^3 bricks whose flag says they hold no negative value.  The flags
+    kf_integrate maintains (a superset: they are never cleared) and the ones rebuilt from an
+    uploaded copy of the same volume must give bit-identical maps, from poses inside and
+    outside the volume."""
+    w = small_workload(6, size=128)
+    g = GFusion(w.config, w.intrinsics)
+    g.Reset(w.poses[0])
+    for k in range(4):
+        g.setPose(w.poses[k])
+        g.depthToVertex(w.frame(k))
+        g.integrate()
+    h = GFusion(w.config, w.intrinsics)
+    h.Reset(w.poses[0])
+    h.setVolumeRaw(g.getVolumeRaw())
+    outside = w.poses[0].copy()
+    outside[:3, 3] -= 0.6 * outside[:3, 2]  # back the camera out along its view axis
+    for pose in (w.poses[4], w.poses[5], outside):
+        for s in (g, h):
+            s.setPose(pose)
+            s.raycast()
+        Vg, Vh = g.getVerts(), h.getVerts()
+        assert (Vg[..., 3] > 0).mean() > 0.1
+        np.testing.assert_array_equal(Vg, Vh)
+        np.testing.assert_array_equal(g.getNorms(), h.getNorms())
+
+
 def _teacher_forced(w, k, track):
     """Both sides track frame k from the pose of frame k-1 against identical reference
     maps (the GPU raycast copied into the oracle) and an identical volume."""
