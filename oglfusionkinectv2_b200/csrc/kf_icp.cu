@@ -49,13 +49,11 @@ struct IcpArgs {
 };
 
 // ---- track.cs:53-133 for one pixel ------------------------------------------------------
-__device__ __forceinline__ int track_pixel(const IcpArgs& a, int l, int x, int y,
+// n, v: the pixel's normal and vertex (loaded one pass ahead by the caller)
+__device__ __forceinline__ int track_pixel(const IcpArgs& a, const float4 n, const float4 v,
                                            const float* T, const float* V, const float* c,
                                            float* f, float* pw) {
-  const size_t i = (size_t)y * a.W[l] + x;
-  const float4 n = __ldg(&a.normal[l][i]);
   if (n.x == 2.0f) return -1;
-  const float4 v = __ldg(&a.vertex[l][i]);
   // z == 0 with a valid normal projects (0,0,0) -> 0/0 in track.cs:72 (undefined in
   // GLSL); treated as "outside the image"
   if (v.z == 0.0f) return -2;
@@ -178,16 +176,30 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
       for (int k = 0; k < (JTJ ? 4 : 28); ++k) acc[k] = 0.0f;
       float pacc[4] = {0.f, 0.f, 0.f, 0.f};  // valid count, sum of world points
       const int stride = nb * KF_TRACK_THREADS;
-      for (int base = (blockIdx.x * kWarps + warp) * 32; base < P; base += stride) {
+      const float4* Nl = a.normal[level];
+      const float4* Vl = a.vertex[level];
+      int base = (blockIdx.x * kWarps + warp) * 32;
+      // the next pass's normal and vertex are in flight while this pass gathers the
+      // reference maps
+      float4 nn = make_float4(2.0f, 0.f, 0.f, 0.f), vn = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (base + lane < P) {
+        nn = __ldg(Nl + base + lane);
+        vn = __ldg(Vl + base + lane);
+      }
+      for (; base < P; base += stride) {
         const int i = base + lane;
+        const float4 n = nn, v = vn;
+        if (i + stride < P) {
+          nn = __ldg(Nl + i + stride);
+          vn = __ldg(Vl + i + stride);
+        }
         float f[7] = {0, 0, 0, 0, 0, 0, 0};
         float pw[3] = {0, 0, 0};
         int status = 0;
         if (i < P) {
-          const int y = i / Wl, x = i - y * Wl;
-          status = track_pixel(a, level, x, y, T, V, c, f, pw);
+          status = track_pixel(a, n, v, T, V, c, f, pw);
           a.status[level][i] = status;
-          if (a.q1 && (y & 7) != 7) status = 0;  // only work group 7 reaches the solver
+          if (a.q1 && ((i / Wl) & 7) != 7) status = 0;  // only work group 7 reaches the solver
         }
         const bool use = status == 1;
         if (use) {
@@ -297,10 +309,41 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
       // ---------------- hand-over: last block reduces + solves ----------------
       if (kf_grid_arrive(st, nb, &s_gen, &s_last)) {
         {
-          const int k = tid & 31, r = tid >> 5;
-          double v = 0.0;
-          for (unsigned b = r; b < nb; b += kWarps) v += (double)__ldcg(&a.partials[(size_t)b * 32 + k]);
-          s_red[r][k] = v;
+          // fixed-order FP64 sum of the nb partial rows: thread (r0, q) sums columns
+          // 4q..4q+3 of rows r0, r0 + 32, ... with all of its loads in flight at once
+          const int q = tid & 7, r0 = tid >> 3;
+          const float4* P4 = reinterpret_cast<const float4*>(a.partials);
+          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+          constexpr int kChunk = 12;
+          for (unsigned b0 = r0; b0 < nb; b0 += 32u * kChunk) {
+            float4 buf[kChunk];
+#pragma unroll
+            for (int m = 0; m < kChunk; ++m) {
+              const unsigned b = b0 + 32u * m;
+              buf[m] = b < nb ? __ldcg(P4 + (size_t)b * 8 + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int m = 0; m < kChunk; ++m) {
+              s0 += (double)buf[m].x;
+              s1 += (double)buf[m].y;
+              s2 += (double)buf[m].z;
+              s3 += (double)buf[m].w;
+            }
+          }
+          // the warp's four row groups (lanes q, q+8, q+16, q+24), then the warps in order
+#pragma unroll
+          for (int o = 8; o < 32; o <<= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+          }
+          if (lane < 8) {
+            s_red[warp][4 * lane + 0] = s0;
+            s_red[warp][4 * lane + 1] = s1;
+            s_red[warp][4 * lane + 2] = s2;
+            s_red[warp][4 * lane + 3] = s3;
+          }
         }
         __syncthreads();
         if (tid < 32) {
@@ -310,68 +353,76 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
           s_sums[tid] = v;
         }
         __syncthreads();
-        if (tid == 0) {
+        if (warp == 0) {
+          // ---- solve, lane-parallel in warp 0 ----
           // reduce.cs counts every pixel of the (group-7) rows in sums[28]
           const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
           const double nvalid = s_sums[28];
           const double cx = s_cd[0], cy = s_cd[1], cz = s_cd[2];
-          double bp[6], Cp[36], xp[6];
-          for (int k = 0; k < 6; ++k) bp[k] = s_sums[1 + k];
-          kf_make_jtj(&s_sums[7], Cp);
-          const double ae = sqrt(s_sums[0] / count);  // getReduction :1167
-          kf_cholesky6(Cp, bp, xp);
+          double xp[6];
+          kf_cholesky6_warp(&s_sums[7], &s_sums[1], xp, lane);
           // back to the reference's variables: w = w', t = t' - w x c
           double x[6];
           x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
           x[0] = xp[0] - (x[4] * cz - x[5] * cy);
           x[1] = xp[1] - (x[5] * cx - x[3] * cz);
           x[2] = xp[2] - (x[3] * cy - x[4] * cx);
-          // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2 (gFusion.cpp:700-703)
+          // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2 (gFusion.cpp:700-703);
+          // lanes 0..2 evaluate the three sincos at once
+          double sn, cs;
+          sincos(lane == 0 ? x[3] : (lane == 1 ? x[4] : x[5]), &sn, &cs);
+          const double sa = __shfl_sync(0xffffffffu, sn, 0), ca = __shfl_sync(0xffffffffu, cs, 0);
+          const double sb = __shfl_sync(0xffffffffu, sn, 1), cb = __shfl_sync(0xffffffffu, cs, 1);
+          const double sc = __shfl_sync(0xffffffffu, sn, 2), cc = __shfl_sync(0xffffffffu, cs, 2);
           double R[9];
-          kf_euler_xyz(x[3], x[4], x[5], R);
-          for (int cc = 0; cc < 3; ++cc)
-            for (int r = 0; r < 3; ++r) s_D[cc * 4 + r] = R[cc * 3 + r];
-          s_D[3] = s_D[7] = s_D[11] = 0;
-          s_D[12] = x[0]; s_D[13] = x[1]; s_D[14] = x[2]; s_D[15] = 1;
-          const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] +
-                                  x[4] * x[4] + x[5] * x[5]);
-          s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
-          st->iter_conv = s_conv;
-          st->ae = ae;
-          // the centred row; the tail turns the last one into the reference's world form
-          for (int k = 0; k < 28; ++k) st->iter_csums[k] = s_sums[k];
-          st->iter_csums[28] = count;
-          st->iter_ccenter[0] = cx; st->iter_ccenter[1] = cy; st->iter_ccenter[2] = cz;
-          // next centre: this iteration's centroid of the valid points
-          if (nvalid > 0) {
-            s_cd[0] = s_sums[29] / nvalid;
-            s_cd[1] = s_sums[30] / nvalid;
-            s_cd[2] = s_sums[31] / nvalid;
+          kf_euler_xyz_from_sincos(sa, ca, sb, cb, sc, cc, R);
+          // pose = delta * pose, one element per lane (delta column-major: R | x0..2)
+          double pn = 0.0;
+          if (lane < 16) {
+            const int r = lane & 3, col = lane >> 2;
+            // row r of delta, selected without indexing registers by lane
+            const double d0 = r == 0 ? R[0] : (r == 1 ? R[1] : (r == 2 ? R[2] : 0.0));
+            const double d1 = r == 0 ? R[3] : (r == 1 ? R[4] : (r == 2 ? R[5] : 0.0));
+            const double d2 = r == 0 ? R[6] : (r == 1 ? R[7] : (r == 2 ? R[8] : 0.0));
+            const double d3 = r == 0 ? x[0] : (r == 1 ? x[1] : (r == 2 ? x[2] : 1.0));
+            pn += d0 * s_pose[col * 4 + 0];
+            pn += d1 * s_pose[col * 4 + 1];
+            pn += d2 * s_pose[col * 4 + 2];
+            pn += d3 * s_pose[col * 4 + 3];
           }
-          for (int r = 0; r < 3; ++r) {
-            st->iter_center[r] = s_cd[r];
-            s_c[r] = (float)s_cd[r];
-            st->iter_cf[r] = s_c[r];
+          if (lane < 28) st->iter_csums[lane] = s_sums[lane];
+          if (lane == 28) st->iter_csums[28] = count;
+          if (lane == 29) {
+            const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] +
+                                    x[4] * x[4] + x[5] * x[5]);
+            s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
+            st->iter_conv = s_conv;
           }
-        }
-        __syncthreads();
-        // pose = delta * pose, one element per thread
-        double pn = 0.0;
-        if (tid < 16) {
-          const int r = tid & 3, cc = tid >> 2;
-          for (int k = 0; k < 4; ++k) pn += s_D[k * 4 + r] * s_pose[cc * 4 + k];
-        }
-        __syncthreads();
-        if (tid < 16) {
-          s_pose[tid] = pn;
-          st->iter_pose[tid] = pn;
-          s_T[tid] = (float)pn;
-          st->iter_T[tid] = s_T[tid];
-        }
-        __syncthreads();
-        if (a.same_pixel && tid == 0) {
-          make_float_mats(a, s_pose, s_ray, s_T, s_V);
-          for (int k = 0; k < 16; ++k) st->iter_V[k] = s_V[k];
+          if (lane == 30) st->ae = sqrt(s_sums[0] / count);  // getReduction :1167
+          __syncwarp();
+          if (lane < 16) {
+            s_pose[lane] = pn;
+            st->iter_pose[lane] = pn;
+            s_T[lane] = (float)pn;
+            st->iter_T[lane] = s_T[lane];
+          }
+          double cn = 0.0;
+          if (lane < 3) {
+            // the centred row's centre; the tail turns the last row into the world form
+            st->iter_ccenter[lane] = s_cd[lane];
+            // next centre: this iteration's centroid of the valid points
+            cn = nvalid > 0 ? s_sums[29 + lane] / nvalid : s_cd[lane];
+            st->iter_center[lane] = cn;
+            s_c[lane] = (float)cn;
+            st->iter_cf[lane] = s_c[lane];
+          }
+          __syncwarp();
+          if (lane < 3) s_cd[lane] = cn;
+          __syncwarp();
+          if (a.same_pixel && lane == 0) {
+            make_float_mats(a, s_pose, s_ray, s_T, s_V);
+            for (int k = 0; k < 16; ++k) st->iter_V[k] = s_V[k];
+          }
         }
         kf_grid_release(st);
       } else {

@@ -222,11 +222,8 @@ __host__ __device__ inline void kf_rigid_inverse(const double* T, double* out) {
 
 // glm::eulerAngleXYZ(t1,t2,t3) = Rx(t1) * Ry(t2) * Rz(t3) (used at gFusion.cpp:700),
 // written out from the three elementary rotations; column-major 3x3.
-__host__ __device__ inline void kf_euler_xyz(double a, double b, double c, double* R) {
-  double sa, ca, sb, cb, sc, cc;
-  sincos(a, &sa, &ca);
-  sincos(b, &sb, &cb);
-  sincos(c, &sc, &cc);
+__host__ __device__ inline void kf_euler_xyz_from_sincos(double sa, double ca, double sb, double cb, double sc,
+                                                         double cc, double* R) {
   // column 0
   R[0] = cb * cc;
   R[1] = ca * sc + sa * sb * cc;
@@ -239,6 +236,14 @@ __host__ __device__ inline void kf_euler_xyz(double a, double b, double c, doubl
   R[6] = sb;
   R[7] = -sa * cb;
   R[8] = ca * cb;
+}
+
+__host__ __device__ inline void kf_euler_xyz(double a, double b, double c, double* R) {
+  double sa, ca, sb, cb, sc, cc;
+  sincos(a, &sa, &ca);
+  sincos(b, &sb, &cb);
+  sincos(c, &sc, &cc);
+  kf_euler_xyz_from_sincos(sa, ca, sb, cb, sc, cc, R);
 }
 
 // exp of Twist(xi) (gFusion.cpp:811-833): closed-form SE(3) exponential, xi = (w, v).
@@ -370,6 +375,65 @@ __host__ __device__ inline void kf_make_jtj(const double* v21, double* C) {
     }
 }
 
+// kf_cholesky6 for one warp: C given as the 21 upper-triangular values of reduce.cs rows
+// 7..27 (row-major), b as 6 values, both in shared or global memory read by every lane.
+// Lane i < 6 factors row i; every lane returns the whole solution in x (zero when C is
+// not numerically positive definite, as kf_cholesky6).
+__device__ inline void kf_cholesky6_warp(const double* v21, const double* b, double* x, int lane) {
+  auto at = [&](int i, int j) {
+    if (i > j) { const int t = i; i = j; j = t; }
+    return v21[6 * i - (i * (i - 1)) / 2 + (j - i)];
+  };
+  const int i = lane < 6 ? lane : 5;
+  double row[6], Lrow[6], Lcol[6];
+  double dmax = 0.0;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    row[j] = at(i, j);
+    Lrow[j] = 0.0;
+    Lcol[j] = 0.0;
+    dmax = fmax(dmax, fabs(at(j, j)));
+  }
+  const double eps = 1e-13 * dmax;
+  bool spd = true;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const double d = __shfl_sync(0xffffffffu, row[j], j);  // C_jj - sum_k L_jk^2
+    if (!(d > eps)) { spd = false; break; }                 // uniform: d is broadcast
+    const double ljj = sqrt(d);
+    const double lij = lane == j ? ljj : (lane > j ? row[j] / ljj : 0.0);
+    Lrow[j] = lij;
+    if (lane == j) Lcol[j] = ljj;
+#pragma unroll
+    for (int k = j + 1; k < 6; ++k) {
+      const double lkj = __shfl_sync(0xffffffffu, lij, k);
+      if (lane > j) row[k] = fma(-lij, lkj, row[k]);
+      if (lane == j) Lcol[k] = lkj;
+    }
+  }
+  if (!spd) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) x[k] = 0.0;
+    return;
+  }
+  // L y = b, then L^T x = y
+  double y = b[i];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    if (lane == k) y = y / Lrow[k];
+    const double yk = __shfl_sync(0xffffffffu, y, k);
+    if (lane > k) y = fma(-Lrow[k], yk, y);
+  }
+#pragma unroll
+  for (int k = 5; k >= 0; --k) {
+    if (lane == k) y = y / Lcol[k];
+    const double xk = __shfl_sync(0xffffffffu, y, k);
+    if (lane < k) y = fma(-Lcol[k], xk, y);
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) x[k] = __shfl_sync(0xffffffffu, y, k);
+}
+
 // ---------------------------------------------------------------------------------------
 // Grid hand-over for the persistent (cooperatively launched) tracking kernels.
 // kf_grid_arrive: every block calls it after writing its partial sums; it returns true
@@ -377,37 +441,47 @@ __host__ __device__ inline void kf_make_jtj(const double* v21, double* C) {
 // kf_grid_release.  The other blocks wait in kf_grid_wait.  Every wait is bounded: after
 // KF_BARRIER_SPIN_CYCLES the block records KF_DEV_ERR_TIMEOUT in st->error and stops;
 // callers leave their loops when kf_grid_wait returns false.
+__device__ __forceinline__ unsigned kf_ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned kf_ld_relaxed_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The bar.sync before thread 0's gpu-scope release (or acq_rel) orders every thread's
+// earlier stores of the block before it; an acquirer that observes the release sees them.
 __device__ inline bool kf_grid_arrive(KfDevState* st, unsigned nblocks, unsigned* s_gen,
                                       int* s_last) {
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
-    *s_gen = *(volatile unsigned*)&st->barrier_gen;
-    __threadfence();
-    unsigned arrived = atomicAdd(&st->barrier_count, 1u) + 1u;
-    *s_last = (arrived == nblocks);
-    __threadfence();
+    // the generation cannot advance before this block has arrived
+    *s_gen = kf_ld_relaxed_gpu(&st->barrier_gen);
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(&st->barrier_count) : "memory");
+    *s_last = (old + 1u == nblocks);
   }
   __syncthreads();
   return *s_last != 0;
 }
 
 __device__ inline void kf_grid_release(KfDevState* st) {
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
-    st->barrier_count = 0;
-    __threadfence();
-    atomicAdd(&st->barrier_gen, 1u);
+    asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(&st->barrier_count) : "memory");
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&st->barrier_gen) : "memory");
   }
 }
 
 __device__ inline bool kf_grid_wait(KfDevState* st, const unsigned* s_gen, int* s_flag) {
   if (threadIdx.x == 0) {
-    volatile unsigned* vgen = &st->barrier_gen;
     int ok = 1;
-    long long t0 = clock64();
-    while (*vgen == *s_gen) {
+    const long long t0 = clock64();
+    while (kf_ld_acquire_gpu(&st->barrier_gen) == *s_gen) {
       if (*(volatile int*)&st->error) { ok = 0; break; }
       if (clock64() - t0 > KF_BARRIER_SPIN_CYCLES) {
         atomicExch(&st->error, KF_DEV_ERR_TIMEOUT);
@@ -416,7 +490,6 @@ __device__ inline bool kf_grid_wait(KfDevState* st, const unsigned* s_gen, int* 
       }
       __nanosleep(32);
     }
-    __threadfence();
     if (*(volatile int*)&st->error) ok = 0;
     *s_flag = ok;
   }

@@ -262,8 +262,11 @@ __global__ void __launch_bounds__(256) scan_generate_kernel(ScanArgs a) {
   }
 }
 
+// Grows a device buffer to at least `bytes`, by 1.5x steps so that a mesh that grows
+// from one extraction to the next does not reallocate (and synchronise) every time.
 int ensure(kf_session* s, void** p, size_t* cap, size_t bytes) {
   if (*cap >= bytes && *p) return KF_OK;
+  bytes = std::max(bytes, *cap + *cap / 2);
   cudaFree(*p);
   *p = nullptr;
   *cap = 0;

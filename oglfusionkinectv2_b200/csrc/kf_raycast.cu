@@ -10,7 +10,7 @@
 // central-difference trilinear gradient (getGradient :229-276), zero when its length is
 // zero.  Misses write zero vertex and normal.
 //
-// B200 design: one thread per pixel, 32x8 tiles so a warp's rays stay coherent and its
+// B200 design: one thread per pixel, 32x4 tiles so a warp's rays stay coherent and its
 // trilinear taps share L1 lines; the value plane alone is read (2 B per tap for the
 // 16-bit storages).  The march position is t0 + k * step (one rounding) rather than the
 // reference's repeated float addition.  Once the march is in its fine-step phase it
@@ -38,6 +38,11 @@ struct RayArgs {
   const uint32_t* bricks;
   int bx, by, bz;
 };
+
+// 32 x 4 pixel tiles: ray lengths vary a lot, and small blocks keep the SMs evenly loaded
+// to the end of the launch (512 x 424 gives 1,696 blocks)
+constexpr int kRayRows = 4;
+constexpr int kRayThreads = 32 * kRayRows;
 
 template <int S>
 struct Sampler {
@@ -69,7 +74,7 @@ struct Sampler {
 };
 
 template <int S>
-__global__ void __launch_bounds__(256) raycast_kernel(RayArgs a) {
+__global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs a) {
   __shared__ float s_view[12];  // rows of m_pose * invK: (R K^-1 | t)
   if (threadIdx.y == 0 && threadIdx.x < 12) {
     // view = m_pose * invK (gFusion.cpp:1296) from the FP32 pose rows and float invK
@@ -317,8 +322,8 @@ int kf_launch_raycast(kf_session* s) {
   a.st_out = s->d_state;
   a.bricks = s->d_bricks;
   a.bx = s->bx; a.by = s->by; a.bz = s->bz;
-  dim3 block(32, 8);
-  dim3 grid((a.W + 31) / 32, (a.H + 7) / 8);
+  dim3 block(32, kRayRows);
+  dim3 grid((a.W + 31) / 32, (a.H + kRayRows - 1) / kRayRows);
   switch (s->cfg.storage) {
     case KF_STORAGE_F32F32: raycast_kernel<KF_STORAGE_F32F32><<<grid, block, 0, s->stream>>>(a); break;
     case KF_STORAGE_F16U16: raycast_kernel<KF_STORAGE_F16U16><<<grid, block, 0, s->stream>>>(a); break;

@@ -293,7 +293,8 @@ class GFusion:
         return n.value
 
     def getTimes(self) -> np.ndarray:
-        """Device ms of the last pyramid, track, integrate, recover, raycast stages."""
+        """Device ms of the last pyramid, track, integrate, recover and raycast stages and
+        of the last marching-cubes extraction."""
         a = (C.c_float * 6)()
         self._check(self.lib.kf_get_stage_times(self._h, a), "kf_get_stage_times")
         return np.array(list(a), dtype=np.float32)
