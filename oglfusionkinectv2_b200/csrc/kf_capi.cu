@@ -398,7 +398,7 @@ int kf_session_device_bytes(const kf_config* cfg, const kf_intrinsics* in, uint6
   b += px * (4 + 16 + 16 + 4) * 2;         // three levels (sum < 4/3 of level 0)
   b += px * 32;                            // raycast maps
   b += px * 32;                            // sdf rows
-  b += (uint64_t)KF_MAX_TRACK_BLOCKS * 32 * 4 + sizeof(KfDevState);
+  b += (uint64_t)2 * KF_MAX_TRACK_BLOCKS * 32 * 4 + sizeof(KfDevState);
   *bytes = b;
   return KF_OK;
 }
@@ -451,7 +451,7 @@ int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out)
   if ((rc = dalloc(s, &s->d_ref_vertex, px))) return bail(rc);
   if ((rc = dalloc(s, &s->d_ref_normal, px))) return bail(rc);
   if ((rc = dalloc(s, &s->d_sdf_rows, px * 8))) return bail(rc);
-  if ((rc = dalloc(s, &s->d_partials, (size_t)KF_MAX_TRACK_BLOCKS * 32))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_partials, (size_t)2 * KF_MAX_TRACK_BLOCKS * 32))) return bail(rc);
   if ((rc = dalloc(s, &s->d_state, 1))) return bail(rc);
   if ((rc = dalloc(s, &s->d_u32_scalar, 4))) return bail(rc);
   cudaMemsetAsync(s->d_ref_vertex, 0, px * 16, s->stream);

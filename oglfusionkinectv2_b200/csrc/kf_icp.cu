@@ -126,14 +126,13 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
   __shared__ double s_old[16];
   __shared__ double s_ray[16];
   __shared__ double s_cd[3];
-  __shared__ double s_D[16];
   __shared__ float s_T[16], s_V[16], s_c[3];
   __shared__ float s_warp[kWarps][64];
   __shared__ float s_pw[kWarps][4];
   __shared__ double s_red[kWarps][32];
   __shared__ double s_sums[32];
-  __shared__ unsigned s_gen;
-  __shared__ int s_last, s_flag, s_conv;
+  __shared__ double s_csums[29], s_ccenter[3], s_ae;  // last centred row (for the tail)
+  __shared__ int s_flag, s_conv;
   __shared__ __align__(16) __nv_bfloat16 s_hi[JTJ ? kWarps : 1][8][40];
   __shared__ __align__(16) __nv_bfloat16 s_mid[JTJ ? kWarps : 1][8][40];
   __shared__ __align__(16) __nv_bfloat16 s_lo[JTJ ? kWarps : 1][8][40];
@@ -161,6 +160,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
 
   bool ok = true;
   int iters_run = 0;
+  unsigned gi = 0;  // iterations of this launch so far: grid barrier target and partials buffer
   for (int level = 2; level >= 0 && ok; --level) {
     const int Wl = a.W[level], Hl = a.H[level];
     const int P = Wl * Hl;
@@ -255,6 +255,9 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
       }
 
       // ---------------- block partial: 28 sums + valid count + point sum --------------
+      // two partial buffers, alternating by iteration: a block can only write iteration
+      // k + 1's row after every block has passed barrier k, i.e. finished reading row k - 1
+      float* part = a.partials + (size_t)(gi & 1u) * KF_MAX_TRACK_BLOCKS * 32;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         float v = pacc[k];
@@ -275,7 +278,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
           float v = 0.0f;
 #pragma unroll
           for (int w = 0; w < kWarps; ++w) v += s_warp[w][tid];
-          a.partials[(size_t)blockIdx.x * 32 + tid] = v;
+          part[(size_t)blockIdx.x * 32 + tid] = v;
         }
       } else {
         // lane (g, t) holds M[g][2t], M[g][2t+1] as rows g + g+8 of the accumulator
@@ -296,151 +299,129 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
           float v = 0.0f;
 #pragma unroll
           for (int w = 0; w < kWarps; ++w) v += s_warp[w][r * 8 + cc];
-          a.partials[(size_t)blockIdx.x * 32 + tid] = v;
+          part[(size_t)blockIdx.x * 32 + tid] = v;
         }
       }
       if (tid >= 28 && tid < 32) {
         float v = 0.0f;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) v += s_pw[w][tid - 28];
-        a.partials[(size_t)blockIdx.x * 32 + tid] = v;
+        part[(size_t)blockIdx.x * 32 + tid] = v;
       }
 
-      // ---------------- hand-over: last block reduces + solves ----------------
-      if (kf_grid_arrive(st, nb, &s_gen, &s_last)) {
-        {
-          // fixed-order FP64 sum of the nb partial rows: thread (r0, q) sums columns
-          // 4q..4q+3 of rows r0, r0 + 32, ... with all of its loads in flight at once
-          const int q = tid & 7, r0 = tid >> 3;
-          const float4* P4 = reinterpret_cast<const float4*>(a.partials);
-          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-          constexpr int kChunk = 12;
-          for (unsigned b0 = r0; b0 < nb; b0 += 32u * kChunk) {
-            float4 buf[kChunk];
+      // ---------------- grid barrier; then every block reduces and solves ----------------
+      // Every block sums the same partial rows in the same order and solves the same system
+      // in FP64, so all blocks hold bit-identical results without a second hand-over, and
+      // the solve's code stays warm in every SM's instruction cache.
+      ok = kf_grid_sync(st, nb * (gi + 1u), &s_flag);
+      if (!ok) break;
+      {
+        // fixed-order FP64 sum of the nb partial rows: thread (r0, q) sums columns
+        // 4q..4q+3 of rows r0, r0 + 32, ... with all of its loads in flight at once
+        const int q = tid & 7, r0 = tid >> 3;
+        const float4* P4 = reinterpret_cast<const float4*>(part);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        constexpr int kChunk = 12;
+        for (unsigned b0 = r0; b0 < nb; b0 += 32u * kChunk) {
+          float4 buf[kChunk];
 #pragma unroll
-            for (int m = 0; m < kChunk; ++m) {
-              const unsigned b = b0 + 32u * m;
-              buf[m] = b < nb ? __ldcg(P4 + (size_t)b * 8 + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-#pragma unroll
-            for (int m = 0; m < kChunk; ++m) {
-              s0 += (double)buf[m].x;
-              s1 += (double)buf[m].y;
-              s2 += (double)buf[m].z;
-              s3 += (double)buf[m].w;
-            }
+          for (int m = 0; m < kChunk; ++m) {
+            const unsigned b = b0 + 32u * m;
+            buf[m] = b < nb ? __ldcg(P4 + (size_t)b * 8 + q) : make_float4(0.f, 0.f, 0.f, 0.f);
           }
-          // the warp's four row groups (lanes q, q+8, q+16, q+24), then the warps in order
 #pragma unroll
-          for (int o = 8; o < 32; o <<= 1) {
-            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-            s3 += __shfl_xor_sync(0xffffffffu, s3, o);
-          }
-          if (lane < 8) {
-            s_red[warp][4 * lane + 0] = s0;
-            s_red[warp][4 * lane + 1] = s1;
-            s_red[warp][4 * lane + 2] = s2;
-            s_red[warp][4 * lane + 3] = s3;
+          for (int m = 0; m < kChunk; ++m) {
+            s0 += (double)buf[m].x;
+            s1 += (double)buf[m].y;
+            s2 += (double)buf[m].z;
+            s3 += (double)buf[m].w;
           }
         }
-        __syncthreads();
-        if (tid < 32) {
-          double v = 0.0;
+        // the warp's four row groups (lanes q, q+8, q+16, q+24), then the warps in order
 #pragma unroll
-          for (int r = 0; r < kWarps; ++r) v += s_red[r][tid];
-          s_sums[tid] = v;
+        for (int o = 8; o < 32; o <<= 1) {
+          s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+          s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+          s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+          s3 += __shfl_xor_sync(0xffffffffu, s3, o);
         }
-        __syncthreads();
-        if (warp == 0) {
-          // ---- solve, lane-parallel in warp 0 ----
-          // reduce.cs counts every pixel of the (group-7) rows in sums[28]
-          const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
-          const double nvalid = s_sums[28];
-          const double cx = s_cd[0], cy = s_cd[1], cz = s_cd[2];
-          double xp[6];
-          kf_cholesky6_warp(&s_sums[7], &s_sums[1], xp, lane);
-          // back to the reference's variables: w = w', t = t' - w x c
-          double x[6];
-          x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
-          x[0] = xp[0] - (x[4] * cz - x[5] * cy);
-          x[1] = xp[1] - (x[5] * cx - x[3] * cz);
-          x[2] = xp[2] - (x[3] * cy - x[4] * cx);
-          // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2 (gFusion.cpp:700-703);
-          // lanes 0..2 evaluate the three sincos at once
-          double sn, cs;
-          sincos(lane == 0 ? x[3] : (lane == 1 ? x[4] : x[5]), &sn, &cs);
-          const double sa = __shfl_sync(0xffffffffu, sn, 0), ca = __shfl_sync(0xffffffffu, cs, 0);
-          const double sb = __shfl_sync(0xffffffffu, sn, 1), cb = __shfl_sync(0xffffffffu, cs, 1);
-          const double sc = __shfl_sync(0xffffffffu, sn, 2), cc = __shfl_sync(0xffffffffu, cs, 2);
-          double R[9];
-          kf_euler_xyz_from_sincos(sa, ca, sb, cb, sc, cc, R);
-          // pose = delta * pose, one element per lane (delta column-major: R | x0..2)
-          double pn = 0.0;
-          if (lane < 16) {
-            const int r = lane & 3, col = lane >> 2;
-            // row r of delta, selected without indexing registers by lane
-            const double d0 = r == 0 ? R[0] : (r == 1 ? R[1] : (r == 2 ? R[2] : 0.0));
-            const double d1 = r == 0 ? R[3] : (r == 1 ? R[4] : (r == 2 ? R[5] : 0.0));
-            const double d2 = r == 0 ? R[6] : (r == 1 ? R[7] : (r == 2 ? R[8] : 0.0));
-            const double d3 = r == 0 ? x[0] : (r == 1 ? x[1] : (r == 2 ? x[2] : 1.0));
-            pn += d0 * s_pose[col * 4 + 0];
-            pn += d1 * s_pose[col * 4 + 1];
-            pn += d2 * s_pose[col * 4 + 2];
-            pn += d3 * s_pose[col * 4 + 3];
-          }
-          if (lane < 28) st->iter_csums[lane] = s_sums[lane];
-          if (lane == 28) st->iter_csums[28] = count;
-          if (lane == 29) {
-            const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] +
-                                    x[4] * x[4] + x[5] * x[5]);
-            s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
-            st->iter_conv = s_conv;
-          }
-          if (lane == 30) st->ae = sqrt(s_sums[0] / count);  // getReduction :1167
-          __syncwarp();
-          if (lane < 16) {
-            s_pose[lane] = pn;
-            st->iter_pose[lane] = pn;
-            s_T[lane] = (float)pn;
-            st->iter_T[lane] = s_T[lane];
-          }
-          double cn = 0.0;
-          if (lane < 3) {
-            // the centred row's centre; the tail turns the last row into the world form
-            st->iter_ccenter[lane] = s_cd[lane];
-            // next centre: this iteration's centroid of the valid points
-            cn = nvalid > 0 ? s_sums[29 + lane] / nvalid : s_cd[lane];
-            st->iter_center[lane] = cn;
-            s_c[lane] = (float)cn;
-            st->iter_cf[lane] = s_c[lane];
-          }
-          __syncwarp();
-          if (lane < 3) s_cd[lane] = cn;
-          __syncwarp();
-          if (a.same_pixel && lane == 0) {
-            make_float_mats(a, s_pose, s_ray, s_T, s_V);
-            for (int k = 0; k < 16; ++k) st->iter_V[k] = s_V[k];
-          }
-        }
-        kf_grid_release(st);
-      } else {
-        ok = kf_grid_wait(st, &s_gen, &s_flag);
-        if (ok) {
-          if (tid < 16) {
-            s_pose[tid] = __ldcg(&st->iter_pose[tid]);
-            s_T[tid] = __ldcg(&st->iter_T[tid]);
-            if (a.same_pixel) s_V[tid] = __ldcg(&st->iter_V[tid]);
-          } else if (tid == 16) {
-            s_conv = __ldcg(&st->iter_conv);
-          } else if (tid < 20) {
-            s_cd[tid - 17] = __ldcg(&st->iter_center[tid - 17]);
-            s_c[tid - 17] = __ldcg(&st->iter_cf[tid - 17]);
-          }
+        if (lane < 8) {
+          s_red[warp][4 * lane + 0] = s0;
+          s_red[warp][4 * lane + 1] = s1;
+          s_red[warp][4 * lane + 2] = s2;
+          s_red[warp][4 * lane + 3] = s3;
         }
       }
-      if (!ok) break;
+      __syncthreads();
+      if (tid < 32) {
+        double v = 0.0;
+#pragma unroll
+        for (int r = 0; r < kWarps; ++r) v += s_red[r][tid];
+        s_sums[tid] = v;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        // ---- solve, lane-parallel in warp 0 ----
+        // reduce.cs counts every pixel of the (group-7) rows in sums[28]
+        const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
+        const double nvalid = s_sums[28];
+        const double cx = s_cd[0], cy = s_cd[1], cz = s_cd[2];
+        double xp[6];
+        kf_cholesky6_warp(&s_sums[7], &s_sums[1], xp, lane);
+        // back to the reference's variables: w = w', t = t' - w x c
+        double x[6];
+        x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
+        x[0] = xp[0] - (x[4] * cz - x[5] * cy);
+        x[1] = xp[1] - (x[5] * cx - x[3] * cz);
+        x[2] = xp[2] - (x[3] * cy - x[4] * cx);
+        // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2 (gFusion.cpp:700-703);
+        // lanes 0..2 evaluate the three sincos at once
+        double sn, cs;
+        kf_sincos_step(lane == 0 ? x[3] : (lane == 1 ? x[4] : x[5]), &sn, &cs);
+        const double sa = __shfl_sync(0xffffffffu, sn, 0), ca = __shfl_sync(0xffffffffu, cs, 0);
+        const double sb = __shfl_sync(0xffffffffu, sn, 1), cb = __shfl_sync(0xffffffffu, cs, 1);
+        const double sc = __shfl_sync(0xffffffffu, sn, 2), cc = __shfl_sync(0xffffffffu, cs, 2);
+        double R[9];
+        kf_euler_xyz_from_sincos(sa, ca, sb, cb, sc, cc, R);
+        // pose = delta * pose, one element per lane (delta column-major: R | x0..2)
+        double pn = 0.0;
+        if (lane < 16) {
+          const int r = lane & 3, col = lane >> 2;
+          // row r of delta, selected without indexing registers by lane
+          const double d0 = r == 0 ? R[0] : (r == 1 ? R[1] : (r == 2 ? R[2] : 0.0));
+          const double d1 = r == 0 ? R[3] : (r == 1 ? R[4] : (r == 2 ? R[5] : 0.0));
+          const double d2 = r == 0 ? R[6] : (r == 1 ? R[7] : (r == 2 ? R[8] : 0.0));
+          const double d3 = r == 0 ? x[0] : (r == 1 ? x[1] : (r == 2 ? x[2] : 1.0));
+          pn += d0 * s_pose[col * 4 + 0];
+          pn += d1 * s_pose[col * 4 + 1];
+          pn += d2 * s_pose[col * 4 + 2];
+          pn += d3 * s_pose[col * 4 + 3];
+        }
+        // the centred row and its centre; the tail turns the last one into the world form
+        if (lane < 28) s_csums[lane] = s_sums[lane];
+        if (lane == 28) s_csums[28] = count;
+        if (lane == 29) {
+          const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] +
+                                  x[4] * x[4] + x[5] * x[5]);
+          s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
+        }
+        if (lane == 30) s_ae = sqrt(s_sums[0] / count);  // getReduction :1167
+        // next centre: this iteration's centroid of the valid points
+        const double cn = lane < 3 ? (nvalid > 0 ? s_sums[29 + lane] / nvalid : s_cd[lane]) : 0.0;
+        __syncwarp();
+        if (lane < 16) {
+          s_pose[lane] = pn;
+          s_T[lane] = (float)pn;
+        }
+        if (lane < 3) {
+          s_ccenter[lane] = s_cd[lane];
+          s_cd[lane] = cn;
+          s_c[lane] = (float)cn;
+        }
+        __syncwarp();
+        if (a.same_pixel && lane == 0) make_float_mats(a, s_pose, s_ray, s_T, s_V);
+      }
+      ++gi;
       __syncthreads();
       ++iters_run;
       if (s_conv) break;  // result.norm() < 1e-5 && != 0 leaves this level (:707-708)
@@ -449,14 +430,13 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
 
   // ---------------- Track() tail (:715-723) + frame policy, block 0 only -----------------
   if (blockIdx.x != 0 || tid != 0 || !ok) return;
-  const double ae = iters_run ? __ldcg(&st->ae) : 0.0;
+  const double ae = iters_run ? s_ae : 0.0;
+  st->ae = ae;
   if (iters_run) {
     // the last reduction row in the reference's world form: b = M b', C = M C' M^T,
     // M = [[I, 0], [[c]x, I]]
-    double cs[29];
-    for (int k = 0; k < 29; ++k) cs[k] = __ldcg(&st->iter_csums[k]);
-    const double cx = __ldcg(&st->iter_ccenter[0]), cy = __ldcg(&st->iter_ccenter[1]),
-                 cz = __ldcg(&st->iter_ccenter[2]);
+    const double* cs = s_csums;
+    const double cx = s_ccenter[0], cy = s_ccenter[1], cz = s_ccenter[2];
     double Cp[36], Mx[36], MC[36];
     kf_make_jtj(&cs[7], Cp);
     for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;

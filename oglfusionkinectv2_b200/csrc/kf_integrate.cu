@@ -15,7 +15,8 @@
 // half-spaces returns at once, so voxels that cannot project into the image cost nothing;
 // inside, every voxel runs the reference's tests.  Per voxel one reciprocal replaces the
 // shader's divisions by z (u = fx * x/z + cx + 0.5 is the reference's (fx x + cx z)/z + 0.5
-// up to rounding).  The weight plane is read only where eta > -mu, and a voxel whose
+// up to rounding), and the reciprocal, square root and running-average division use the
+// hardware approximations (2 ulp; GLSL allows 2.5 ulp for division).  The weight plane is read only where eta > -mu, and a voxel whose
 // encoded value and weight do not change is not written back.
 #include "kf_internal.cuh"
 
@@ -49,26 +50,26 @@ constexpr int kZC = 16;  // voxels per thread along z
 // True when the box of voxel centres [b0, b1] (index space, inclusive) lies entirely on the
 // outside of one of the five half-spaces whose intersection is the set of voxels
 // integrate.cs can touch: z >= 1e-4, 0 <= u <= W-1, 0 <= v <= H-1 (u, v the +0.5-rounded
-// projection).  Conservative: a box that is not culled is tested voxel by voxel.
+// projection).  Conservative: a box that is not culled is tested voxel by voxel.  Called by
+// a whole warp: lane & 7 evaluates one corner, the ballots combine them.
 __device__ bool box_outside_frustum(const IntArgs& a, const float* inv, const int* b0, const int* b1) {
   const float vx = a.dimx / a.nx, vy = a.dimy / a.ny, vz = a.dimz / a.nz;
   const float kx0 = a.cx + 0.5f, kx1 = a.cx + 0.5f - (float)(a.W - 1);
   const float ky0 = a.cy + 0.5f, ky1 = a.cy + 0.5f - (float)(a.H - 1);
-  bool all_out[5] = {true, true, true, true, true};
-  for (int c = 0; c < 8; ++c) {
-    const float wx = ((c & 1 ? b1[0] : b0[0]) + 0.5f) * vx;
-    const float wy = ((c & 2 ? b1[1] : b0[1]) + 0.5f) * vy;
-    const float wz = ((c & 4 ? b1[2] : b0[2]) + 0.5f) * vz;
-    const float X = inv[0] * wx + inv[1] * wy + inv[2] * wz + inv[3];
-    const float Y = inv[4] * wx + inv[5] * wy + inv[6] * wz + inv[7];
-    const float Z = inv[8] * wx + inv[9] * wy + inv[10] * wz + inv[11];
-    all_out[0] &= Z - 1e-4f < 0.0f;
-    all_out[1] &= a.fx * X + kx0 * Z < 0.0f;
-    all_out[2] &= -(a.fx * X + kx1 * Z) < 0.0f;
-    all_out[3] &= a.fy * Y + ky0 * Z < 0.0f;
-    all_out[4] &= -(a.fy * Y + ky1 * Z) < 0.0f;
-  }
-  return all_out[0] || all_out[1] || all_out[2] || all_out[3] || all_out[4];
+  const int c = threadIdx.x & 7;
+  const float wx = ((c & 1 ? b1[0] : b0[0]) + 0.5f) * vx;
+  const float wy = ((c & 2 ? b1[1] : b0[1]) + 0.5f) * vy;
+  const float wz = ((c & 4 ? b1[2] : b0[2]) + 0.5f) * vz;
+  const float X = inv[0] * wx + inv[1] * wy + inv[2] * wz + inv[3];
+  const float Y = inv[4] * wx + inv[5] * wy + inv[6] * wz + inv[7];
+  const float Z = inv[8] * wx + inv[9] * wy + inv[10] * wz + inv[11];
+  const unsigned o0 = __ballot_sync(0xffffffffu, Z - 1e-4f < 0.0f);
+  const unsigned o1 = __ballot_sync(0xffffffffu, a.fx * X + kx0 * Z < 0.0f);
+  const unsigned o2 = __ballot_sync(0xffffffffu, -(a.fx * X + kx1 * Z) < 0.0f);
+  const unsigned o3 = __ballot_sync(0xffffffffu, a.fy * Y + ky0 * Z < 0.0f);
+  const unsigned o4 = __ballot_sync(0xffffffffu, -(a.fy * Y + ky1 * Z) < 0.0f);
+  return (o0 & 0xffu) == 0xffu || (o1 & 0xffu) == 0xffu || (o2 & 0xffu) == 0xffu ||
+         (o3 & 0xffu) == 0xffu || (o4 & 0xffu) == 0xffu;
 }
 
 // The z-chunk [zb, zb + kZC) of column (x, y); returns which z-bricks received a negative
@@ -101,7 +102,7 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
     const float fk = (float)k;
     const float pz = fmaf(fk, dz[2], p0[2]);
     if (pz < 0.0001f) continue;
-    const float iz = 1.0f / pz;
+    const float iz = __fdividef(1.0f, pz);  // hardware reciprocal (2 ulp)
     const float rx = fmaf(fk, dz[0], p0[0]) * iz;  // pos.x / pos.z
     const float ry = fmaf(fk, dz[1], p0[1]) * iz;
     // cameraX.x / cameraX.z + 0.5 = fx * x/z + cx + 0.5 (K has no skew, :67)
@@ -110,14 +111,15 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
     if (u < 0.0f || u > fW1 || v < 0.0f || v > fH1) continue;
     const float d = __ldg(a.depth + (uint32_t)(int)v * (uint32_t)a.W + (uint32_t)(int)u) * 0.001f;
     if (d == 0.0f) continue;
-    const float diff = (d - pz) * sqrtf(fmaf(rx, rx, fmaf(ry, ry, 1.0f)));
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, 1.0f));
+    const float diff = (d - pz) * (r2 * rsqrtf(r2));  // sqrt(r2), r2 >= 1
     if (diff > -a.mu) {
       const float sdf = fminf(1.0f, diff * a.inv_mu);
       const V oldv = vf[idx];
       const Wt oldw = vw[idx];
       const float F = Vox<S>::raw_nc(&oldv, 0) * Vox<S>::kRawToF;
       const float w = Vox<S>::weight(&oldw, 0);
-      const float wd = (w * F + sdf) / (w + 1.0f);
+      const float wd = __fdividef(fmaf(w, F, sdf), w + 1.0f);
       float nF, nw;
       if (!a.band) {
         // the reference's earlier update (integrate.cs:115-150)
@@ -158,11 +160,12 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a) {
 #pragma unroll
   for (int k = 0; k < 12; ++k) inv[k] = a.st->inv_rows[k];
   const int xb = blockIdx.x * 32, yb = blockIdx.y * 8, zb = blockIdx.z * kZC;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
+  if (threadIdx.y == 0) {
     // one voxel of margin on every side absorbs the rounding of the per-voxel tests
     const int b0[3] = {xb - 1, yb - 1, zb - 1};
     const int b1[3] = {xb + 32, yb + 8, zb + kZC};
-    s_cull = box_outside_frustum(a, inv, b0, b1) ? 1 : 0;
+    const bool out = box_outside_frustum(a, inv, b0, b1);
+    if (threadIdx.x == 0) s_cull = out ? 1 : 0;
   }
   {
     const int t = threadIdx.y * 32 + threadIdx.x;

@@ -50,19 +50,7 @@ struct KfDevState {
   unsigned barrier_count;
   unsigned barrier_gen;
   int pad0_;
-  // hand-over between iterations of the persistent tracking kernels
-  double iter_pose[16]; // pose after the last solve (ICP) / camera-to-world (SDF)
-  double iter_result[6];// SDF twist accumulator
-  double iter_center[3];// ICP accumulation centre for the next iteration (world)
-  double iter_csums[32];// centred reduction row of the last ICP iteration
-  double iter_ccenter[3];// centre that row was accumulated about
-  float iter_T[16];     // FP32 pose for the next iteration (published by the last block)
-  float iter_V[16];     // FP32 view = K * inverse(.) for the next iteration
-  float iter_cf[3];     // FP32 centre for the next iteration
-  int pad1_;
   double icp_center_cam[3];  // ICP centre at the end of the last frame (camera frame)
-  int iter_conv;        // convergence flag of the last solve
-  int pad_[3];
   double lib_pose[KF_MAX_LIBRARY][16];  // pose library
 };
 // Bytes of KfDevState the host reads after a frame step (pose and result flags).
@@ -99,7 +87,7 @@ struct kf_session {
   float4* d_ref_vertex = nullptr;
   float4* d_ref_normal = nullptr;
   float* d_sdf_rows = nullptr;  // persistent trackSDF rows, 8 floats per level-0 pixel
-  float* d_partials = nullptr;  // [2][KF_MAX_TRACK_BLOCKS][32]
+  float* d_partials = nullptr;  // [2][KF_MAX_TRACK_BLOCKS][32] (alternating by iteration)
 
   KfDevState* d_state = nullptr;
   KfDevState* h_state = nullptr;  // pinned mirror
@@ -375,10 +363,46 @@ __host__ __device__ inline void kf_make_jtj(const double* v21, double* C) {
     }
 }
 
+// 1 / sqrt(d) to FP64 precision without a divide or square root: an FP32 estimate refined
+// by two Newton-Raphson steps for f(y) = 1/y^2 - d, y <- y (3 - d y^2) / 2; each step
+// roughly doubles the correct bits (22 -> 44 -> FP64 rounding).  Outside FP32's normal
+// range the estimate comes from 1 / sqrt(d) directly.
+__device__ __forceinline__ double kf_rsqrt_newton(double d) {
+  double y = (d > 1e-30 && d < 1e30) ? (double)rsqrtf((float)d) : 1.0 / sqrt(d);
+  const double h = 0.5 * d;
+  y = y * fma(-h * y, y, 1.5);
+  y = y * fma(-h * y, y, 1.5);
+  return y;
+}
+
+// sin and cos; below |x| = 0.25 by their Taylor series through x^11 and x^12 (the first
+// omitted terms are < 3e-18 relative), which is the whole range of a Gauss-Newton step.
+__device__ __forceinline__ void kf_sincos_step(double x, double* s, double* c) {
+  if (fabs(x) < 0.25) {
+    const double x2 = x * x;
+    double ps = -1.0 / 39916800.0;                 // -1/11!
+    ps = fma(ps, x2, 1.0 / 362880.0);              //  1/9!
+    ps = fma(ps, x2, -1.0 / 5040.0);               // -1/7!
+    ps = fma(ps, x2, 1.0 / 120.0);                 //  1/5!
+    ps = fma(ps, x2, -1.0 / 6.0);                  // -1/3!
+    double pc = 1.0 / 479001600.0;                 //  1/12!
+    pc = fma(pc, x2, -1.0 / 3628800.0);            // -1/10!
+    pc = fma(pc, x2, 1.0 / 40320.0);               //  1/8!
+    pc = fma(pc, x2, -1.0 / 720.0);                // -1/6!
+    pc = fma(pc, x2, 1.0 / 24.0);                  //  1/4!
+    pc = fma(pc, x2, -0.5);                        // -1/2!
+    *s = fma(x * x2, ps, x);
+    *c = fma(x2, pc, 1.0);
+  } else {
+    sincos(x, s, c);
+  }
+}
+
 // kf_cholesky6 for one warp: C given as the 21 upper-triangular values of reduce.cs rows
 // 7..27 (row-major), b as 6 values, both in shared or global memory read by every lane.
 // Lane i < 6 factors row i; every lane returns the whole solution in x (zero when C is
-// not numerically positive definite, as kf_cholesky6).
+// not numerically positive definite, as kf_cholesky6).  The pivots' reciprocals come from
+// kf_rsqrt_newton, so the dependent chain holds multiplies and shuffles, no divides.
 __device__ inline void kf_cholesky6_warp(const double* v21, const double* b, double* x, int lane) {
   auto at = [&](int i, int j) {
     if (i > j) { const int t = i; i = j; j = t; }
@@ -386,7 +410,7 @@ __device__ inline void kf_cholesky6_warp(const double* v21, const double* b, dou
   };
   const int i = lane < 6 ? lane : 5;
   double row[6], Lrow[6], Lcol[6];
-  double dmax = 0.0;
+  double dmax = 0.0, inv_diag = 0.0;  // inv_diag: 1 / L_ii of this lane's row
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
     row[j] = at(i, j);
@@ -400,10 +424,13 @@ __device__ inline void kf_cholesky6_warp(const double* v21, const double* b, dou
   for (int j = 0; j < 6; ++j) {
     const double d = __shfl_sync(0xffffffffu, row[j], j);  // C_jj - sum_k L_jk^2
     if (!(d > eps)) { spd = false; break; }                 // uniform: d is broadcast
-    const double ljj = sqrt(d);
-    const double lij = lane == j ? ljj : (lane > j ? row[j] / ljj : 0.0);
+    const double r = kf_rsqrt_newton(d);                    // 1 / L_jj
+    const double lij = lane == j ? d * r : (lane > j ? row[j] * r : 0.0);
     Lrow[j] = lij;
-    if (lane == j) Lcol[j] = ljj;
+    if (lane == j) {
+      Lcol[j] = lij;
+      inv_diag = r;
+    }
 #pragma unroll
     for (int k = j + 1; k < 6; ++k) {
       const double lkj = __shfl_sync(0xffffffffu, lij, k);
@@ -420,13 +447,13 @@ __device__ inline void kf_cholesky6_warp(const double* v21, const double* b, dou
   double y = b[i];
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    if (lane == k) y = y / Lrow[k];
+    if (lane == k) y = y * inv_diag;
     const double yk = __shfl_sync(0xffffffffu, y, k);
     if (lane > k) y = fma(-Lrow[k], yk, y);
   }
 #pragma unroll
   for (int k = 5; k >= 0; --k) {
-    if (lane == k) y = y / Lcol[k];
+    if (lane == k) y = y * inv_diag;
     const double xk = __shfl_sync(0xffffffffu, y, k);
     if (lane < k) y = fma(-Lcol[k], xk, y);
   }
@@ -435,53 +462,29 @@ __device__ inline void kf_cholesky6_warp(const double* v21, const double* b, dou
 }
 
 // ---------------------------------------------------------------------------------------
-// Grid hand-over for the persistent (cooperatively launched) tracking kernels.
-// kf_grid_arrive: every block calls it after writing its partial sums; it returns true
-// in exactly one block (the last to arrive), which then reduces, solves and calls
-// kf_grid_release.  The other blocks wait in kf_grid_wait.  Every wait is bounded: after
-// KF_BARRIER_SPIN_CYCLES the block records KF_DEV_ERR_TIMEOUT in st->error and stops;
-// callers leave their loops when kf_grid_wait returns false.
+// Grid barrier for the persistent (cooperatively launched) tracking kernels: every block
+// calls kf_grid_sync after writing its partial sums and continues once all have.  Every
+// wait is bounded: after KF_BARRIER_SPIN_CYCLES the block records KF_DEV_ERR_TIMEOUT in
+// st->error and stops; callers leave their loops when kf_grid_sync returns false, and a
+// block that sees another block's error stops too.
 __device__ __forceinline__ unsigned kf_ld_acquire_gpu(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 
-__device__ __forceinline__ unsigned kf_ld_relaxed_gpu(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// The bar.sync before thread 0's gpu-scope release (or acq_rel) orders every thread's
-// earlier stores of the block before it; an acquirer that observes the release sees them.
-__device__ inline bool kf_grid_arrive(KfDevState* st, unsigned nblocks, unsigned* s_gen,
-                                      int* s_last) {
+// The bar.sync before thread 0's gpu-scope release orders every thread's earlier stores
+// of the block before it; an acquirer that observes the release sees them.
+// Grid barrier over barrier_count, which only grows during a launch (the launcher zeroes
+// it): every block adds one and waits until `target` arrivals in total.  One release
+// reduction per block and no reset step; bounded like kf_grid_wait.
+__device__ inline bool kf_grid_sync(KfDevState* st, unsigned target, int* s_flag) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    // the generation cannot advance before this block has arrived
-    *s_gen = kf_ld_relaxed_gpu(&st->barrier_gen);
-    unsigned old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(&st->barrier_count) : "memory");
-    *s_last = (old + 1u == nblocks);
-  }
-  __syncthreads();
-  return *s_last != 0;
-}
-
-__device__ inline void kf_grid_release(KfDevState* st) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(&st->barrier_count) : "memory");
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&st->barrier_gen) : "memory");
-  }
-}
-
-__device__ inline bool kf_grid_wait(KfDevState* st, const unsigned* s_gen, int* s_flag) {
-  if (threadIdx.x == 0) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&st->barrier_count) : "memory");
     int ok = 1;
     const long long t0 = clock64();
-    while (kf_ld_acquire_gpu(&st->barrier_gen) == *s_gen) {
+    while (kf_ld_acquire_gpu(&st->barrier_count) < target) {
       if (*(volatile int*)&st->error) { ok = 0; break; }
       if (clock64() - t0 > KF_BARRIER_SPIN_CYCLES) {
         atomicExch(&st->error, KF_DEV_ERR_TIMEOUT);

@@ -279,6 +279,13 @@ int ensure(kf_session* s, void** p, size_t* cap, size_t bytes) {
   return KF_OK;
 }
 
+// Bytes for the vertex buffer: the vertices needed now, but at least room for one triangle
+// per 256 cubes (a fused scene's surface is about one triangle per 600 cubes), so a mesh
+// that grows as frames are fused rarely reallocates.
+size_t vertex_bytes(size_t ncube, size_t nverts) {
+  return std::max<size_t>(16, std::max(nverts, ncube / 256 * 3) * 16);
+}
+
 int histopyramid(kf_session* s, float iso, uint32_t* n_tri) {
   const int nx = s->cfg.nx, ny = s->cfg.ny, nz = s->cfg.nz;
   int P = 1, top = 0;
@@ -333,7 +340,7 @@ int histopyramid(kf_session* s, float iso, uint32_t* n_tri) {
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_u32_scalar, s->d_mc_levels[top], 4, cudaMemcpyDeviceToHost, s->stream));
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   const uint32_t T = s->h_u32_scalar[0];
-  int rc = ensure(s, (void**)&s->d_mc_vertices, &s->mc_vertex_cap, std::max<size_t>(1, (size_t)T * 3 * 16));
+  int rc = ensure(s, (void**)&s->d_mc_vertices, &s->mc_vertex_cap, vertex_bytes(ncube, (size_t)T * 3));
   if (rc) return rc;
   // device copy of the level pointer table
   std::vector<uint32_t*> host_levels(s->d_mc_levels);
@@ -408,7 +415,7 @@ int classic(kf_session* s, float iso, uint32_t* n_tri) {
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_u32_scalar, d_tot, 4, cudaMemcpyDeviceToHost, s->stream));
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   const uint32_t nverts = s->h_u32_scalar[0];
-  rc = ensure(s, (void**)&s->d_mc_vertices, &s->mc_vertex_cap, std::max<size_t>(1, (size_t)nverts * 16));
+  rc = ensure(s, (void**)&s->d_mc_vertices, &s->mc_vertex_cap, vertex_bytes((size_t)s->cfg.nx * s->cfg.ny * s->cfg.nz, (size_t)nverts));
   if (rc) return rc;
   a.out = s->d_mc_vertices;
   switch (s->cfg.storage) {

@@ -16,8 +16,8 @@
 // FP64; camToWorld = exp(Twist(result)) * m_pose_eig_prev.
 //
 // B200 design: like kf_icp.cu, one cooperative launch holds every level and iteration;
-// the last block to arrive reduces the per-block rows in a fixed order in FP64 and
-// solves.  In recover mode the same launch walks the pose library (recoverPose) and
+// after a grid barrier every block reduces the per-block rows in the same fixed order in
+// FP64 and solves the same system.  In recover mode the same launch walks the pose library (recoverPose) and
 // stops at the first pose that tracks.  The persistent row buffer is only written at
 // indices that some level reads back as its stale last column.
 #include "kf_internal.cuh"
@@ -103,8 +103,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
   __shared__ float s_warp[kWarps][28];
   __shared__ double s_red[kWarps][32];
   __shared__ double s_sums[32];
-  __shared__ unsigned s_gen;
-  __shared__ int s_last, s_flag, s_conv;
+  __shared__ int s_flag, s_conv;
 
   KfDevState* st = a.st;
   if (a.gate && *(volatile const int*)a.gate == 0) return;  // uniform over the grid
@@ -116,6 +115,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
 
   bool ok = true, found = false;
   int iters_run = 0;
+  unsigned gi = 0;  // iterations of this launch so far: grid barrier target and partials buffer
   for (int attempt = 0; attempt < attempts && ok && !found; ++attempt) {
     if (tid < 6) s_result[tid] = 0.0;
     if (tid < 16) s_T[tid] = (float)s_prev[tid];  // exp(0) * prev
@@ -164,70 +164,71 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
           for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
           if (lane == 0) s_warp[warp][k] = v;
         }
+        // two partial buffers, alternating by iteration (see kf_icp.cu)
+        float* part = a.partials + (size_t)(gi & 1u) * KF_MAX_TRACK_BLOCKS * 32;
         __syncthreads();
         if (tid < 28) {
           float v = 0.0f;
 #pragma unroll
           for (int w = 0; w < kWarps; ++w) v += s_warp[w][tid];
-          a.partials[(size_t)blockIdx.x * 32 + tid] = v;
+          part[(size_t)blockIdx.x * 32 + tid] = v;
         }
 
-        if (kf_grid_arrive(st, nb, &s_gen, &s_last)) {
-          {
-            const int k = tid & 31, r = tid >> 5;
-            double v = 0.0;
-            if (k < 28)
-              for (unsigned b = r; b < nb; b += kWarps) v += (double)__ldcg(&a.partials[(size_t)b * 32 + k]);
-            s_red[r][k] = v;
-          }
-          __syncthreads();
-          if (tid < 32) {
-            double v = 0.0;
+        // grid barrier; then every block reduces the rows in the same fixed order and
+        // solves the same system, so every block holds bit-identical results
+        ok = kf_grid_sync(st, nb * (gi + 1u), &s_flag);
+        if (!ok) break;
+        ++gi;
+        {
+          const int k = tid & 31, r = tid >> 5;
+          double v = 0.0;
+          if (k < 28)
+            for (unsigned b = r; b < nb; b += kWarps) v += (double)__ldcg(&part[(size_t)b * 32 + k]);
+          s_red[r][k] = v;
+        }
+        __syncthreads();
+        if (tid < 32) {
+          double v = 0.0;
 #pragma unroll
-            for (int r = 0; r < kWarps; ++r) v += s_red[r][tid];
-            s_sums[tid] = v;
+          for (int r = 0; r < kWarps; ++r) v += s_red[r][tid];
+          s_sums[tid] = v;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
+          s_sums[28] = count;
+          s_sums[29] = s_sums[30] = s_sums[31] = 0.0;
+          double b[6], C[36], dx[6];
+          for (int k = 0; k < 6; ++k) b[k] = s_sums[1 + k];
+          kf_make_jtj(&s_sums[7], C);
+          const double ae = sqrt(s_sums[0] / count);
+          double mx = C[0];
+          for (int k = 1; k < 36; ++k) mx = fmax(mx, C[k]);  // maxCoeff (:890)
+          const double scaling = 1.0 / mx;
+          for (int k = 0; k < 36; ++k) C[k] *= scaling;
+          for (int k = 0; k < 6; ++k) b[k] *= scaling;
+          for (int k = 0; k < 6; ++k) C[k * 7] += (double)it * 0.01;
+          kf_ldlt6(C, b, dx);
+          double cn = 0.0;
+          for (int k = 0; k < 6; ++k) {
+            const double prev = s_result[k];
+            const double res = prev - dx[k];
+            const double ch = res - prev;
+            cn += ch * ch;
+            s_result[k] = res;
           }
-          __syncthreads();
-          if (tid == 0) {
-            const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
-            s_sums[28] = count;
-            s_sums[29] = s_sums[30] = s_sums[31] = 0.0;
-            double b[6], C[36], dx[6];
-            for (int k = 0; k < 6; ++k) b[k] = s_sums[1 + k];
-            kf_make_jtj(&s_sums[7], C);
-            const double ae = sqrt(s_sums[0] / count);
-            double mx = C[0];
-            for (int k = 1; k < 36; ++k) mx = fmax(mx, C[k]);  // maxCoeff (:890)
-            const double scaling = 1.0 / mx;
-            for (int k = 0; k < 36; ++k) C[k] *= scaling;
-            for (int k = 0; k < 6; ++k) b[k] *= scaling;
-            for (int k = 0; k < 6; ++k) C[k * 7] += (double)it * 0.01;
-            kf_ldlt6(C, b, dx);
-            double res[6], cn = 0.0;
-            for (int k = 0; k < 6; ++k) {
-              const double prev = s_result[k];
-              res[k] = prev - dx[k];
-              const double ch = res[k] - prev;
-              cn += ch * ch;
-            }
-            cn = sqrt(cn);
-            double E[16], Tn[16];
-            kf_se3_exp(res, E);
-            kf_mat4_mul(E, s_prev, Tn);
-            for (int k = 0; k < 16; ++k) st->iter_pose[k] = Tn[k];
-            for (int k = 0; k < 6; ++k) st->iter_result[k] = res[k];
-            st->iter_conv = ((ae != 0.0 && ae < 1e-3) || cn < 1e-3) ? 1 : 0;
+          cn = sqrt(cn);
+          double E[16], Tn[16], res[6];
+          for (int k = 0; k < 6; ++k) res[k] = s_result[k];
+          kf_se3_exp(res, E);
+          kf_mat4_mul(E, s_prev, Tn);
+          for (int k = 0; k < 16; ++k) s_T[k] = (float)Tn[k];
+          s_conv = ((ae != 0.0 && ae < 1e-3) || cn < 1e-3) ? 1 : 0;
+          if (blockIdx.x == 0) {
             st->ae = ae;
             for (int k = 0; k < 32; ++k) st->sums[k] = s_sums[k];
           }
-          kf_grid_release(st);
-        } else {
-          ok = kf_grid_wait(st, &s_gen, &s_flag);
         }
-        if (!ok) break;
-        if (tid < 16) s_T[tid] = (float)__ldcg(&st->iter_pose[tid]);
-        if (tid < 6) s_result[tid] = __ldcg(&st->iter_result[tid]);
-        if (tid == 16) s_conv = __ldcg(&st->iter_conv);
         __syncthreads();
         ++iters_run;
         if (s_conv) {
