@@ -18,6 +18,7 @@ this host's cores for the same workload.
 from __future__ import annotations
 
 import argparse
+import glob
 import faulthandler
 import json
 import os
@@ -134,6 +135,19 @@ class ClockSampler:
         s = sorted(self.samples)
         return {"sm_mhz": s[len(s) // 2] if s else None, "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(self.reasons), "samples": len(s)}
+
+
+def measured_traffic(workload: str, stage: str):
+    """DRAM bytes (read + write) per launch of the stage's kernel from the committed ncu capture
+    of this workload (profiles/*_traffic.txt: "<kernel> <workload> dram_bytes_per_launch <n>"),
+    or None when none was captured."""
+    kernel = {"integrate": "integrate_kernel", "raycast": "raycast_kernel"}.get(stage)
+    for path in glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "*_traffic.txt")):
+        for line in open(path):
+            f = line.split()
+            if len(f) == 4 and f[0] == kernel and f[1] == workload and f[2] == "dram_bytes_per_launch":
+                return int(f[3])
+    return None
 
 
 def measured_peak_hbm():
@@ -344,7 +358,8 @@ def main():
             "stage_ms": per, "stage_frames": stage_frames,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak if achieved else None),
-                         "peak_source": peak_kind, "algorithmic_bytes": algo, "traffic": None},
+                         "peak_source": peak_kind, "algorithmic_bytes": algo,
+                         "traffic": measured_traffic(w.name, dom)},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "tracked_last": bool(tracked_ok),
