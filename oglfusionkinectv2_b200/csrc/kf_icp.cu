@@ -6,12 +6,15 @@
 //
 // B200 design: ONE cooperative (co-resident) launch runs every pyramid level and every
 // Gauss-Newton iteration of a frame.  Per iteration each block associates its pixels
-// (same-pixel projective association at level-0 resolution), accumulates the 27 sums of
-// reduce.cs, and writes one partial row; the last block to arrive reduces the rows in a
-// fixed order in FP64, solves the 6x6 system by FP64 Cholesky, composes the pose in FP64
-// and releases the others.  No host round trip per iteration (the reference maps the
-// SSBO back every iteration, :1131-1134), no launch per iteration, deterministic sums.
-//
+// (same-pixel projective association at level-0 resolution) and adds the 27 sums of
+// reduce.cs, plus the valid count and the sum of the points, to the session's rows as
+// fixed-point integers (value * 2^32, 64-bit atomics: exact, so the total does not depend
+// on the order or on how the pixels were split among blocks); after a grid barrier every
+// block reads the rows, solves the 6x6 system in FP64 and composes the pose in FP64.  No
+// host round trip per iteration (the reference maps the SSBO back every iteration,
+// :1131-1134), no launch per iteration, deterministic sums.  A batched launch gives each
+// session its own group of blocks, rows and barrier.
+
 // Conditioning: J = [n, p x n] with world p couples rotation and translation strongly
 // (lever arms of metres), so FP32 partial sums lose the small eigen-directions of J^T J.
 // The sums are therefore accumulated with the lever arm taken about a centre c (the
@@ -20,11 +23,15 @@
 // is C = M C' M^T, b = M b', and its solution is t = t' - w x c for the same w.  The
 // reported reduction row is the world form, as the reference's.
 //
-// J^T J contraction: KF_JTJ_FP32 uses FMAs; KF_JTJ_SPLIT_BF16 splits each feature of
-// f = [J'0..J'5, e, 0] into three bf16 terms (hi + mid + lo, 24 significant bits), stages
-// them feature-major per warp, and issues four mma.sync.m16n8k16 per 16 pixels
-// ([hi; mid] x hi, x mid, x lo, and [lo; 0] x hi) with FP32 accumulation: every bf16 x
-// bf16 product is exact in FP32 and only the lo*mid and lo*lo terms (~2^-24) are left out.
+// J^T J contraction: KF_JTJ_FP32 uses FMAs (per-thread FP32 sums, converted per block).
+// KF_JTJ_SPLIT_BF16 splits each feature of f = [J'0..J'5, e, 1] into three bf16 terms
+// (hi + mid + lo, 24 significant bits), stages them feature-major per warp, and issues four
+// mma.sync.m16n8k16 per 16 pixels ([hi; mid] x hi, x mid, x lo, and [lo; q] x hi, q = the
+// point's hi and mid terms) with FP32 accumulation: every bf16 x bf16 product is exact in
+// FP32 and only the lo*mid and lo*lo terms (~2^-24) are left out.  The constant feature 1
+// makes the valid count and the point sums (for the next centre) columns of the same
+// products.  Each warp converts its 32-pixel chunk's sums to fixed point, so a chunk
+// contributes the same bits whichever block, grid or batch processes it.
 #include "kf_internal.cuh"
 
 namespace {
@@ -44,9 +51,20 @@ struct IcpArgs {
   int same_pixel;         // Q4
   int frame_policy;
   int integrate_every;
-  float* partials;        // [gridDim.x][32]
   KfDevState* st;
 };
+
+// A batched launch: the blocks of entry e (one session each) are those whose map word
+// names e; every entry runs its own levels, iterations and grid barrier.
+struct IcpBatch {
+  const IcpArgs* args;        // per entry
+  const uint32_t* block_map;  // per block: entry << 24 | blocks of the entry << 12 | index
+};
+
+// Fixed-point scale of the reduction sums: |sum| < 2^31 for every row entry (the points
+// are within the distance threshold of the raycast surface, inside the volume).
+constexpr float kFix = 4294967296.0f;       // 2^32
+constexpr double kInvFix = 1.0 / 4294967296.0;
 
 // ---- track.cs:53-133 for one pixel ------------------------------------------------------
 // n, v: the pixel's normal and vertex (loaded one pass ahead by the caller)
@@ -120,26 +138,42 @@ __device__ __forceinline__ void make_float_mats(const IcpArgs& a, const double* 
 
 constexpr int kWarps = KF_TRACK_THREADS / 32;
 
-template <int JTJ>
-__global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
+template <int JTJ, bool BATCH>
+__global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one, IcpBatch batch) {
+  __shared__ IcpArgs s_args;
   __shared__ double s_pose[16];
   __shared__ double s_old[16];
   __shared__ double s_ray[16];
   __shared__ double s_cd[3];
   __shared__ float s_T[16], s_V[16], s_c[3];
-  __shared__ float s_warp[kWarps][64];
-  __shared__ float s_pw[kWarps][4];
-  __shared__ double s_red[kWarps][32];
+  __shared__ float s_warp[JTJ ? 1 : kWarps][28];
+  __shared__ float s_pw[JTJ ? 1 : kWarps][4];
+  __shared__ long long s_fix[JTJ ? kWarps : 1][72];
   __shared__ double s_sums[32];
   __shared__ double s_csums[29], s_ccenter[3], s_ae;  // last centred row (for the tail)
   __shared__ int s_flag, s_conv;
   __shared__ __align__(16) __nv_bfloat16 s_hi[JTJ ? kWarps : 1][8][40];
   __shared__ __align__(16) __nv_bfloat16 s_mid[JTJ ? kWarps : 1][8][40];
   __shared__ __align__(16) __nv_bfloat16 s_lo[JTJ ? kWarps : 1][8][40];
+  __shared__ __align__(16) __nv_bfloat16 s_q[JTJ ? kWarps : 1][8][40];
+
+  unsigned local, nb;  // this block's index among its entry's blocks, and their number
+  if constexpr (BATCH) {
+    const uint32_t m = batch.block_map[blockIdx.x];
+    local = m & 0xfffu;
+    nb = (m >> 12) & 0xfffu;
+    const int* src = reinterpret_cast<const int*>(batch.args + (m >> 24));
+    for (int k = threadIdx.x; k < (int)(sizeof(IcpArgs) / 4); k += blockDim.x)
+      reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
+    __syncthreads();
+  } else {
+    local = blockIdx.x;
+    nb = gridDim.x;
+  }
+  const IcpArgs& a = BATCH ? s_args : a_one;
 
   KfDevState* st = a.st;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const unsigned nb = gridDim.x;
 
   if (tid < 16) {
     s_pose[tid] = st->pose[tid];
@@ -160,7 +194,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
 
   bool ok = true;
   int iters_run = 0;
-  unsigned gi = 0;  // iterations of this launch so far: grid barrier target and partials buffer
+  unsigned gi = 0;  // iterations of this launch so far: grid barrier target and sum buffer
   for (int level = 2; level >= 0 && ok; --level) {
     const int Wl = a.W[level], Hl = a.H[level];
     const int P = Wl * Hl;
@@ -171,14 +205,17 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
       c[0] = s_c[0]; c[1] = s_c[1]; c[2] = s_c[2];
 
       // ---------------- track + accumulate ----------------
-      float acc[JTJ ? 4 : 28];
+      long long* accbuf = &a.st->icp_acc[gi % 3u][0];
+      float acc[JTJ ? 1 : 28];
 #pragma unroll
-      for (int k = 0; k < (JTJ ? 4 : 28); ++k) acc[k] = 0.0f;
-      float pacc[4] = {0.f, 0.f, 0.f, 0.f};  // valid count, sum of world points
+      for (int k = 0; k < (JTJ ? 1 : 28); ++k) acc[k] = 0.0f;
+      float pacc[4] = {0.f, 0.f, 0.f, 0.f};  // FP32 path: valid count, sum of world points
+      // split-BF16 path: fixed-point sums of M[g][2t], M[g][2t+1] and of q_g (lane g, t)
+      long long fx0 = 0, fx1 = 0, fxq = 0;
       const int stride = nb * KF_TRACK_THREADS;
       const float4* Nl = a.normal[level];
       const float4* Vl = a.vertex[level];
-      int base = (blockIdx.x * kWarps + warp) * 32;
+      int base = (local * kWarps + warp) * 32;
       // the next pass's normal and vertex are in flight while this pass gathers the
       // reference maps
       float4 nn = make_float4(2.0f, 0.f, 0.f, 0.f), vn = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -202,14 +239,12 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
           if (a.q1 && ((i / Wl) & 7) != 7) status = 0;  // only work group 7 reaches the solver
         }
         const bool use = status == 1;
-        if (use) {
-          pacc[0] += 1.0f;
-          pacc[1] += pw[0];
-          pacc[2] += pw[1];
-          pacc[3] += pw[2];
-        }
         if constexpr (JTJ == 0) {
           if (use) {
+            pacc[0] += 1.0f;
+            pacc[1] += pw[0];
+            pacc[2] += pw[1];
+            pacc[3] += pw[2];
             const float e = f[6];
             acc[0] += e * e;
 #pragma unroll
@@ -221,10 +256,11 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
               for (int cc = r; cc < 6; ++cc) acc[q++] += f[r] * f[cc];
           }
         } else {
-          // stage f = [J'0..J'5, e, 0] as hi + mid + lo bf16, feature-major per warp
+          // stage f = [J'0..J'5, e, 1] as hi + mid + lo bf16 and q = [hi(p), mid(p), 0, 0]
+          // feature-major per warp (zero for pixels that are not used)
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
-            const float v = (use && k < 7) ? f[k] : 0.0f;
+            const float v = use ? (k < 7 ? f[k] : 1.0f) : 0.0f;
             const __nv_bfloat16 hi = __float2bfloat16_rn(v);
             const float r1 = v - __bfloat162float(hi);
             const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
@@ -233,8 +269,18 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
             s_mid[warp][k][lane] = mid;
             s_lo[warp][k][lane] = lo;
           }
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const float p = use ? pw[k] : 0.0f;
+            const __nv_bfloat16 hi = __float2bfloat16_rn(p);
+            s_q[warp][k][lane] = hi;
+            s_q[warp][3 + k][lane] = __float2bfloat16_rn(p - __bfloat162float(hi));
+          }
+          s_q[warp][6][lane] = __float2bfloat16_rn(0.0f);
+          s_q[warp][7][lane] = __float2bfloat16_rn(0.0f);
           __syncwarp();
           const int g = lane >> 2, t = lane & 3;
+          float cA[4] = {0.f, 0.f, 0.f, 0.f}, cB[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int c0 = 16 * h + 2 * t;
@@ -244,28 +290,32 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
             const uint32_t m1 = *reinterpret_cast<const uint32_t*>(&s_mid[warp][g][c0 + 8]);
             const uint32_t l0 = *reinterpret_cast<const uint32_t*>(&s_lo[warp][g][c0]);
             const uint32_t l1 = *reinterpret_cast<const uint32_t*>(&s_lo[warp][g][c0 + 8]);
+            const uint32_t q0 = *reinterpret_cast<const uint32_t*>(&s_q[warp][g][c0]);
+            const uint32_t q1 = *reinterpret_cast<const uint32_t*>(&s_q[warp][g][c0 + 8]);
             // A = [hi; mid] (rows g, g+8); B columns = features of 16 pixels
-            mma_bf16_16816(acc, h0, m0, h1, m1, h0, h1);  // x hi
-            mma_bf16_16816(acc, h0, m0, h1, m1, m0, m1);  // x mid
-            mma_bf16_16816(acc, h0, m0, h1, m1, l0, l1);  // x lo
-            mma_bf16_16816(acc, l0, 0u, l1, 0u, h0, h1);  // [lo; 0] x hi
+            mma_bf16_16816(cA, h0, m0, h1, m1, h0, h1);  // x hi
+            mma_bf16_16816(cA, h0, m0, h1, m1, m0, m1);  // x mid
+            mma_bf16_16816(cA, h0, m0, h1, m1, l0, l1);  // x lo
+            mma_bf16_16816(cB, l0, q0, l1, q1, h0, h1);  // [lo; q] x hi
           }
           __syncwarp();
+          // this 32-pixel chunk's sums, fixed-point: the same chunk gives the same bits
+          // whichever block or launch processes it
+          fx0 += __float2ll_rn((cA[0] + cA[2] + cB[0]) * kFix);
+          fx1 += __float2ll_rn((cA[1] + cA[3] + cB[1]) * kFix);
+          fxq += __float2ll_rn(cB[3] * kFix);  // column 7 (feature 1) of row 8 + g: sum q_g
         }
       }
 
-      // ---------------- block partial: 28 sums + valid count + point sum --------------
-      // two partial buffers, alternating by iteration: a block can only write iteration
-      // k + 1's row after every block has passed barrier k, i.e. finished reading row k - 1
-      float* part = a.partials + (size_t)(gi & 1u) * KF_MAX_TRACK_BLOCKS * 32;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        float v = pacc[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) s_pw[warp][k] = v;
-      }
+      // ---------------- block sums -> the entry's fixed-point rows ----------------
       if constexpr (JTJ == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float v = pacc[k];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) s_pw[warp][k] = v;
+        }
 #pragma unroll
         for (int k = 0; k < 28; ++k) {
           float v = acc[k];
@@ -274,91 +324,55 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
           if (lane == 0) s_warp[warp][k] = v;
         }
         __syncthreads();
-        if (tid < 28) {
+        if (tid < 32) {
           float v = 0.0f;
 #pragma unroll
-          for (int w = 0; w < kWarps; ++w) v += s_warp[w][tid];
-          part[(size_t)blockIdx.x * 32 + tid] = v;
+          for (int w = 0; w < kWarps; ++w) v += tid < 28 ? s_warp[w][tid] : s_pw[w][tid - 28];
+          atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid), (unsigned long long)__float2ll_rn(v * kFix));
         }
       } else {
-        // lane (g, t) holds M[g][2t], M[g][2t+1] as rows g + g+8 of the accumulator
+        // lane (g, t) holds M[g][2t], M[g][2t+1]; lanes t == 3 also sum q_g
         const int g = lane >> 2, t = lane & 3;
-        s_warp[warp][g * 8 + 2 * t] = acc[0] + acc[2];
-        s_warp[warp][g * 8 + 2 * t + 1] = acc[1] + acc[3];
+        s_fix[warp][g * 8 + 2 * t] = fx0;
+        s_fix[warp][g * 8 + 2 * t + 1] = fx1;
+        if (t == 3) s_fix[warp][64 + g] = fxq;
         __syncthreads();
-        if (tid < 28) {
-          int r, cc;
-          if (tid == 0) { r = 6; cc = 6; }
-          else if (tid < 7) { r = tid - 1; cc = 6; }
-          else {
-            int q = tid - 7;
-            r = 0;
-            while (q >= 6 - r) { q -= 6 - r; ++r; }
-            cc = r + q;
-          }
-          float v = 0.0f;
+        if (tid < 32) {
+          // row layout of reduce.cs: 0 sum e^2, 1..6 sum J e, 7..27 J^T J (upper, row-major);
+          // then 28 valid count, 29..31 sum of the points (q = hi(p) + mid(p))
+          long long v = 0;
+          if (tid < 28) {
+            int r, cc;
+            if (tid == 0) { r = 6; cc = 6; }
+            else if (tid < 7) { r = tid - 1; cc = 6; }
+            else {
+              int q = tid - 7;
+              r = 0;
+              while (q >= 6 - r) { q -= 6 - r; ++r; }
+              cc = r + q;
+            }
 #pragma unroll
-          for (int w = 0; w < kWarps; ++w) v += s_warp[w][r * 8 + cc];
-          part[(size_t)blockIdx.x * 32 + tid] = v;
+            for (int w = 0; w < kWarps; ++w) v += s_fix[w][r * 8 + cc];
+          } else if (tid == 28) {
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) v += s_fix[w][63];
+          } else {
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) v += s_fix[w][64 + tid - 29] + s_fix[w][64 + tid - 26];
+          }
+          atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid), (unsigned long long)v);
         }
       }
-      if (tid >= 28 && tid < 32) {
-        float v = 0.0f;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) v += s_pw[w][tid - 28];
-        part[(size_t)blockIdx.x * 32 + tid] = v;
-      }
+      // the buffer of the next iteration was last read before the previous barrier
+      if (local == 0 && tid >= 32 && tid < 64) a.st->icp_acc[(gi + 1u) % 3u][tid - 32] = 0;
 
-      // ---------------- grid barrier; then every block reduces and solves ----------------
-      // Every block sums the same partial rows in the same order and solves the same system
-      // in FP64, so all blocks hold bit-identical results without a second hand-over, and
-      // the solve's code stays warm in every SM's instruction cache.
+      // ---------------- grid barrier; then every block solves ----------------
+      // Every block reads the same exact sums and solves the same system in FP64, so all
+      // blocks hold bit-identical results without a second hand-over, and the solve's code
+      // stays warm in every SM's instruction cache.
       ok = kf_grid_sync(st, nb * (gi + 1u), &s_flag);
       if (!ok) break;
-      {
-        // fixed-order FP64 sum of the nb partial rows: thread (r0, q) sums columns
-        // 4q..4q+3 of rows r0, r0 + 32, ... with all of its loads in flight at once
-        const int q = tid & 7, r0 = tid >> 3;
-        const float4* P4 = reinterpret_cast<const float4*>(part);
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        constexpr int kChunk = 12;
-        for (unsigned b0 = r0; b0 < nb; b0 += 32u * kChunk) {
-          float4 buf[kChunk];
-#pragma unroll
-          for (int m = 0; m < kChunk; ++m) {
-            const unsigned b = b0 + 32u * m;
-            buf[m] = b < nb ? __ldcg(P4 + (size_t)b * 8 + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-          }
-#pragma unroll
-          for (int m = 0; m < kChunk; ++m) {
-            s0 += (double)buf[m].x;
-            s1 += (double)buf[m].y;
-            s2 += (double)buf[m].z;
-            s3 += (double)buf[m].w;
-          }
-        }
-        // the warp's four row groups (lanes q, q+8, q+16, q+24), then the warps in order
-#pragma unroll
-        for (int o = 8; o < 32; o <<= 1) {
-          s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-          s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-          s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-          s3 += __shfl_xor_sync(0xffffffffu, s3, o);
-        }
-        if (lane < 8) {
-          s_red[warp][4 * lane + 0] = s0;
-          s_red[warp][4 * lane + 1] = s1;
-          s_red[warp][4 * lane + 2] = s2;
-          s_red[warp][4 * lane + 3] = s3;
-        }
-      }
-      __syncthreads();
-      if (tid < 32) {
-        double v = 0.0;
-#pragma unroll
-        for (int r = 0; r < kWarps; ++r) v += s_red[r][tid];
-        s_sums[tid] = v;
-      }
+      if (tid < 32) s_sums[tid] = (double)__ldcg(accbuf + tid) * kInvFix;
       __syncthreads();
       if (warp == 0) {
         // ---- solve, lane-parallel in warp 0 ----
@@ -429,7 +443,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a) {
   }
 
   // ---------------- Track() tail (:715-723) + frame policy, block 0 only -----------------
-  if (blockIdx.x != 0 || tid != 0 || !ok) return;
+  if (local != 0 || tid != 0 || !ok) return;
   const double ae = iters_run ? s_ae : 0.0;
   st->ae = ae;
   if (iters_run) {
@@ -528,14 +542,14 @@ int kf_launch_icp(kf_session* s, int frame_policy) {
   a.same_pixel = (s->cfg.quirks & KF_Q4_SAME_PIXEL) ? 1 : 0;
   a.frame_policy = frame_policy;
   a.integrate_every = s->cfg.integrate_every;
-  a.partials = s->d_partials;
   a.st = s->d_state;
 
-  const void* fn = (s->cfg.jtj == KF_JTJ_SPLIT_BF16) ? (const void*)icp_kernel<1> : (const void*)icp_kernel<0>;
+  const void* fn = (s->cfg.jtj == KF_JTJ_SPLIT_BF16) ? (const void*)icp_kernel<1, false>
+                                                      : (const void*)icp_kernel<0, false>;
   int blocks = kf_occupancy_blocks(s, fn, KF_TRACK_THREADS, 0);
   if (blocks <= 0) return KF_ERR_CUDA;
-  // barrier words start at zero for every launch
-  KF_CUDA_TRY(s, cudaMemsetAsync(&s->d_state->barrier_count, 0, 2 * sizeof(unsigned), s->stream));
+  // the barrier counter and the sum buffers start at zero for every launch
+  KF_CUDA_TRY(s, kf_clear_icp_words(s->d_state, s->stream));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(KF_TRACK_THREADS);
@@ -546,10 +560,11 @@ int kf_launch_icp(kf_session* s, int frame_policy) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  const IcpBatch none = {nullptr, nullptr};
   if (s->cfg.jtj == KF_JTJ_SPLIT_BF16)
-    KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, icp_kernel<1>, a));
+    KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, icp_kernel<1, false>, a, none));
   else
-    KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, icp_kernel<0>, a));
+    KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, icp_kernel<0, false>, a, none));
   kf_note_launch(s);
   return KF_OK;
 }

@@ -49,7 +49,9 @@ struct KfDevState {
   int iterations_run;   // ICP/SDF iterations executed by the last tracking call
   unsigned barrier_count;
   unsigned barrier_gen;
-  int pad0_;
+  // ICP reduction rows as fixed-point sums (value * 2^32, exact and order-independent),
+  // three buffers used in turn by successive iterations of a launch
+  alignas(8) long long icp_acc[3][32];
   double icp_center_cam[3];  // ICP centre at the end of the last frame (camera frame)
   double lib_pose[KF_MAX_LIBRARY][16];  // pose library
 };
@@ -498,6 +500,13 @@ __device__ inline bool kf_grid_sync(KfDevState* st, unsigned target, int* s_flag
   }
   __syncthreads();
   return *s_flag != 0;
+}
+
+// Zero the barrier counter and the ICP sum buffers of a state block before a tracking launch.
+inline cudaError_t kf_clear_icp_words(KfDevState* st, cudaStream_t stream) {
+  const size_t b0 = offsetof(KfDevState, barrier_count);
+  const size_t b1 = offsetof(KfDevState, icp_acc) + sizeof(st->icp_acc);
+  return cudaMemsetAsync(reinterpret_cast<char*>(st) + b0, 0, b1 - b0, stream);
 }
 
 // Count kernels launched outside graph capture (captured graphs are counted per replay).
