@@ -227,6 +227,31 @@ KF_API int kf_reset_stage_stats(kf_session* s);
 KF_API int kf_get_launch_count(kf_session* s, uint64_t* launches);
 KF_API int kf_get_stream(kf_session* s, void** cuda_stream);
 
+/* ---- batched frame steps (the batched and served forms; no counterpart in the reference,
+ * whose app runs one session) -----------------------------------------------------------
+ * A batch steps several sessions' frames together, one launch per stage for all of them
+ * (the per-frame body of kinect.cpp:654-695 for each).  Sessions of one step must share
+ * the image size, storage and J^T J form and track by ICP; volume sizes and every other
+ * setting may differ.  Each session's results are bit-identical to stepping it alone
+ * (kf_frame_step_u16).  The step synchronises its stream; the sessions' poses and flags
+ * are readable afterwards (kf_get_pose, ...).  Per-member tables are rebuilt when the set
+ * or order of sessions changes.  A batch is used by one host thread at a time. */
+#define KF_BATCH_MAX_SESSIONS 255
+typedef struct kf_batch kf_batch;
+KF_API int kf_batch_create(int max_sessions, kf_batch** out);
+KF_API int kf_batch_destroy(kf_batch* b);
+KF_API const char* kf_batch_last_error(const kf_batch* b);
+/* host_depth_mm[i]: session i's 512x424-style uint16 frame (pinned memory copies fastest);
+ * tracked[i] (may be NULL) receives the session's tracking result. */
+KF_API int kf_batch_frame_step_u16(kf_batch* b, kf_session* const* sessions,
+                                   const uint16_t* const* host_depth_mm, int n, int32_t* tracked);
+KF_API int kf_batch_frame_step_u16_device(kf_batch* b, kf_session* const* sessions,
+                                          const uint16_t* const* device_depth_mm, int n,
+                                          int32_t* tracked);
+/* Device ms of the last step's stages: pyramid, track, integrate, recover, raycast. */
+KF_API int kf_batch_get_stage_times(kf_batch* b, float* ms5);
+KF_API int kf_batch_get_launch_count(kf_batch* b, uint64_t* launches);
+
 /* ---- marching cubes (MCubes, mcubes.cpp:206-509) ---------------------------------------
  * kf_mc_extract = setIsolevel + generateMarchingCubes; *n_triangles is the triangle count
  * (getNumberTriangles() returns 3x that).  Vertices are float4 in voxel-index units,

@@ -31,6 +31,7 @@ KF_TRACK_ICP = 0
 KF_TRACK_SDF = 1
 KF_MC_HISTOPYRAMID = 0
 KF_MC_SCAN = 1
+KF_BATCH_MAX_SESSIONS = 255
 
 KF_Q1_LAST_GROUP_ONLY = 1 << 0
 KF_Q3_DOWN_FROM_LEFT = 1 << 1
@@ -137,6 +138,13 @@ SIGNATURES = {
     "kf_mc_export_ply": (_I, [_P, C.c_char_p]),
     "kf_prefix_sum_u32": (_I, [_P, _P, C.c_uint64, C.POINTER(C.c_uint32), _P]),
     "kf_prefix_sum_u32_noalloc": (_I, [_P, _P, C.c_uint64, C.POINTER(C.c_uint32), _P]),
+    "kf_batch_create": (_I, [_I, C.POINTER(_P)]),
+    "kf_batch_destroy": (_I, [_P]),
+    "kf_batch_last_error": (C.c_char_p, [_P]),
+    "kf_batch_frame_step_u16": (_I, [_P, C.POINTER(_P), C.POINTER(_P), _I, C.POINTER(C.c_int32)]),
+    "kf_batch_frame_step_u16_device": (_I, [_P, C.POINTER(_P), C.POINTER(_P), _I, C.POINTER(C.c_int32)]),
+    "kf_batch_get_stage_times": (_I, [_P, C.POINTER(C.c_float)]),
+    "kf_batch_get_launch_count": (_I, [_P, C.POINTER(C.c_uint64)]),
 }
 
 _lib = None

@@ -1,0 +1,214 @@
+// kf_batch.cu — batched frame steps: many sessions, one launch per stage.
+//
+// Reference: the per-frame body of kinect.cpp:654-695 (pyramid, Track, integrate when
+// tracked or in the reset window, recoverPose when not tracked, raycast), run for every
+// member session.  The reference has one session; this is the batched form.
+//
+// B200 design: a batch step launches each stage once for all members — the pyramid and
+// raycast grids carry the member in blockIdx.z, integrate walks a flat grid of every
+// member's voxel blocks (a prefix table maps a block to its member), and the tracking
+// kernels split the co-resident grid into one group of blocks per member, each with its
+// own barrier and fixed-point reduction rows.  Per-member arguments live in one device
+// table, rebuilt only when the membership changes.  A member's results are bit-identical
+// to stepping it alone: every kernel computes a member exactly as in its single-session
+// launch, and the ICP sums are exact integers whatever the block split.
+#include <algorithm>
+#include <cstring>
+
+#include "kf_internal.cuh"
+
+namespace {
+
+// Zero each member's tracking words (barrier counters and ICP sum buffers).
+__global__ void batch_clear_kernel(KfDevState* const* states) {
+  KfDevState* st = states[blockIdx.x];
+  if (threadIdx.x == 0) {
+    st->barrier_count = 0;
+    st->sdf_barrier_count = 0;
+  }
+  for (int k = threadIdx.x; k < 3 * 32; k += blockDim.x) (&st->icp_acc[0][0])[k] = 0;
+}
+
+// Gather each member's frame result (the first KF_STATE_RESULT_BYTES of its state).
+__global__ void batch_gather_kernel(KfDevState* const* states, char* heads) {
+  const char* src = reinterpret_cast<const char*>(states[blockIdx.x]);
+  for (int k = threadIdx.x; k < (int)(KF_STATE_RESULT_BYTES / 4); k += blockDim.x)
+    reinterpret_cast<int*>(heads + (size_t)blockIdx.x * KF_STATE_RESULT_BYTES)[k] = reinterpret_cast<const int*>(src)[k];
+}
+
+int bfail(kf_batch* b, int code, const std::string& msg) {
+  b->last_error = msg;
+  return code;
+}
+
+int check_members(kf_batch* b, kf_session* const* ss, int n) {
+  kf_session* s0 = ss[0];
+  for (int e = 0; e < n; ++e) {
+    kf_session* s = ss[e];
+    if (!s) return bfail(b, KF_ERR_INVALID_ARGUMENT, "null session");
+    if (s->device != b->device) return bfail(b, KF_ERR_INVALID_ARGUMENT, "session on another device");
+    if (s->W[0] != s0->W[0] || s->H[0] != s0->H[0])
+      return bfail(b, KF_ERR_INVALID_ARGUMENT, "sessions of one batch step need the same image size");
+    if (s->cfg.storage != s0->cfg.storage || s->cfg.jtj != s0->cfg.jtj)
+      return bfail(b, KF_ERR_INVALID_ARGUMENT, "sessions of one batch step need the same storage and J^T J form");
+    if (s->cfg.tracking != KF_TRACK_ICP) return bfail(b, KF_ERR_INVALID_ARGUMENT, "batched frame steps track by ICP");
+    for (int f = 0; f < e; ++f)
+      if (ss[f] == s) return bfail(b, KF_ERR_INVALID_ARGUMENT, "a session appears twice in one batch step");
+  }
+  return KF_OK;
+}
+
+int rebuild_tables(kf_batch* b, kf_session* const* ss, int n) {
+  b->members.assign(ss, ss + n);
+  b->table_used = 0;
+  KfDevState** hs = nullptr;
+  b->states = static_cast<KfDevState* const*>(kf_batch_table(b, sizeof(KfDevState*) * n, reinterpret_cast<void**>(&hs)));
+  if (!b->states) return bfail(b, KF_ERR_CAPACITY, "batch table full");
+  for (int e = 0; e < n; ++e) hs[e] = ss[e]->d_state;
+  int rc;
+  if ((rc = kf_batch_prepare_pyramid(b)) || (rc = kf_batch_prepare_icp(b)) || (rc = kf_batch_prepare_integrate(b)) ||
+      (rc = kf_batch_prepare_sdf(b)) || (rc = kf_batch_prepare_raycast(b))) {
+    b->members.clear();
+    return bfail(b, rc, "batch tables: too many sessions for the table or the co-resident grid");
+  }
+  KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_table, b->h_table, b->table_used, cudaMemcpyHostToDevice, b->stream));
+  return KF_OK;
+}
+
+int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth, int n, int32_t* tracked,
+               cudaMemcpyKind kind) {
+  if (!b || !ss || !depth || n <= 0) return KF_ERR_INVALID_ARGUMENT;
+  if (n > b->cap) return bfail(b, KF_ERR_CAPACITY, "more sessions than the batch was created for");
+  int rc = check_members(b, ss, n);
+  if (rc) return rc;
+  for (int e = 0; e < n; ++e)
+    if (!depth[e]) return bfail(b, KF_ERR_INVALID_ARGUMENT, "null depth frame");
+  int cur = 0;
+  KF_CUDA_TRY(b, cudaGetDevice(&cur));
+  if (cur != b->device) KF_CUDA_TRY(b, cudaSetDevice(b->device));
+  const bool same = (int)b->members.size() == n && std::equal(ss, ss + n, b->members.begin());
+  if (!same && (rc = rebuild_tables(b, ss, n))) return rc;
+  // a member's own stream may still hold work (an asynchronous frame step)
+  for (int e = 0; e < n; ++e)
+    if (cudaStreamQuery(ss[e]->stream) != cudaSuccess) KF_CUDA_TRY(b, cudaStreamSynchronize(ss[e]->stream));
+  const size_t px = (size_t)ss[0]->W[0] * ss[0]->H[0];
+  for (int e = 0; e < n; ++e)
+    KF_CUDA_TRY(b, cudaMemcpyAsync(ss[e]->d_depth_u16, depth[e], px * 2, kind, b->stream));
+  KF_CUDA_TRY(b, cudaEventRecord(b->ev[0], b->stream));
+  batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
+  KF_CUDA_TRY(b, cudaGetLastError());
+  if ((rc = kf_batch_launch_pyramid(b, n))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(b->ev[1], b->stream));
+  if ((rc = kf_batch_launch_icp(b))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(b->ev[2], b->stream));
+  if ((rc = kf_batch_launch_integrate(b))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(b->ev[3], b->stream));
+  if ((rc = kf_batch_launch_sdf_recover(b))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(b->ev[4], b->stream));
+  if ((rc = kf_batch_launch_raycast(b, n))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(b->ev[5], b->stream));
+  batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
+  KF_CUDA_TRY(b, cudaGetLastError());
+  b->launches += 2;
+  KF_CUDA_TRY(b, cudaMemcpyAsync(b->h_heads, b->d_heads, (size_t)n * KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost,
+                                 b->stream));
+  KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < 5; ++i) KF_CUDA_TRY(b, cudaEventElapsedTime(&b->stage_ms[i], b->ev[i], b->ev[i + 1]));
+  b->steps += 1;
+  int first_err = KF_OK;
+  for (int e = 0; e < n; ++e) {
+    kf_session* s = ss[e];
+    std::memcpy(s->h_state, b->h_heads + (size_t)e * KF_STATE_RESULT_BYTES, KF_STATE_RESULT_BYTES);
+    if (tracked) tracked[e] = s->h_state->tracked;
+    if (s->h_state->error) {
+      const int err = s->h_state->error;
+      s->h_state->error = 0;
+      KF_CUDA_TRY(b, cudaMemsetAsync(&s->d_state->error, 0, sizeof(int), b->stream));
+      s->last_error = "device wait timed out (error " + std::to_string(err) + ")";
+      if (!first_err) first_err = bfail(b, KF_ERR_TIMEOUT, "session " + std::to_string(e) + ": " + s->last_error);
+    }
+  }
+  if (first_err) KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  return first_err;
+}
+
+void free_batch(kf_batch* b) {
+  cudaFree(b->d_table);
+  cudaFreeHost(b->h_table);
+  cudaFree(b->d_heads);
+  cudaFreeHost(b->h_heads);
+  for (auto& e : b->ev)
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int kf_batch_create(int max_sessions, kf_batch** out) {
+  if (!out || max_sessions <= 0 || max_sessions > KF_BATCH_MAX_SESSIONS) return KF_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return KF_ERR_NO_DEVICE;
+  }
+  kf_batch* b = new (std::nothrow) kf_batch();
+  if (!b) return KF_ERR_OUT_OF_MEMORY;
+  b->cap = max_sessions;
+  auto bail = [&](int code) {
+    free_batch(b);
+    delete b;
+    return code;
+  };
+  if (cudaGetDevice(&b->device) != cudaSuccess) return bail(KF_ERR_CUDA);
+  if (cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess)
+    return bail(KF_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(KF_ERR_CUDA);
+  for (auto& e : b->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bail(KF_ERR_CUDA);
+  // per member: seven argument records (< 2 KB) and two block maps of the co-resident grid
+  b->table_cap = 64 * 1024 + (size_t)max_sessions * 2048;
+  if (cudaMallocHost((void**)&b->h_table, b->table_cap) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  if (cudaMalloc((void**)&b->d_table, b->table_cap) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  const size_t hb = (size_t)max_sessions * KF_STATE_RESULT_BYTES;
+  if (cudaMallocHost((void**)&b->h_heads, hb) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  if (cudaMalloc((void**)&b->d_heads, hb) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  *out = b;
+  return KF_OK;
+}
+
+int kf_batch_destroy(kf_batch* b) {
+  if (!b) return KF_ERR_INVALID_ARGUMENT;
+  cudaStreamSynchronize(b->stream);
+  free_batch(b);
+  delete b;
+  return KF_OK;
+}
+
+const char* kf_batch_last_error(const kf_batch* b) { return b ? b->last_error.c_str() : "null batch"; }
+
+int kf_batch_frame_step_u16(kf_batch* b, kf_session* const* sessions, const uint16_t* const* host_depth_mm, int n,
+                            int32_t* tracked) {
+  return batch_step(b, sessions, host_depth_mm, n, tracked, cudaMemcpyHostToDevice);
+}
+
+int kf_batch_frame_step_u16_device(kf_batch* b, kf_session* const* sessions, const uint16_t* const* device_depth_mm,
+                                   int n, int32_t* tracked) {
+  return batch_step(b, sessions, device_depth_mm, n, tracked, cudaMemcpyDeviceToDevice);
+}
+
+int kf_batch_get_stage_times(kf_batch* b, float* ms) {
+  if (!b || !ms) return KF_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < 5; ++i) ms[i] = b->stage_ms[i];
+  return KF_OK;
+}
+
+int kf_batch_get_launch_count(kf_batch* b, uint64_t* n) {
+  if (!b || !n) return KF_ERR_INVALID_ARGUMENT;
+  *n = b->launches;
+  return KF_OK;
+}
+
+}  // extern "C"

@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       // Every block reads the same exact sums and solves the same system in FP64, so all
       // blocks hold bit-identical results without a second hand-over, and the solve's code
       // stays warm in every SM's instruction cache.
-      ok = kf_grid_sync(st, nb * (gi + 1u), &s_flag);
+      ok = kf_grid_sync(st, &st->barrier_count, nb * (gi + 1u), &s_flag);
       if (!ok) break;
       if (tid < 32) s_sums[tid] = (double)__ldcg(accbuf + tid) * kInvFix;
       __syncthreads();
@@ -520,7 +520,9 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
 
 }  // namespace
 
-int kf_launch_icp(kf_session* s, int frame_policy) {
+namespace {
+
+IcpArgs make_icp_args(kf_session* s, int frame_policy) {
   IcpArgs a;
   for (int l = 0; l < 3; ++l) {
     a.vertex[l] = s->d_vertex[l];
@@ -543,28 +545,68 @@ int kf_launch_icp(kf_session* s, int frame_policy) {
   a.frame_policy = frame_policy;
   a.integrate_every = s->cfg.integrate_every;
   a.st = s->d_state;
+  return a;
+}
 
+cudaLaunchConfig_t coop_config(dim3 grid, cudaStream_t stream, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(KF_TRACK_THREADS);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+}  // namespace
+
+int kf_launch_icp(kf_session* s, int frame_policy) {
+  const IcpArgs a = make_icp_args(s, frame_policy);
   const void* fn = (s->cfg.jtj == KF_JTJ_SPLIT_BF16) ? (const void*)icp_kernel<1, false>
                                                       : (const void*)icp_kernel<0, false>;
   int blocks = kf_occupancy_blocks(s, fn, KF_TRACK_THREADS, 0);
   if (blocks <= 0) return KF_ERR_CUDA;
   // the barrier counter and the sum buffers start at zero for every launch
   KF_CUDA_TRY(s, kf_clear_icp_words(s->d_state, s->stream));
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(blocks);
-  cfg.blockDim = dim3(KF_TRACK_THREADS);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s->stream;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cudaLaunchConfig_t cfg = coop_config(dim3(blocks), s->stream, attr);
   const IcpBatch none = {nullptr, nullptr};
   if (s->cfg.jtj == KF_JTJ_SPLIT_BF16)
     KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, icp_kernel<1, false>, a, none));
   else
     KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, icp_kernel<0, false>, a, none));
   kf_note_launch(s);
+  return KF_OK;
+}
+
+// ---- batched: every member's frame-step ICP in one cooperative launch ----
+int kf_batch_prepare_icp(kf_batch* b) {
+  const int n = (int)b->members.size();
+  IcpArgs* h = nullptr;
+  b->icp_args = kf_batch_table(b, sizeof(IcpArgs) * n, reinterpret_cast<void**>(&h));
+  if (!b->icp_args) return KF_ERR_CAPACITY;
+  for (int e = 0; e < n; ++e) h[e] = make_icp_args(b->members[e], 1);
+  kf_session* s0 = b->members[0];
+  const void* fn = (s0->cfg.jtj == KF_JTJ_SPLIT_BF16) ? (const void*)icp_kernel<1, true>
+                                                       : (const void*)icp_kernel<0, true>;
+  const int total = kf_occupancy_blocks(s0, fn, KF_TRACK_THREADS, 0);
+  if (total <= 0) return KF_ERR_CUDA;
+  b->icp_blocks = total;
+  return kf_batch_block_map(b, total, &b->icp_map);
+}
+
+int kf_batch_launch_icp(kf_batch* b) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = coop_config(dim3(b->icp_blocks), b->stream, attr);
+  const IcpBatch batch = {static_cast<const IcpArgs*>(b->icp_args), b->icp_map};
+  const IcpArgs none{};
+  if (b->members[0]->cfg.jtj == KF_JTJ_SPLIT_BF16)
+    KF_CUDA_TRY(b, cudaLaunchKernelEx(&cfg, icp_kernel<1, true>, none, batch));
+  else
+    KF_CUDA_TRY(b, cudaLaunchKernelEx(&cfg, icp_kernel<0, true>, none, batch));
+  b->launches += 1;
   return KF_OK;
 }

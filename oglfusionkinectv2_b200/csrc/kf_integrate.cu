@@ -149,8 +149,39 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   return zneg;
 }
 
-template <int S>
-__global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a) {
+// A batched launch: flat block b belongs to the entry e with prefix[e] <= b < prefix[e + 1].
+struct IntBatch {
+  const IntArgs* args;
+  const uint32_t* prefix;  // n + 1 entries
+  int n;
+};
+
+template <int S, bool BATCH>
+__global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBatch batch) {
+  __shared__ IntArgs s_args;
+  int bxi, byi, bzi;  // this block's position in its volume's block grid
+  if constexpr (BATCH) {
+    // binary search of the entry (uniform over the block)
+    int lo = 0, hi = batch.n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(batch.prefix + mid) <= blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int* src = reinterpret_cast<const int*>(batch.args + lo);
+    for (int k = tid; k < (int)(sizeof(IntArgs) / 4); k += 256) reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
+    __syncthreads();
+    const uint32_t local = blockIdx.x - __ldg(batch.prefix + lo);
+    const uint32_t gx = (uint32_t)(s_args.nx + 31) / 32, gy = (uint32_t)(s_args.ny + 7) / 8;
+    bxi = (int)(local % gx);
+    byi = (int)((local / gx) % gy);
+    bzi = (int)(local / (gx * gy));
+  } else {
+    bxi = blockIdx.x;
+    byi = blockIdx.y;
+    bzi = blockIdx.z;
+  }
+  const IntArgs& a = BATCH ? s_args : a_one;
   __shared__ int s_cull;
   // negative-value flags of the bricks this block may touch, dilated by one voxel towards
   // -x/-y/-z: [z: bz0-1 .. bz0+1][y: by0-1 .. by0][x: bx0-1 .. bx0+3]
@@ -159,7 +190,7 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a) {
   float inv[12];  // inverse(m_pose), rows of [R^T | -R^T t] (integrate uses glm::inverse, :1242)
 #pragma unroll
   for (int k = 0; k < 12; ++k) inv[k] = a.st->inv_rows[k];
-  const int xb = blockIdx.x * 32, yb = blockIdx.y * 8, zb = blockIdx.z * kZC;
+  const int xb = bxi * 32, yb = byi * 8, zb = bzi * kZC;
   if (threadIdx.y == 0) {
     // one voxel of margin on every side absorbs the rounding of the per-voxel tests
     const int b0[3] = {xb - 1, yb - 1, zb - 1};
@@ -205,7 +236,9 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a) {
 
 }  // namespace
 
-int kf_launch_integrate(kf_session* s, int gated) {
+namespace {
+
+IntArgs make_int_args(kf_session* s, int gated) {
   IntArgs a;
   a.vol = s->d_vol;
   a.count = s->vol_count;
@@ -222,14 +255,54 @@ int kf_launch_integrate(kf_session* s, int gated) {
   a.st = s->d_state;
   a.bricks = s->d_bricks;
   a.bx = s->bx; a.by = s->by; a.bz = s->bz;
+  return a;
+}
+
+template <bool BATCH>
+void launch_int(int storage, dim3 grid, cudaStream_t st, const IntArgs& a, const IntBatch& b) {
   dim3 block(32, 8);
-  dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + kZC - 1) / kZC);
-  switch (s->cfg.storage) {
-    case KF_STORAGE_F32F32: integrate_kernel<KF_STORAGE_F32F32><<<grid, block, 0, s->stream>>>(a); break;
-    case KF_STORAGE_F16U16: integrate_kernel<KF_STORAGE_F16U16><<<grid, block, 0, s->stream>>>(a); break;
-    default: integrate_kernel<KF_STORAGE_RG16I><<<grid, block, 0, s->stream>>>(a); break;
+  switch (storage) {
+    case KF_STORAGE_F32F32: integrate_kernel<KF_STORAGE_F32F32, BATCH><<<grid, block, 0, st>>>(a, b); break;
+    case KF_STORAGE_F16U16: integrate_kernel<KF_STORAGE_F16U16, BATCH><<<grid, block, 0, st>>>(a, b); break;
+    default: integrate_kernel<KF_STORAGE_RG16I, BATCH><<<grid, block, 0, st>>>(a, b); break;
   }
+}
+
+}  // namespace
+
+int kf_launch_integrate(kf_session* s, int gated) {
+  const IntArgs a = make_int_args(s, gated);
+  dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + kZC - 1) / kZC);
+  launch_int<false>(s->cfg.storage, grid, s->stream, a, IntBatch{nullptr, nullptr, 0});
   KF_CUDA_TRY(s, cudaGetLastError());
   kf_note_launch(s);
+  return KF_OK;
+}
+
+// ---- batched: every member's gated frame-step integrate in one launch ----
+int kf_batch_prepare_integrate(kf_batch* b) {
+  const int n = (int)b->members.size();
+  IntArgs* h = nullptr;
+  uint32_t* hp = nullptr;
+  b->int_args = kf_batch_table(b, sizeof(IntArgs) * n, reinterpret_cast<void**>(&h));
+  b->int_prefix = static_cast<const uint32_t*>(kf_batch_table(b, 4 * (size_t)(n + 1), reinterpret_cast<void**>(&hp)));
+  if (!b->int_args || !b->int_prefix) return KF_ERR_CAPACITY;
+  uint64_t total = 0;
+  for (int e = 0; e < n; ++e) {
+    h[e] = make_int_args(b->members[e], 1);
+    hp[e] = (uint32_t)total;
+    total += (uint64_t)((h[e].nx + 31) / 32) * ((h[e].ny + 7) / 8) * ((h[e].nz + kZC - 1) / kZC);
+  }
+  if (total >= (1ull << 31)) return KF_ERR_CAPACITY;
+  hp[n] = (uint32_t)total;
+  b->int_blocks = (uint32_t)total;
+  return KF_OK;
+}
+
+int kf_batch_launch_integrate(kf_batch* b) {
+  const IntBatch batch = {static_cast<const IntArgs*>(b->int_args), b->int_prefix, (int)b->members.size()};
+  launch_int<true>(b->members[0]->cfg.storage, dim3(b->int_blocks), b->stream, IntArgs{}, batch);
+  KF_CUDA_TRY(b, cudaGetLastError());
+  b->launches += 1;
   return KF_OK;
 }

@@ -47,8 +47,8 @@ struct KfDevState {
   int do_integrate;     // frame policy: integrate this frame
   int reset_window;     // kinect.cpp `reset` flag
   int iterations_run;   // ICP/SDF iterations executed by the last tracking call
-  unsigned barrier_count;
-  unsigned barrier_gen;
+  unsigned barrier_count;      // grid barrier of the ICP launch
+  unsigned sdf_barrier_count;  // grid barrier of the SDF launch
   // ICP reduction rows as fixed-point sums (value * 2^32, exact and order-independent),
   // three buffers used in turn by successive iterations of a launch
   alignas(8) long long icp_acc[3][32];
@@ -477,16 +477,16 @@ __device__ __forceinline__ unsigned kf_ld_acquire_gpu(const unsigned* p) {
 
 // The bar.sync before thread 0's gpu-scope release orders every thread's earlier stores
 // of the block before it; an acquirer that observes the release sees them.
-// Grid barrier over barrier_count, which only grows during a launch (the launcher zeroes
-// it): every block adds one and waits until `target` arrivals in total.  One release
+// Grid barrier over a counter that only grows during a launch (the launcher zeroes it):
+// every block adds one and waits until `target` arrivals in total.  One release
 // reduction per block and no reset step; bounded like kf_grid_wait.
-__device__ inline bool kf_grid_sync(KfDevState* st, unsigned target, int* s_flag) {
+__device__ inline bool kf_grid_sync(KfDevState* st, unsigned* counter, unsigned target, int* s_flag) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&st->barrier_count) : "memory");
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
     int ok = 1;
     const long long t0 = clock64();
-    while (kf_ld_acquire_gpu(&st->barrier_count) < target) {
+    while (kf_ld_acquire_gpu(counter) < target) {
       if (*(volatile int*)&st->error) { ok = 0; break; }
       if (clock64() - t0 > KF_BARRIER_SPIN_CYCLES) {
         atomicExch(&st->error, KF_DEV_ERR_TIMEOUT);
@@ -501,6 +501,82 @@ __device__ inline bool kf_grid_sync(KfDevState* st, unsigned target, int* s_flag
   __syncthreads();
   return *s_flag != 0;
 }
+
+// ---------------------------------------------------------------------------------------
+// batched frame steps (kf_batch.cu): sessions of equal image size, storage and J^T J form
+// step together, one launch per stage; per-session arguments live in a device table that
+// is rebuilt only when the membership changes.
+struct kf_batch {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  int cap = 0;
+  std::string last_error;
+  std::vector<kf_session*> members;  // membership of the uploaded tables
+  // argument tables: pinned host copy and device copy
+  char* h_table = nullptr;
+  char* d_table = nullptr;
+  size_t table_cap = 0, table_used = 0;
+  // device pointers into d_table, set by the kf_batch_prepare_* functions
+  KfDevState* const* states = nullptr;
+  const void* pyr_args = nullptr;
+  const void* vn_args = nullptr;
+  int vn_pixels = 0, W1 = 0, H1 = 0;
+  const void* icp_args = nullptr;
+  const uint32_t* icp_map = nullptr;
+  int icp_blocks = 0;
+  const void* sdf_args = nullptr;
+  const uint32_t* sdf_map = nullptr;
+  int sdf_blocks = 0;
+  const void* int_args = nullptr;
+  const uint32_t* int_prefix = nullptr;
+  uint32_t int_blocks = 0;
+  const void* ray_args = nullptr;
+  // gathered frame results: [cap][KF_STATE_RESULT_BYTES]
+  char* d_heads = nullptr;
+  char* h_heads = nullptr;
+  cudaEvent_t ev[6] = {};
+  float stage_ms[5] = {0, 0, 0, 0, 0};
+  uint64_t steps = 0;
+  uint64_t launches = 0;
+};
+
+// Reserves `bytes` in the host table (256-byte aligned); returns the matching device
+// pointer, or nullptr when the table is full.
+inline void* kf_batch_table(kf_batch* b, size_t bytes, void** host) {
+  const size_t off = (b->table_used + 255) & ~(size_t)255;
+  if (off + bytes > b->table_cap) return nullptr;
+  b->table_used = off + bytes;
+  *host = b->h_table + off;
+  return b->d_table + off;
+}
+
+// Splits `total` co-resident blocks of a persistent tracking kernel evenly over the
+// batch's members: word = entry << 24 | blocks of the entry << 12 | index.
+inline int kf_batch_block_map(kf_batch* b, int total, const uint32_t** d_map) {
+  const int n = (int)b->members.size();
+  if (n > total || n > 255 || total / n > 4095) return KF_ERR_CAPACITY;
+  uint32_t* h = nullptr;
+  *d_map = static_cast<const uint32_t*>(kf_batch_table(b, (size_t)total * 4, reinterpret_cast<void**>(&h)));
+  if (!*d_map) return KF_ERR_CAPACITY;
+  int k = 0;
+  for (int e = 0; e < n; ++e) {
+    const int cnt = total / n + (e < total % n ? 1 : 0);
+    for (int i = 0; i < cnt; ++i) h[k++] = (uint32_t)e << 24 | (uint32_t)cnt << 12 | (uint32_t)i;
+  }
+  return KF_OK;
+}
+
+int kf_batch_prepare_pyramid(kf_batch* b);
+int kf_batch_prepare_icp(kf_batch* b);
+int kf_batch_prepare_sdf(kf_batch* b);
+int kf_batch_prepare_integrate(kf_batch* b);
+int kf_batch_prepare_raycast(kf_batch* b);
+int kf_batch_launch_pyramid(kf_batch* b, int n);
+int kf_batch_launch_icp(kf_batch* b);
+int kf_batch_launch_sdf_recover(kf_batch* b);
+int kf_batch_launch_integrate(kf_batch* b);
+int kf_batch_launch_raycast(kf_batch* b, int n);
 
 // Zero the barrier counter and the ICP sum buffers of a state block before a tracking launch.
 inline cudaError_t kf_clear_icp_words(KfDevState* st, cudaStream_t stream) {

@@ -21,8 +21,11 @@ struct PyrArgs {
 };
 
 // One thread per level-1 pixel; a 32x8 block also produces a 16x4 level-2 tile.
-__global__ void __launch_bounds__(256) depth_mip_kernel(PyrArgs a) {
+// BATCH: blockIdx.z selects the session's arguments in `many`.
+template <bool BATCH>
+__global__ void __launch_bounds__(256) depth_mip_kernel(PyrArgs one, const PyrArgs* many) {
   __shared__ float s_l1[8][33];
+  const PyrArgs a = BATCH ? many[blockIdx.z] : one;
   const int x1 = blockIdx.x * 32 + threadIdx.x;
   const int y1 = blockIdx.y * 8 + threadIdx.y;
   float m = 0.0f;
@@ -83,7 +86,9 @@ __device__ __forceinline__ float3 neighbour(const VNArgs& a, int l, int x, int y
   return make_float3(v.x, v.y, v.z);
 }
 
-__global__ void __launch_bounds__(256) vertex_normal_kernel(VNArgs a) {
+template <bool BATCH>
+__global__ void __launch_bounds__(256) vertex_normal_kernel(VNArgs one, const VNArgs* many) {
+  const VNArgs& a = BATCH ? many[blockIdx.y] : one;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= a.start[3]) return;
   const int l = gid < a.start[1] ? 0 : (gid < a.start[2] ? 1 : 2);
@@ -145,9 +150,7 @@ VNArgs make_vn_args(kf_session* s, int mode) {
   return a;
 }
 
-}  // namespace
-
-int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32) {
+PyrArgs make_pyr_args(kf_session* s, const uint16_t* d_u16, const float* d_f32) {
   PyrArgs a;
   a.in_u16 = d_u16;
   a.in_f32 = d_u16 ? nullptr : d_f32;
@@ -156,9 +159,16 @@ int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32) 
     a.W[l] = s->W[l];
     a.H[l] = s->H[l];
   }
+  return a;
+}
+
+}  // namespace
+
+int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32) {
+  const PyrArgs a = make_pyr_args(s, d_u16, d_f32);
   dim3 block(32, 8);
   dim3 grid((s->W[1] + 31) / 32, (s->H[1] + 7) / 8);
-  depth_mip_kernel<<<grid, block, 0, s->stream>>>(a);
+  depth_mip_kernel<false><<<grid, block, 0, s->stream>>>(a, nullptr);
   kf_note_launch(s);
   KF_CUDA_TRY(s, cudaGetLastError());
   return KF_OK;
@@ -168,7 +178,7 @@ static int launch_vn(kf_session* s, int mode) {
   VNArgs a = make_vn_args(s, mode);
   const int threads = 256;
   const int blocks = (a.start[3] + threads - 1) / threads;
-  vertex_normal_kernel<<<blocks, threads, 0, s->stream>>>(a);
+  vertex_normal_kernel<false><<<blocks, threads, 0, s->stream>>>(a, nullptr);
   kf_note_launch(s);
   KF_CUDA_TRY(s, cudaGetLastError());
   return KF_OK;
@@ -177,3 +187,34 @@ static int launch_vn(kf_session* s, int mode) {
 int kf_launch_vertex(kf_session* s) { return launch_vn(s, 1); }
 int kf_launch_normal(kf_session* s) { return launch_vn(s, 2); }
 int kf_launch_vertex_normal(kf_session* s) { return launch_vn(s, 3); }
+
+// ---- batched: every member's uint16 upload buffer -> its pyramid, one launch per kernel ----
+int kf_batch_prepare_pyramid(kf_batch* b) {
+  const int n = (int)b->members.size();
+  PyrArgs* hp = nullptr;
+  VNArgs* hv = nullptr;
+  b->pyr_args = kf_batch_table(b, sizeof(PyrArgs) * n, reinterpret_cast<void**>(&hp));
+  b->vn_args = kf_batch_table(b, sizeof(VNArgs) * n, reinterpret_cast<void**>(&hv));
+  if (!b->pyr_args || !b->vn_args) return KF_ERR_CAPACITY;
+  for (int e = 0; e < n; ++e) {
+    kf_session* s = b->members[e];
+    hp[e] = make_pyr_args(s, s->d_depth_u16, nullptr);
+    hv[e] = make_vn_args(s, 3);
+  }
+  b->vn_pixels = hv[0].start[3];
+  b->W1 = b->members[0]->W[1];
+  b->H1 = b->members[0]->H[1];
+  return KF_OK;
+}
+
+int kf_batch_launch_pyramid(kf_batch* b, int n) {
+  dim3 block(32, 8);
+  dim3 grid((b->W1 + 31) / 32, (b->H1 + 7) / 8, n);
+  depth_mip_kernel<true><<<grid, block, 0, b->stream>>>(PyrArgs{}, static_cast<const PyrArgs*>(b->pyr_args));
+  KF_CUDA_TRY(b, cudaGetLastError());
+  dim3 g2((b->vn_pixels + 255) / 256, n);
+  vertex_normal_kernel<true><<<g2, 256, 0, b->stream>>>(VNArgs{}, static_cast<const VNArgs*>(b->vn_args));
+  KF_CUDA_TRY(b, cudaGetLastError());
+  b->launches += 2;
+  return KF_OK;
+}

@@ -73,9 +73,18 @@ struct Sampler {
   }
 };
 
-template <int S>
-__global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs a) {
+// BATCH: blockIdx.z selects the session's arguments in `many`.
+template <int S, bool BATCH>
+__global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs one, const RayArgs* many) {
+  __shared__ RayArgs s_args;
   __shared__ float s_view[12];  // rows of m_pose * invK: (R K^-1 | t)
+  if constexpr (BATCH) {
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int* src = reinterpret_cast<const int*>(many + blockIdx.z);
+    for (int k = tid; k < (int)(sizeof(RayArgs) / 4); k += kRayThreads) reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
+    __syncthreads();
+  }
+  const RayArgs& a = BATCH ? s_args : one;
   if (threadIdx.y == 0 && threadIdx.x < 12) {
     // view = m_pose * invK (gFusion.cpp:1296) from the FP32 pose rows and float invK
     const int r = threadIdx.x >> 2, c = threadIdx.x & 3;
@@ -292,7 +301,9 @@ int kf_rebuild_bricks(kf_session* s) {
   return KF_OK;
 }
 
-int kf_launch_raycast(kf_session* s) {
+namespace {
+
+RayArgs make_ray_args(kf_session* s) {
   RayArgs a;
   a.vol = s->d_vol;
   a.nx = s->cfg.nx; a.ny = s->cfg.ny; a.nz = s->cfg.nz;
@@ -322,14 +333,45 @@ int kf_launch_raycast(kf_session* s) {
   a.st_out = s->d_state;
   a.bricks = s->d_bricks;
   a.bx = s->bx; a.by = s->by; a.bz = s->bz;
+  return a;
+}
+
+template <bool BATCH>
+void launch_ray(int storage, dim3 grid, cudaStream_t st, const RayArgs& a, const RayArgs* many) {
   dim3 block(32, kRayRows);
-  dim3 grid((a.W + 31) / 32, (a.H + kRayRows - 1) / kRayRows);
-  switch (s->cfg.storage) {
-    case KF_STORAGE_F32F32: raycast_kernel<KF_STORAGE_F32F32><<<grid, block, 0, s->stream>>>(a); break;
-    case KF_STORAGE_F16U16: raycast_kernel<KF_STORAGE_F16U16><<<grid, block, 0, s->stream>>>(a); break;
-    default: raycast_kernel<KF_STORAGE_RG16I><<<grid, block, 0, s->stream>>>(a); break;
+  switch (storage) {
+    case KF_STORAGE_F32F32: raycast_kernel<KF_STORAGE_F32F32, BATCH><<<grid, block, 0, st>>>(a, many); break;
+    case KF_STORAGE_F16U16: raycast_kernel<KF_STORAGE_F16U16, BATCH><<<grid, block, 0, st>>>(a, many); break;
+    default: raycast_kernel<KF_STORAGE_RG16I, BATCH><<<grid, block, 0, st>>>(a, many); break;
   }
+}
+
+}  // namespace
+
+int kf_launch_raycast(kf_session* s) {
+  const RayArgs a = make_ray_args(s);
+  dim3 grid((a.W + 31) / 32, (a.H + kRayRows - 1) / kRayRows);
+  launch_ray<false>(s->cfg.storage, grid, s->stream, a, nullptr);
   KF_CUDA_TRY(s, cudaGetLastError());
   kf_note_launch(s);
+  return KF_OK;
+}
+
+// ---- batched: every member's raycast in one launch (blockIdx.z = member) ----
+int kf_batch_prepare_raycast(kf_batch* b) {
+  const int n = (int)b->members.size();
+  RayArgs* h = nullptr;
+  b->ray_args = kf_batch_table(b, sizeof(RayArgs) * n, reinterpret_cast<void**>(&h));
+  if (!b->ray_args) return KF_ERR_CAPACITY;
+  for (int e = 0; e < n; ++e) h[e] = make_ray_args(b->members[e]);
+  return KF_OK;
+}
+
+int kf_batch_launch_raycast(kf_batch* b, int n) {
+  kf_session* s0 = b->members[0];
+  dim3 grid((s0->W[0] + 31) / 32, (s0->H[0] + kRayRows - 1) / kRayRows, n);
+  launch_ray<true>(s0->cfg.storage, grid, b->stream, RayArgs{}, static_cast<const RayArgs*>(b->ray_args));
+  KF_CUDA_TRY(b, cudaGetLastError());
+  b->launches += 1;
   return KF_OK;
 }

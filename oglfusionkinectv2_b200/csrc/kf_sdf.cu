@@ -95,8 +95,16 @@ __device__ __forceinline__ void sdf_row(const SdfArgs& a, int l, size_t i, const
 
 constexpr int kWarps = KF_TRACK_THREADS / 32;
 
-template <int S>
-__global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
+// A batched launch: the blocks of entry e are those whose map word names e (as in
+// kf_icp.cu); every entry runs its own attempts, levels, iterations and barrier.
+struct SdfBatch {
+  const SdfArgs* args;
+  const uint32_t* block_map;  // per block: entry << 24 | blocks of the entry << 12 | index
+};
+
+template <int S, bool BATCH>
+__global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a_one, SdfBatch batch) {
+  __shared__ SdfArgs s_args;
   __shared__ double s_prev[16];     // m_pose_eig_prev
   __shared__ double s_result[6];
   __shared__ float s_T[16];
@@ -105,10 +113,23 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
   __shared__ double s_sums[32];
   __shared__ int s_flag, s_conv;
 
+  unsigned local, nb;  // this block's index among its entry's blocks, and their number
+  if constexpr (BATCH) {
+    const uint32_t m = batch.block_map[blockIdx.x];
+    local = m & 0xfffu;
+    nb = (m >> 12) & 0xfffu;
+    const int* src = reinterpret_cast<const int*>(batch.args + (m >> 24));
+    for (int k = threadIdx.x; k < (int)(sizeof(SdfArgs) / 4); k += blockDim.x)
+      reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
+    __syncthreads();
+  } else {
+    local = blockIdx.x;
+    nb = gridDim.x;
+  }
+  const SdfArgs& a = BATCH ? s_args : a_one;
   KfDevState* st = a.st;
-  if (a.gate && *(volatile const int*)a.gate == 0) return;  // uniform over the grid
+  if (a.gate && *(volatile const int*)a.gate == 0) return;  // uniform over the entry's blocks
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const unsigned nb = gridDim.x;
   const int attempts = a.recover ? st->lib_size : 1;
   if (tid < 16) s_prev[tid] = st->pose_eig[tid];
   __syncthreads();
@@ -132,7 +153,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
 #pragma unroll
         for (int k = 0; k < 28; ++k) acc[k] = 0.0f;
         const float e2 = a.q6 ? 2.0f : 1.0f;
-        for (int i = blockIdx.x * KF_TRACK_THREADS + tid; i < P; i += nb * KF_TRACK_THREADS) {
+        for (int i = local * KF_TRACK_THREADS + tid; i < P; i += nb * KF_TRACK_THREADS) {
           const int y = i / Wl, x = i - y * Wl;
           float row[8];
           if (a.q7 && x == Wl - 1) {
@@ -171,12 +192,12 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
           float v = 0.0f;
 #pragma unroll
           for (int w = 0; w < kWarps; ++w) v += s_warp[w][tid];
-          part[(size_t)blockIdx.x * 32 + tid] = v;
+          part[(size_t)local * 32 + tid] = v;
         }
 
         // grid barrier; then every block reduces the rows in the same fixed order and
         // solves the same system, so every block holds bit-identical results
-        ok = kf_grid_sync(st, nb * (gi + 1u), &s_flag);
+        ok = kf_grid_sync(st, &st->sdf_barrier_count, nb * (gi + 1u), &s_flag);
         if (!ok) break;
         ++gi;
         {
@@ -224,7 +245,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
           kf_mat4_mul(E, s_prev, Tn);
           for (int k = 0; k < 16; ++k) s_T[k] = (float)Tn[k];
           s_conv = ((ae != 0.0 && ae < 1e-3) || cn < 1e-3) ? 1 : 0;
-          if (blockIdx.x == 0) {
+          if (local == 0) {
             st->ae = ae;
             for (int k = 0; k < 32; ++k) st->sums[k] = s_sums[k];
           }
@@ -239,7 +260,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
     }
     if (!ok) break;
     // TrackSDF tail (:991-1012), block 0 writes the state
-    if (blockIdx.x == 0 && tid == 0) {
+    if (local == 0 && tid == 0) {
       double res[6], sum = 0.0;
       for (int k = 0; k < 6; ++k) { res[k] = s_result[k]; sum += res[k]; }
       if (isnan(sum))
@@ -261,13 +282,14 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS) sdf_kernel(SdfArgs a) {
     }
     found = tracked;
   }
-  if (blockIdx.x == 0 && tid == 0 && ok && a.recover) st->recover_found = found ? 1 : 0;
+  if (local == 0 && tid == 0 && ok && a.recover) st->recover_found = found ? 1 : 0;
 }
 
 }  // namespace
 
-int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy) {
-  (void)frame_policy;
+namespace {
+
+SdfArgs make_sdf_args(kf_session* s, int recover, int gated) {
   SdfArgs a;
   for (int l = 0; l < 3; ++l) {
     a.vertex[l] = s->d_vertex[l];
@@ -291,30 +313,66 @@ int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy) {
   a.st = s->d_state;
   a.recover = recover;
   a.gate = gated ? &s->d_state->need_recover : nullptr;
+  return a;
+}
 
-  const void* fn;
-  switch (s->cfg.storage) {
-    case KF_STORAGE_F32F32: fn = (const void*)sdf_kernel<KF_STORAGE_F32F32>; break;
-    case KF_STORAGE_F16U16: fn = (const void*)sdf_kernel<KF_STORAGE_F16U16>; break;
-    default: fn = (const void*)sdf_kernel<KF_STORAGE_RG16I>; break;
+template <bool BATCH>
+const void* sdf_fn(int storage) {
+  switch (storage) {
+    case KF_STORAGE_F32F32: return (const void*)sdf_kernel<KF_STORAGE_F32F32, BATCH>;
+    case KF_STORAGE_F16U16: return (const void*)sdf_kernel<KF_STORAGE_F16U16, BATCH>;
+    default: return (const void*)sdf_kernel<KF_STORAGE_RG16I, BATCH>;
   }
-  const int blocks = kf_occupancy_blocks(s, fn, KF_TRACK_THREADS, 0);
-  if (blocks <= 0) return KF_ERR_CUDA;
-  KF_CUDA_TRY(s, cudaMemsetAsync(&s->d_state->barrier_count, 0, 2 * sizeof(unsigned), s->stream));
+}
+
+template <bool BATCH>
+cudaError_t launch_sdf(int storage, int blocks, cudaStream_t stream, const SdfArgs& a, const SdfBatch& b) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(KF_TRACK_THREADS);
-  cfg.stream = s->stream;
+  cfg.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  switch (s->cfg.storage) {
-    case KF_STORAGE_F32F32: KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, sdf_kernel<KF_STORAGE_F32F32>, a)); break;
-    case KF_STORAGE_F16U16: KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, sdf_kernel<KF_STORAGE_F16U16>, a)); break;
-    default: KF_CUDA_TRY(s, cudaLaunchKernelEx(&cfg, sdf_kernel<KF_STORAGE_RG16I>, a)); break;
+  switch (storage) {
+    case KF_STORAGE_F32F32: return cudaLaunchKernelEx(&cfg, sdf_kernel<KF_STORAGE_F32F32, BATCH>, a, b);
+    case KF_STORAGE_F16U16: return cudaLaunchKernelEx(&cfg, sdf_kernel<KF_STORAGE_F16U16, BATCH>, a, b);
+    default: return cudaLaunchKernelEx(&cfg, sdf_kernel<KF_STORAGE_RG16I, BATCH>, a, b);
   }
+}
+
+}  // namespace
+
+int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy) {
+  (void)frame_policy;
+  const SdfArgs a = make_sdf_args(s, recover, gated);
+  const int blocks = kf_occupancy_blocks(s, sdf_fn<false>(s->cfg.storage), KF_TRACK_THREADS, 0);
+  if (blocks <= 0) return KF_ERR_CUDA;
+  KF_CUDA_TRY(s, cudaMemsetAsync(&s->d_state->sdf_barrier_count, 0, sizeof(unsigned), s->stream));
+  KF_CUDA_TRY(s, launch_sdf<false>(s->cfg.storage, blocks, s->stream, a, SdfBatch{nullptr, nullptr}));
   kf_note_launch(s);
+  return KF_OK;
+}
+
+// ---- batched: every member's gated recoverPose in one cooperative launch ----
+int kf_batch_prepare_sdf(kf_batch* b) {
+  const int n = (int)b->members.size();
+  SdfArgs* h = nullptr;
+  b->sdf_args = kf_batch_table(b, sizeof(SdfArgs) * n, reinterpret_cast<void**>(&h));
+  if (!b->sdf_args) return KF_ERR_CAPACITY;
+  for (int e = 0; e < n; ++e) h[e] = make_sdf_args(b->members[e], 1, 1);
+  kf_session* s0 = b->members[0];
+  const int total = kf_occupancy_blocks(s0, sdf_fn<true>(s0->cfg.storage), KF_TRACK_THREADS, 0);
+  if (total <= 0) return KF_ERR_CUDA;
+  b->sdf_blocks = total;
+  return kf_batch_block_map(b, total, &b->sdf_map);
+}
+
+int kf_batch_launch_sdf_recover(kf_batch* b) {
+  const SdfBatch batch = {static_cast<const SdfArgs*>(b->sdf_args), b->sdf_map};
+  KF_CUDA_TRY(b, launch_sdf<true>(b->members[0]->cfg.storage, b->sdf_blocks, b->stream, SdfArgs{}, batch));
+  b->launches += 1;
   return KF_OK;
 }

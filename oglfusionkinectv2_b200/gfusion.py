@@ -321,6 +321,65 @@ class GFusion:
         return p.value or 0
 
 
+class GFusionBatch:
+    """Batched frame steps over several GFusion sessions (kf_batch_*): one launch per stage
+    for all of them; each session's results equal stepping it alone."""
+
+    def __init__(self, max_sessions: int):
+        self.lib = L.load()
+        h = C.c_void_p()
+        L.check(self.lib.kf_batch_create(int(max_sessions), C.byref(h)), "kf_batch_create")
+        self._h = h
+        self.max_sessions = int(max_sessions)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.kf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != L.KF_OK:
+            msg = self.lib.kf_batch_last_error(self._h)
+            raise L.KfError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def frameStep(self, sessions, frames) -> np.ndarray:
+        """sessions: GFusion list; frames: uint16 H x W arrays (host).  Returns tracked flags."""
+        n = len(sessions)
+        hs = (C.c_void_p * n)(*[s.handle.value for s in sessions])
+        arrs = [np.ascontiguousarray(f, dtype=np.uint16) for f in frames]
+        ps = (C.c_void_p * n)(*[a.ctypes.data for a in arrs])
+        t = (C.c_int32 * n)()
+        self._check(self.lib.kf_batch_frame_step_u16(self._h, hs, ps, n, t), "kf_batch_frame_step_u16")
+        return np.array(list(t), dtype=bool)
+
+    def frameStepDevice(self, sessions, device_ptrs) -> np.ndarray:
+        """As frameStep, with each frame already in device memory (uint16 pointers)."""
+        n = len(sessions)
+        hs = (C.c_void_p * n)(*[s.handle.value for s in sessions])
+        ps = (C.c_void_p * n)(*[int(p) for p in device_ptrs])
+        t = (C.c_int32 * n)()
+        self._check(self.lib.kf_batch_frame_step_u16_device(self._h, hs, ps, n, t),
+                    "kf_batch_frame_step_u16_device")
+        return np.array(list(t), dtype=bool)
+
+    def stageTimes(self) -> np.ndarray:
+        """Device ms of the last step: pyramid, track, integrate, recover, raycast."""
+        a = (C.c_float * 5)()
+        self._check(self.lib.kf_batch_get_stage_times(self._h, a), "kf_batch_get_stage_times")
+        return np.array(list(a), dtype=np.float32)
+
+    def launchCount(self) -> int:
+        n = C.c_uint64()
+        self._check(self.lib.kf_batch_get_launch_count(self._h, C.byref(n)), "kf_batch_get_launch_count")
+        return int(n.value)
+
+
 class MCubes:
     """Marching-cubes extraction of a GFusion volume (mcubes.h:48-168)."""
 

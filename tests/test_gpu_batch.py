@@ -1,0 +1,129 @@
+"""Batched frame steps (kf_batch_*): several sessions of different volume sizes and scenes
+stepped together give the same results as each stepped alone.
+
+With the split-BF16 J^T J form the ICP sums are exact fixed-point integers, so poses,
+raycast maps and volumes are bit-identical whatever the batch; membership may change from
+step to step (continuous batching)."""
+import numpy as np
+import pytest
+
+from helpers import small_workload
+from oglfusionkinectv2_b200 import GFusion, GFusionBatch, _lib as L
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [64, 96, 128, 80]
+SEEDS = [0xC0FFEE + 1, 0xC0FFEE + 21, 0xC0FFEE + 71, 0xC0FFEE + 31]
+
+
+def workloads(n_frames, storage=L.KF_STORAGE_F16U16, jtj=L.KF_JTJ_SPLIT_BF16):
+    return [small_workload(n_frames, size=sz, storage=storage, jtj=jtj, quirks=L.KF_QUIRKS_TRACKING, seed=sd)
+            for sz, sd in zip(SIZES, SEEDS)]
+
+
+def fresh(ws):
+    gs = []
+    for w in ws:
+        g = GFusion(w.config, w.intrinsics)
+        g.Reset(w.poses[0])
+        gs.append(g)
+    return gs
+
+
+def snapshot(g):
+    return g.getPose(), g.getVerts(), g.getNorms(), g.getVolumeRaw()
+
+
+def assert_same(a, b):
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_batch_equals_alone_bit_exact():
+    F = 6
+    ws = workloads(F)
+    frames = [[w.frame(k) for k in range(F)] for w in ws]
+    alone = fresh(ws)
+    tr_alone = np.array([[g.frameStep(frames[i][k]) for k in range(F)] for i, g in enumerate(alone)])
+    together = fresh(ws)
+    batch = GFusionBatch(8)
+    tr_batch = np.array([batch.frameStep(together, [frames[i][k] for i in range(len(ws))]) for k in range(F)]).T
+    np.testing.assert_array_equal(tr_alone, tr_batch)
+    assert tr_batch[:, -1].all()
+    for ga, gb in zip(alone, together):
+        assert_same(snapshot(ga), snapshot(gb))
+    t = batch.stageTimes()
+    assert (t >= 0).all() and t[1] > 0
+
+
+def test_batch_membership_changes():
+    """Sessions join and leave between steps; each still matches its alone run."""
+    F = 5
+    ws = workloads(F)
+    frames = [[w.frame(k) for k in range(F)] for w in ws]
+    alone = fresh(ws)
+    for i, g in enumerate(alone):
+        for k in range(F):
+            g.frameStep(frames[i][k])
+    mixed = fresh(ws)
+    batch = GFusionBatch(4)
+    nxt = [0] * len(ws)
+    plan = [[0, 1, 2, 3], [1], [0, 2], [3, 2, 1], [0], [0, 1, 2, 3], [2, 3], [1, 3], [0, 1, 2, 3], [0, 2, 3], [1]]
+    for members in plan:
+        members = [m for m in members if nxt[m] < F]
+        if not members:
+            continue
+        batch.frameStep([mixed[m] for m in members], [frames[m][nxt[m]] for m in members])
+        for m in members:
+            nxt[m] += 1
+    for i, g in enumerate(mixed):
+        while nxt[i] < F:
+            g.frameStep(frames[i][nxt[i]])  # the rest alone
+            nxt[i] += 1
+    for ga, gb in zip(alone, mixed):
+        assert_same(snapshot(ga), snapshot(gb))
+
+
+def test_batch_fp32_jtj_within_tolerance():
+    """The FP32 J^T J form sums per block in FP32, so a different block split may round
+    differently: poses agree within the parity tolerance (0.1 mm / 0.01 deg)."""
+    F = 5
+    # scenes and sizes whose tracking is well conditioned (a few mm from the ground truth)
+    ws = [small_workload(F, size=sz, storage=L.KF_STORAGE_F32F32, jtj=L.KF_JTJ_FP32, quirks=L.KF_QUIRKS_TRACKING,
+                         seed=0xC0FFEE + sd) for sz, sd in ((128, 21), (112, 71), (96, 1))]
+    frames = [[w.frame(k) for k in range(F)] for w in ws]
+    alone = fresh(ws)
+    for i, g in enumerate(alone):
+        for k in range(F):
+            g.frameStep(frames[i][k])
+    together = fresh(ws)
+    batch = GFusionBatch(3)
+    for k in range(F):
+        batch.frameStep(together, [frames[i][k] for i in range(len(ws))])
+    for ga, gb in zip(alone, together):
+        Pa, Pb = ga.getPose(), gb.getPose()
+        assert np.abs(Pa[:3, 3] - Pb[:3, 3]).max() < 1e-4
+        R = Pa[:3, :3].T @ Pb[:3, :3]
+        assert np.degrees(np.arccos(np.clip((np.trace(R) - 1) / 2, -1, 1))) < 0.01
+
+
+def test_batch_rejects_bad_membership():
+    ws = workloads(1)
+    gs = fresh(ws[:2])
+    f = ws[0].frame(0)
+    batch = GFusionBatch(2)
+    with pytest.raises(L.KfError) as e:
+        batch.frameStep([gs[0], gs[0]], [f, f])
+    assert e.value.status == L.KF_ERR_INVALID_ARGUMENT
+    other = small_workload(1, size=64, storage=L.KF_STORAGE_F32F32, jtj=L.KF_JTJ_SPLIT_BF16)
+    g32 = GFusion(other.config, other.intrinsics)
+    g32.Reset(other.poses[0])
+    with pytest.raises(L.KfError) as e:
+        batch.frameStep([gs[0], g32], [f, f])
+    assert e.value.status == L.KF_ERR_INVALID_ARGUMENT
+    g3 = fresh(ws[2:3])[0]
+    with pytest.raises(L.KfError) as e:
+        batch.frameStep([gs[0], gs[1], g3], [f, f, f])
+    assert e.value.status == L.KF_ERR_CAPACITY
+    # a valid step still works after the refusals
+    assert batch.frameStep(gs, [f, f]).shape == (2,)
