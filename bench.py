@@ -45,6 +45,10 @@ def parse():
     p.add_argument("--cpu-frames", type=int, default=4, help="oracle frames timed for cpu_baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--form", choices=["plain", "batched", "served"], default="plain",
+                   help="plain: the single-session frame step (default line); batched: config 3; served: config 4")
+    p.add_argument("--sessions", type=int, default=64, help="batched form: sessions per batch")
+    p.add_argument("--duration", type=float, default=30.0, help="served form: seconds of arrivals")
     return p.parse_args()
 
 
@@ -193,6 +197,219 @@ def cpu_baseline(args, w, frames_by_idx):
                       f"after {warm} untimed frames (FP64 oracle, OpenMP, {cores} threads)"}
 
 
+def rmse_translation(est, gt) -> float:
+    d = np.array([np.linalg.norm(np.asarray(a)[:3, 3] - np.asarray(b)[:3, 3]) for a, b in zip(est, gt)])
+    return float(np.sqrt(np.mean(d * d))) if len(d) else 0.0
+
+
+def run_batched(args):
+    """Config 3: sessions of uneven volume sizes stepped together (one launch per stage),
+    against the same sessions stepped one at a time through the single-session path."""
+    import torch
+    from oglfusionkinectv2_b200 import GFusion, GFusionBatch, synth
+    K, W = args.steps, max(3, args.warmup)
+    K_plain = min(K, 20)
+    n_frames = W + K + 2 + K_plain
+    ws = synth.batched_c3(args.sessions, n_frames=n_frames)
+    torch.cuda.set_device(0)
+    log(f"rendering {len(ws)} x {n_frames} frames on the device")
+    frames = [w.frames_torch(range(n_frames), "cuda") for w in ws]
+    torch.cuda.synchronize()
+    fbytes = 512 * 424 * 2
+    gs = []
+    for w in ws:
+        g = GFusion(w.config, w.intrinsics)
+        g.Reset(w.poses[0])
+        gs.append(g)
+    batch = GFusionBatch(len(gs))
+    ptr = lambda i: [f.data_ptr() + i * fbytes for f in frames]
+    est = [[] for _ in gs]
+    for i in range(W):
+        batch.frameStepDevice(gs, ptr(i))
+        for j, P in enumerate(batch.poses(len(gs))):
+            est[j].append(P)
+    torch.cuda.synchronize()
+    lat, stage = [], np.zeros(5)
+    launches0 = batch.launchCount()
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        for i in range(W, W + K):
+            ts = time.perf_counter()
+            batch.frameStepDevice(gs, ptr(i))  # synchronises: the step's results are on the host
+            lat.append(1000 * (time.perf_counter() - ts))
+            stage += batch.stageTimes()
+            for j, P in enumerate(batch.poses(len(gs))):
+                est[j].append(P)
+        wall = time.perf_counter() - t0
+    launches = batch.launchCount() - launches0
+    # the plain path: the same sessions, one frame step at a time (two untimed frames build
+    # each session's frame graphs)
+    for i in range(W + K, W + K + 2):
+        for j, g in enumerate(gs):
+            g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
+            est[j].append(g.getPose())
+    tp = time.perf_counter()
+    for i in range(W + K + 2, W + K + 2 + K_plain):
+        for j, g in enumerate(gs):
+            g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
+    plain_wall = time.perf_counter() - tp
+    # the plain configuration (FP32 TSDF + weight, FP32 J^T J), same scenes and sizes, one
+    # session at a time through the single-session frame step
+    from oglfusionkinectv2_b200 import _lib as L
+    g32 = []
+    for w in ws:
+        c = w.config
+        c32 = type(c)(**{**c.__dict__, "storage": L.KF_STORAGE_F32F32, "jtj": L.KF_JTJ_FP32})
+        g = GFusion(c32, w.intrinsics)
+        g.Reset(w.poses[0])
+        g32.append(g)
+    for i in range(W):
+        for j, g in enumerate(g32):
+            g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
+    tq = time.perf_counter()
+    for i in range(W, W + K_plain):
+        for j, g in enumerate(g32):
+            g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
+    plain32_wall = time.perf_counter() - tq
+    del g32
+    ate = [rmse_translation(e, w.poses[:len(e)]) for e, w in zip(est, ws)]
+    sizes = [w.config.volumeSize[0] for w in ws]
+    value = len(gs) * K / wall
+    plain = len(gs) * K_plain / plain_wall
+    line = {"metric": f"aggregate frames/s, batched form ({len(gs)} sessions, 128-384^3 F16U16)",
+            "value": value, "unit": "frames/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": 1000 * wall / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "c3_batched", "sessions": len(gs),
+                       "sizes": {str(z): sizes.count(z) for z in sorted(set(sizes))},
+                       "storage": "f16u16", "jtj": "bf16", "depth": "512x424 uint16 (device-resident)",
+                       "l2": "volumes 0.5 GB-5 GB total > L2"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "stage_ms_per_step": dict(zip(["pyramid", "track", "integrate", "recover", "raycast"],
+                                          (stage / K).tolist())),
+            "plain_one_at_a_time": {"value": plain, "unit": "frames/s", "steps": K_plain,
+                                    "form": "same sessions (F16U16, split-BF16), single-session frame step",
+                                    "ratio_batched_over_plain": value / plain},
+            "plain_fp32_one_at_a_time": {"value": len(ws) * K_plain / plain32_wall, "unit": "frames/s",
+                                         "steps": K_plain,
+                                         "form": "same scenes and sizes, FP32 TSDF + FP32 J^T J, single-session frame step",
+                                         "ratio_batched_over_plain": value / (len(ws) * K_plain / plain32_wall)},
+            "ate_mm": {"mean": 1000 * float(np.mean(ate)), "max": 1000 * float(np.max(ate))},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def serve_pass(server, arrivals, seqs, gt, duration, fbytes, max_slots):
+    """Drive `server` in real time for `duration` seconds: sessions arrive per `arrivals`,
+    stream their frames at 30 Hz from the device-resident sequences, and are closed when
+    done.  Returns (frames stepped, sessions admitted, max admission wait, per-session
+    translation errors)."""
+    L_seq = seqs[0].shape[0]
+    waiting = list(arrivals)
+    active = {}  # sid -> [arrival, t_admit, frames, scene, submitted, errs]
+    errs_done = []
+    max_wait = 0.0
+    t0 = server.now()
+    frames = 0
+    admitted = 0
+    while True:
+        t = server.now() - t0
+        if t > duration:
+            break
+        while waiting and waiting[0].t <= t:
+            a = waiting[0]
+            cfg = gt[a.scene][1]
+            cfg.volumeSize = (a.size, a.size, a.size)
+            sid = server.open(cfg, gt[a.scene][2], gt[a.scene][0][0])
+            if sid is None:
+                break
+            waiting.pop(0)
+            max_wait = max(max_wait, t - a.t)
+            active[sid] = [a, t, a.frames, a.scene, 0, []]
+            admitted += 1
+        for sid, st in active.items():
+            a, ta, n, sc, sub, _ = st
+            due = min(n, int((t - ta) * 30.0) + 1)
+            while sub < due:
+                p = sub % (2 * L_seq - 2)
+                idx = p if p < L_seq else 2 * L_seq - 2 - p
+                server.submit_device(sid, seqs[sc].data_ptr() + idx * fbytes)
+                sub += 1
+            st[4] = sub
+        n_done = server.step()
+        frames += n_done
+        if n_done:
+            ids, poses, _ = server.last_step(max_slots)
+            for sid, P in zip(ids.tolist(), poses):
+                a, ta, n, sc, sub, errs = active[sid]
+                done = len(errs) + 1
+                p = (done - 1) % (2 * L_seq - 2)
+                idx = p if p < L_seq else 2 * L_seq - 2 - p
+                errs.append(float(np.linalg.norm(P[:3, 3] - gt[sc][0][idx][:3, 3])))
+                if done >= n:
+                    errs_done.append(errs)
+                    server.close_session(sid)
+                    del active[sid]
+    errs_all = errs_done + [st[5] for st in active.values()]
+    for sid in list(active):
+        server.close_session(sid)
+    return frames, admitted, max_wait, errs_all
+
+
+def run_served(args):
+    """Config 4: Poisson session arrivals, 30 Hz frame streams, admission by slots and free
+    device memory, continuous batching; against the same arrival process stepped one
+    session at a time."""
+    import torch
+    from oglfusionkinectv2_b200 import GFusionServer, synth
+    torch.cuda.set_device(0)
+    n_scenes, L_seq = 16, 300
+    arrivals = synth.served_c4(args.duration, n_scenes=n_scenes)
+    scenes = [synth.session_scene(L_seq, splitmix(0xC0FFEE + 4000 + k), 128, phase_deg=22.5 * k,
+                                  deg_per_frame=0.5 if k % 2 else -0.5) for k in range(n_scenes)]
+    log(f"rendering {n_scenes} x {L_seq} frames on the device; {len(arrivals)} arrivals in {args.duration} s")
+    seqs = [w.frames_torch(range(L_seq), "cuda") for w in scenes]
+    torch.cuda.synchronize()
+    gt = [(w.poses, w.config, w.intrinsics) for w in scenes]
+    fbytes = 512 * 424 * 2
+    slots = 64
+    results = {}
+    for name, max_batch in (("served", 64), ("plain_one_at_a_time", 1)):
+        server = GFusionServer(max_sessions=slots, max_batch=max_batch)
+        with ClockSampler(0) as clk:
+            frames, admitted, max_wait, errs = serve_pass(server, arrivals, seqs, gt, args.duration, fbytes, slots)
+        st = server.stats()
+        server.close()
+        flat = [e for es in errs for e in es]
+        results[name] = {"frames_per_s": frames / args.duration, "frames": frames, "p50_ms": st["p50_ms"],
+                         "p99_ms": st["p99_ms"], "max_ms": st["max_ms"], "sessions_admitted": admitted,
+                         "max_admission_wait_s": max_wait, "busy_fraction": st["busy_s"] / args.duration,
+                         "pose_err_mm": {"median": 1000 * float(np.median(flat)) if flat else None,
+                                         "p99": 1000 * float(np.percentile(flat, 99)) if flat else None},
+                         "clocks": clk.summary()}
+        log(f"{name}: {results[name]['frames_per_s']:.0f} frames/s p50 {st['p50_ms']:.1f} ms p99 {st['p99_ms']:.1f} ms")
+    sv, pl = results["served"], results["plain_one_at_a_time"]
+    line = {"metric": "aggregate frames/s, served form (Poisson 20 sessions/s, 30 Hz streams, 128-512^3)",
+            "value": sv["frames_per_s"], "unit": "frames/s", "n_gpus": 1, "steps": sv["frames"], "warmup": 0,
+            "ms_per_step": 1000.0 / sv["frames_per_s"] if sv["frames_per_s"] else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "c4_served", "duration_s": args.duration, "arrivals": len(arrivals),
+                       "slots": slots, "max_batch": 64, "storage": "f16u16", "jtj": "bf16",
+                       "scenes": f"{n_scenes} seeded sequences of {L_seq} frames, replayed back and forth"},
+            "latency_ms": {"p50": sv["p50_ms"], "p99": sv["p99_ms"], "max": sv["max_ms"]},
+            "served": sv, "plain_one_at_a_time": pl,
+            "ratio_served_over_plain": sv["frames_per_s"] / pl["frames_per_s"] if pl["frames_per_s"] else None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def splitmix(x: int) -> int:
+    from oglfusionkinectv2_b200 import synth
+    return synth.splitmix64(x) & 0xFFFFFFFF
+
+
 def run_reference(args):
     """--impl reference: the reference algorithm's CPU port on this host, same workload."""
     rank = int(os.environ.get("RANK", "0"))
@@ -235,6 +452,10 @@ def log(msg):
 def main():
     faulthandler.enable()
     args = parse()
+    if args.form == "batched" and args.impl == "ours":
+        return run_batched(args)
+    if args.form == "served" and args.impl == "ours":
+        return run_served(args)
     if args.impl == "reference":
         return run_reference(args)
     rank = int(os.environ.get("RANK", "0"))

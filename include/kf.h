@@ -248,9 +248,63 @@ KF_API int kf_batch_frame_step_u16(kf_batch* b, kf_session* const* sessions,
 KF_API int kf_batch_frame_step_u16_device(kf_batch* b, kf_session* const* sessions,
                                           const uint16_t* const* device_depth_mm, int n,
                                           int32_t* tracked);
+/* The poses (camera-to-world, column-major) of the last step's first n sessions, in step
+ * order, without another device round trip. */
+KF_API int kf_batch_get_poses(kf_batch* b, int n, double* poses16);
 /* Device ms of the last step's stages: pyramid, track, integrate, recover, raycast. */
 KF_API int kf_batch_get_stage_times(kf_batch* b, float* ms5);
 KF_API int kf_batch_get_launch_count(kf_batch* b, uint64_t* launches);
+
+/* ---- served form (no counterpart in the reference) --------------------------------------
+ * A request loop over resident sessions: kf_server_open admits a session while a slot and
+ * the device-memory budget allow (KF_ERR_ADMISSION otherwise: retry after a close), frames
+ * are queued with their arrival time as they come, and each kf_server_step runs one
+ * batched frame step over the sessions with a waiting frame (oldest waiting frame first,
+ * up to max_batch): continuous batching.  Frame latency = arrival to pose on the host.
+ * All sessions use the server's storage and J^T J form and track by ICP. */
+typedef struct kf_server_config {
+  uint64_t hbm_budget_bytes; /* admission budget; 0 = free device memory at creation - 8 GiB */
+  int32_t max_sessions;      /* resident session slots                                     */
+  int32_t max_batch;         /* sessions per batched step (<= KF_BATCH_MAX_SESSIONS)       */
+  int32_t storage;           /* KF_STORAGE_* of every session (default F16U16)             */
+  int32_t jtj;               /* KF_JTJ_* of every session (default split-BF16)             */
+  int32_t reserved[8];
+} kf_server_config;
+typedef struct kf_server_stats_t {
+  uint64_t frames;           /* frames stepped since the last reset                         */
+  uint64_t steps;            /* batched steps                                               */
+  double busy_s;             /* seconds spent in batched steps                              */
+  double p50_ms, p99_ms, max_ms; /* frame latency (arrival -> pose on the host)             */
+  uint64_t bytes_in_use;     /* admitted sessions' device bytes                             */
+  int32_t active_sessions;
+  int32_t reserved[7];
+} kf_server_stats_t;
+typedef struct kf_server kf_server;
+KF_API int kf_server_config_default(kf_server_config* cfg);
+KF_API int kf_server_create(const kf_server_config* cfg, kf_server** out);
+KF_API int kf_server_destroy(kf_server* v);
+KF_API const char* kf_server_last_error(const kf_server* v);
+KF_API double kf_server_now(void); /* the server's clock (seconds, monotonic) */
+/* cfg's storage, jtj and tracking are replaced by the server's form. */
+KF_API int kf_server_open(kf_server* v, const kf_config* cfg, const kf_intrinsics* intr,
+                          const double pose[16], int* session_id);
+/* The session's slot is freed at once; its device memory is kept for the next admission of
+ * the same volume size, and released when the budget needs it (or at kf_server_destroy). */
+KF_API int kf_server_close(kf_server* v, int session_id);
+/* Queue a frame; it arrives now.  Host frames are copied (up to 8 waiting per session);
+ * device frames are read in place and must stay valid until the step that uses them. */
+KF_API int kf_server_submit(kf_server* v, int session_id, const uint16_t* host_depth_mm);
+KF_API int kf_server_submit_device(kf_server* v, int session_id, const uint16_t* device_depth_mm);
+KF_API int kf_server_step(kf_server* v, int* frames_done);
+KF_API int kf_server_get_pose(kf_server* v, int session_id, double pose16[16], int* tracked,
+                              uint64_t* frames_done);
+/* The sessions of the last kf_server_step (up to max_n): ids, poses (16 doubles each,
+ * column-major) and tracked flags, in step order; *n receives the count. */
+KF_API int kf_server_last_step(kf_server* v, int max_n, int* session_ids, double* poses16,
+                               int32_t* tracked, int* n);
+KF_API int kf_server_pending(kf_server* v, int session_id, int* queued);
+KF_API int kf_server_stats(kf_server* v, kf_server_stats_t* stats);
+KF_API int kf_server_reset_stats(kf_server* v);
 
 /* ---- marching cubes (MCubes, mcubes.cpp:206-509) ---------------------------------------
  * kf_mc_extract = setIsolevel + generateMarchingCubes; *n_triangles is the triangle count

@@ -2,7 +2,7 @@
 philipNoonan/oglFusionKinectV2 (C ABI in include/kf.h, CUDA kernels in csrc/)."""
 from . import _lib
 from ._lib import KfError, load
-from .gfusion import GFusion, GFusionBatch, GFusionConfig, Intrinsics, MCubes, decode_volume, prefix_sum_device
+from .gfusion import GFusion, GFusionBatch, GFusionConfig, GFusionServer, Intrinsics, MCubes, decode_volume, prefix_sum_device
 
-__all__ = ["GFusion", "GFusionBatch", "GFusionConfig", "Intrinsics", "MCubes", "KfError", "load",
+__all__ = ["GFusion", "GFusionBatch", "GFusionConfig", "GFusionServer", "Intrinsics", "MCubes", "KfError", "load",
            "decode_volume", "prefix_sum_device", "_lib"]

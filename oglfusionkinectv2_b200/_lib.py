@@ -144,10 +144,39 @@ SIGNATURES = {
     "kf_batch_frame_step_u16": (_I, [_P, C.POINTER(_P), C.POINTER(_P), _I, C.POINTER(C.c_int32)]),
     "kf_batch_frame_step_u16_device": (_I, [_P, C.POINTER(_P), C.POINTER(_P), _I, C.POINTER(C.c_int32)]),
     "kf_batch_get_stage_times": (_I, [_P, C.POINTER(C.c_float)]),
+    "kf_batch_get_poses": (_I, [_P, _I, _P]),
     "kf_batch_get_launch_count": (_I, [_P, C.POINTER(C.c_uint64)]),
+    "kf_server_config_default": (_I, [_P]),
+    "kf_server_create": (_I, [_P, C.POINTER(_P)]),
+    "kf_server_destroy": (_I, [_P]),
+    "kf_server_last_error": (C.c_char_p, [_P]),
+    "kf_server_now": (C.c_double, []),
+    "kf_server_open": (_I, [_P, _P, _P, _P, C.POINTER(_I)]),
+    "kf_server_close": (_I, [_P, _I]),
+    "kf_server_submit": (_I, [_P, _I, _P]),
+    "kf_server_submit_device": (_I, [_P, _I, _P]),
+    "kf_server_step": (_I, [_P, C.POINTER(_I)]),
+    "kf_server_get_pose": (_I, [_P, _I, _P, C.POINTER(_I), C.POINTER(C.c_uint64)]),
+    "kf_server_pending": (_I, [_P, _I, C.POINTER(_I)]),
+    "kf_server_last_step": (_I, [_P, _I, _P, _P, _P, C.POINTER(_I)]),
+    "kf_server_stats": (_I, [_P, _P]),
+    "kf_server_reset_stats": (_I, [_P]),
 }
 
 _lib = None
+
+
+class ServerConfig(C.Structure):
+    """kf_server_config (kf.h)."""
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_sessions", C.c_int32), ("max_batch", C.c_int32),
+                ("storage", C.c_int32), ("jtj", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
+class ServerStats(C.Structure):
+    """kf_server_stats_t (kf.h)."""
+    _fields_ = [("frames", C.c_uint64), ("steps", C.c_uint64), ("busy_s", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("bytes_in_use", C.c_uint64), ("active_sessions", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 def load(path: str = LIB_PATH) -> C.CDLL:

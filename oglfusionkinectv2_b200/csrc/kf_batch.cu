@@ -58,8 +58,17 @@ int check_members(kf_batch* b, kf_session* const* ss, int n) {
   return KF_OK;
 }
 
+bool same_members(const kf_batch* b, kf_session* const* ss, int n) {
+  if ((int)b->members.size() != n) return false;
+  for (int e = 0; e < n; ++e)
+    if (b->members[e] != ss[e] || b->member_keys[e] != std::make_pair(ss[e]->uid, ss[e]->layout)) return false;
+  return true;
+}
+
 int rebuild_tables(kf_batch* b, kf_session* const* ss, int n) {
   b->members.assign(ss, ss + n);
+  b->member_keys.resize(n);
+  for (int e = 0; e < n; ++e) b->member_keys[e] = std::make_pair(ss[e]->uid, ss[e]->layout);
   b->table_used = 0;
   KfDevState** hs = nullptr;
   b->states = static_cast<KfDevState* const*>(kf_batch_table(b, sizeof(KfDevState*) * n, reinterpret_cast<void**>(&hs)));
@@ -69,6 +78,7 @@ int rebuild_tables(kf_batch* b, kf_session* const* ss, int n) {
   if ((rc = kf_batch_prepare_pyramid(b)) || (rc = kf_batch_prepare_icp(b)) || (rc = kf_batch_prepare_integrate(b)) ||
       (rc = kf_batch_prepare_sdf(b)) || (rc = kf_batch_prepare_raycast(b))) {
     b->members.clear();
+    b->member_keys.clear();
     return bfail(b, rc, "batch tables: too many sessions for the table or the co-resident grid");
   }
   KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_table, b->h_table, b->table_used, cudaMemcpyHostToDevice, b->stream));
@@ -86,18 +96,28 @@ int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth,
   int cur = 0;
   KF_CUDA_TRY(b, cudaGetDevice(&cur));
   if (cur != b->device) KF_CUDA_TRY(b, cudaSetDevice(b->device));
-  const bool same = (int)b->members.size() == n && std::equal(ss, ss + n, b->members.begin());
-  if (!same && (rc = rebuild_tables(b, ss, n))) return rc;
+  // a destroyed session's address may come back for a new one, and a session may
+  // reallocate its buffers: the tables are keyed by (address, uid, layout)
+  if (!same_members(b, ss, n) && (rc = rebuild_tables(b, ss, n))) return rc;
   // a member's own stream may still hold work (an asynchronous frame step)
   for (int e = 0; e < n; ++e)
     if (cudaStreamQuery(ss[e]->stream) != cudaSuccess) KF_CUDA_TRY(b, cudaStreamSynchronize(ss[e]->stream));
-  const size_t px = (size_t)ss[0]->W[0] * ss[0]->H[0];
-  for (int e = 0; e < n; ++e)
-    KF_CUDA_TRY(b, cudaMemcpyAsync(ss[e]->d_depth_u16, depth[e], px * 2, kind, b->stream));
+  const uint16_t* const* inputs = nullptr;
+  if (kind == cudaMemcpyHostToDevice) {
+    const size_t px = (size_t)ss[0]->W[0] * ss[0]->H[0];
+    for (int e = 0; e < n; ++e)
+      KF_CUDA_TRY(b, cudaMemcpyAsync(ss[e]->d_depth_u16, depth[e], px * 2, kind, b->stream));
+  } else {
+    // device frames are read in place: one small upload of their addresses
+    for (int e = 0; e < n; ++e) b->h_inputs[e] = depth[e];
+    KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_inputs, b->h_inputs, n * sizeof(uint16_t*), cudaMemcpyHostToDevice,
+                                   b->stream));
+    inputs = b->d_inputs;
+  }
   KF_CUDA_TRY(b, cudaEventRecord(b->ev[0], b->stream));
   batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
   KF_CUDA_TRY(b, cudaGetLastError());
-  if ((rc = kf_batch_launch_pyramid(b, n))) return rc;
+  if ((rc = kf_batch_launch_pyramid(b, n, inputs))) return rc;
   KF_CUDA_TRY(b, cudaEventRecord(b->ev[1], b->stream));
   if ((rc = kf_batch_launch_icp(b))) return rc;
   KF_CUDA_TRY(b, cudaEventRecord(b->ev[2], b->stream));
@@ -115,6 +135,7 @@ int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth,
   KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
   for (int i = 0; i < 5; ++i) KF_CUDA_TRY(b, cudaEventElapsedTime(&b->stage_ms[i], b->ev[i], b->ev[i + 1]));
   b->steps += 1;
+  b->last_n = n;
   int first_err = KF_OK;
   for (int e = 0; e < n; ++e) {
     kf_session* s = ss[e];
@@ -137,6 +158,8 @@ void free_batch(kf_batch* b) {
   cudaFreeHost(b->h_table);
   cudaFree(b->d_heads);
   cudaFreeHost(b->h_heads);
+  cudaFree(b->d_inputs);
+  cudaFreeHost(b->h_inputs);
   for (auto& e : b->ev)
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -175,6 +198,10 @@ int kf_batch_create(int max_sessions, kf_batch** out) {
   const size_t hb = (size_t)max_sessions * KF_STATE_RESULT_BYTES;
   if (cudaMallocHost((void**)&b->h_heads, hb) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
   if (cudaMalloc((void**)&b->d_heads, hb) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  if (cudaMallocHost((void**)&b->h_inputs, max_sessions * sizeof(uint16_t*)) != cudaSuccess)
+    return bail(KF_ERR_OUT_OF_MEMORY);
+  if (cudaMalloc((void**)&b->d_inputs, max_sessions * sizeof(uint16_t*)) != cudaSuccess)
+    return bail(KF_ERR_OUT_OF_MEMORY);
   *out = b;
   return KF_OK;
 }
@@ -202,6 +229,14 @@ int kf_batch_frame_step_u16_device(kf_batch* b, kf_session* const* sessions, con
 int kf_batch_get_stage_times(kf_batch* b, float* ms) {
   if (!b || !ms) return KF_ERR_INVALID_ARGUMENT;
   for (int i = 0; i < 5; ++i) ms[i] = b->stage_ms[i];
+  return KF_OK;
+}
+
+int kf_batch_get_poses(kf_batch* b, int n, double* poses) {
+  if (!b || !poses || n < 0) return KF_ERR_INVALID_ARGUMENT;
+  if (n > b->last_n) return bfail(b, KF_ERR_INVALID_ARGUMENT, "more poses than the last step had sessions");
+  for (int e = 0; e < n; ++e)
+    std::memcpy(poses + 16 * e, b->h_heads + (size_t)e * KF_STATE_RESULT_BYTES, 16 * sizeof(double));
   return KF_OK;
 }
 

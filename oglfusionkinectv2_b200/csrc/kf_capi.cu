@@ -12,6 +12,8 @@
 #include <mutex>
 #include <new>
 
+#include <atomic>
+
 #include "kf_internal.cuh"
 
 namespace {
@@ -165,6 +167,7 @@ void set_pose_fields(kf_session* s, const double* pose, bool reset_eig) {
 }
 
 int alloc_volume(kf_session* s) {
+  s->layout += 1;
   cudaFree(s->d_vol);
   s->d_vol = nullptr;
   cudaFree(s->d_bricks);
@@ -415,6 +418,8 @@ int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out)
   }
   kf_session* s = new (std::nothrow) kf_session();
   if (!s) return KF_ERR_OUT_OF_MEMORY;
+  static std::atomic<uint64_t> next_uid{1};
+  s->uid = next_uid.fetch_add(1);
   s->cfg = *cfg;
   if (s->cfg.integrate_every <= 0) s->cfg.integrate_every = 1;
   s->intr = *intr;
@@ -495,6 +500,9 @@ int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
   }
   if ((rc = pull_state(s))) return rc;
   s->h_state->lib_size = 0;  // poseLibrary.resize(0)
+  // the ICP accumulation centre is carried from frame to frame; a new reconstruction starts
+  // from the camera origin, as a new session does
+  for (int k = 0; k < 3; ++k) s->h_state->icp_center_cam[k] = 0.0;
   set_pose_fields(s, pose, true);
   // the app's "Reset Volume" (kinect.cpp:446-477): reset = true, counter = 0, then a
   // raycast of the empty volume, i.e. zero reference maps
@@ -533,7 +541,7 @@ int kf_set_pose(kf_session* s, const double pose[16]) {
 
 int kf_get_pose(kf_session* s, double pose[16]) {
   if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
-  int rc = pull_state(s);
+  int rc = pull_state_head(s);
   if (rc) return rc;
   std::memcpy(pose, s->h_state->pose, 16 * sizeof(double));
   return KF_OK;
@@ -547,6 +555,7 @@ int kf_set_config(kf_session* s, const kf_config* cfg) {
   const bool realloc = cfg->nx != s->cfg.nx || cfg->ny != s->cfg.ny || cfg->nz != s->cfg.nz ||
                        cfg->storage != s->cfg.storage;
   s->cfg = *cfg;
+  s->layout += 1;  // kernel arguments derived from the configuration change
   if (s->cfg.integrate_every <= 0) s->cfg.integrate_every = 1;
   drop_graph(s);
   if (realloc) {

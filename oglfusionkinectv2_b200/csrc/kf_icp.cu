@@ -199,9 +199,9 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
     const int Wl = a.W[level], Hl = a.H[level];
     const int P = Wl * Hl;
     for (int it = 0; it < a.iters[level]; ++it) {
-      float T[16], V[16], c[3];
-#pragma unroll
-      for (int k = 0; k < 16; ++k) { T[k] = s_T[k]; V[k] = s_V[k]; }
+      // Ttrack and view stay in shared memory (broadcast reads), which leaves the registers
+      // for two pixels in flight per thread
+      float c[3];
       c[0] = s_c[0]; c[1] = s_c[1]; c[2] = s_c[2];
 
       // ---------------- track + accumulate ----------------
@@ -212,33 +212,9 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       float pacc[4] = {0.f, 0.f, 0.f, 0.f};  // FP32 path: valid count, sum of world points
       // split-BF16 path: fixed-point sums of M[g][2t], M[g][2t+1] and of q_g (lane g, t)
       long long fx0 = 0, fx1 = 0, fxq = 0;
-      const int stride = nb * KF_TRACK_THREADS;
-      const float4* Nl = a.normal[level];
-      const float4* Vl = a.vertex[level];
-      int base = (local * kWarps + warp) * 32;
-      // the next pass's normal and vertex are in flight while this pass gathers the
-      // reference maps
-      float4 nn = make_float4(2.0f, 0.f, 0.f, 0.f), vn = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (base + lane < P) {
-        nn = __ldg(Nl + base + lane);
-        vn = __ldg(Vl + base + lane);
-      }
-      for (; base < P; base += stride) {
-        const int i = base + lane;
-        const float4 n = nn, v = vn;
-        if (i + stride < P) {
-          nn = __ldg(Nl + i + stride);
-          vn = __ldg(Vl + i + stride);
-        }
-        float f[7] = {0, 0, 0, 0, 0, 0, 0};
-        float pw[3] = {0, 0, 0};
-        int status = 0;
-        if (i < P) {
-          status = track_pixel(a, n, v, T, V, c, f, pw);
-          a.status[level][i] = status;
-          if (a.q1 && ((i / Wl) & 7) != 7) status = 0;  // only work group 7 reaches the solver
-        }
-        const bool use = status == 1;
+
+      // one pixel's row into this thread's sums (FP32) or its 32-pixel chunk (split-BF16)
+      auto accumulate = [&](bool use, const float* f, const float* pw) {
         if constexpr (JTJ == 0) {
           if (use) {
             pacc[0] += 1.0f;
@@ -305,6 +281,40 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
           fx1 += __float2ll_rn((cA[1] + cA[3] + cB[1]) * kFix);
           fxq += __float2ll_rn(cB[3] * kFix);  // column 7 (feature 1) of row 8 + g: sum q_g
         }
+      };
+
+      // Each warp takes two 32-pixel chunks per step (the chunks of two consecutive grid
+      // passes), so two pixels' gathers are in flight per thread, and the step after that
+      // one's vertices and normals are loaded meanwhile.
+      const int stride = nb * KF_TRACK_THREADS;
+      const float4* Nl = a.normal[level];
+      const float4* Vl = a.vertex[level];
+      const int first = (local * kWarps + warp) * 32;
+      const float4 none = make_float4(2.0f, 0.f, 0.f, 0.f), zero = make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 n0 = none, v0 = zero, n1 = none, v1 = zero;
+      if (first + lane < P) { n0 = __ldg(Nl + first + lane); v0 = __ldg(Vl + first + lane); }
+      if (first + stride + lane < P) { n1 = __ldg(Nl + first + stride + lane); v1 = __ldg(Vl + first + stride + lane); }
+      for (int base = first; base < P; base += 2 * stride) {
+        const int i0 = base + lane, i1 = base + stride + lane;
+        const float4 na = n0, va = v0, nb1 = n1, vb1 = v1;
+        n0 = none; v0 = zero; n1 = none; v1 = zero;
+        if (i0 + 2 * stride < P) { n0 = __ldg(Nl + i0 + 2 * stride); v0 = __ldg(Vl + i0 + 2 * stride); }
+        if (i1 + 2 * stride < P) { n1 = __ldg(Nl + i1 + 2 * stride); v1 = __ldg(Vl + i1 + 2 * stride); }
+        float f0[7] = {0, 0, 0, 0, 0, 0, 0}, f1[7] = {0, 0, 0, 0, 0, 0, 0};
+        float pw0[3] = {0, 0, 0}, pw1[3] = {0, 0, 0};
+        int st0 = 0, st1 = 0;
+        if (i0 < P) st0 = track_pixel(a, na, va, s_T, s_V, c, f0, pw0);
+        if (i1 < P) st1 = track_pixel(a, nb1, vb1, s_T, s_V, c, f1, pw1);
+        if (i0 < P) {
+          a.status[level][i0] = st0;
+          if (a.q1 && ((i0 / Wl) & 7) != 7) st0 = 0;  // only work group 7 reaches the solver
+        }
+        if (i1 < P) {
+          a.status[level][i1] = st1;
+          if (a.q1 && ((i1 / Wl) & 7) != 7) st1 = 0;
+        }
+        accumulate(st0 == 1, f0, pw0);
+        if (base + stride < P) accumulate(st1 == 1, f1, pw1);  // warp-uniform
       }
 
       // ---------------- block sums -> the entry's fixed-point rows ----------------

@@ -62,6 +62,11 @@ static_assert(KF_STATE_RESULT_BYTES == 144, "frame result head: pose, tracked, e
 struct kf_session {
   kf_config cfg{};
   kf_intrinsics intr{};
+  // identity of the session's kernel arguments: uid is unique per created session, layout
+  // changes whenever a buffer is (re)allocated or the configuration is set (batched steps
+  // cache per-member argument tables)
+  uint64_t uid = 0;
+  uint64_t layout = 0;
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
@@ -513,6 +518,7 @@ struct kf_batch {
   int cap = 0;
   std::string last_error;
   std::vector<kf_session*> members;  // membership of the uploaded tables
+  std::vector<std::pair<uint64_t, uint64_t>> member_keys;  // (uid, layout) of each member
   // argument tables: pinned host copy and device copy
   char* h_table = nullptr;
   char* d_table = nullptr;
@@ -535,6 +541,10 @@ struct kf_batch {
   // gathered frame results: [cap][KF_STATE_RESULT_BYTES]
   char* d_heads = nullptr;
   char* h_heads = nullptr;
+  int last_n = 0;
+  // per-step device input pointers (device-resident frames are read in place)
+  const uint16_t** h_inputs = nullptr;  // pinned, cap
+  const uint16_t** d_inputs = nullptr;  // device, cap
   cudaEvent_t ev[6] = {};
   float stage_ms[5] = {0, 0, 0, 0, 0};
   uint64_t steps = 0;
@@ -572,7 +582,7 @@ int kf_batch_prepare_icp(kf_batch* b);
 int kf_batch_prepare_sdf(kf_batch* b);
 int kf_batch_prepare_integrate(kf_batch* b);
 int kf_batch_prepare_raycast(kf_batch* b);
-int kf_batch_launch_pyramid(kf_batch* b, int n);
+int kf_batch_launch_pyramid(kf_batch* b, int n, const uint16_t* const* d_inputs);
 int kf_batch_launch_icp(kf_batch* b);
 int kf_batch_launch_sdf_recover(kf_batch* b);
 int kf_batch_launch_integrate(kf_batch* b);

@@ -23,9 +23,11 @@ struct PyrArgs {
 // One thread per level-1 pixel; a 32x8 block also produces a 16x4 level-2 tile.
 // BATCH: blockIdx.z selects the session's arguments in `many`.
 template <bool BATCH>
-__global__ void __launch_bounds__(256) depth_mip_kernel(PyrArgs one, const PyrArgs* many) {
+__global__ void __launch_bounds__(256) depth_mip_kernel(PyrArgs one, const PyrArgs* many,
+                                                        const uint16_t* const* inputs) {
   __shared__ float s_l1[8][33];
-  const PyrArgs a = BATCH ? many[blockIdx.z] : one;
+  PyrArgs a = BATCH ? many[blockIdx.z] : one;
+  if (BATCH && inputs) a.in_u16 = inputs[blockIdx.z];  // this step's frame, read in place
   const int x1 = blockIdx.x * 32 + threadIdx.x;
   const int y1 = blockIdx.y * 8 + threadIdx.y;
   float m = 0.0f;
@@ -168,7 +170,7 @@ int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32) 
   const PyrArgs a = make_pyr_args(s, d_u16, d_f32);
   dim3 block(32, 8);
   dim3 grid((s->W[1] + 31) / 32, (s->H[1] + 7) / 8);
-  depth_mip_kernel<false><<<grid, block, 0, s->stream>>>(a, nullptr);
+  depth_mip_kernel<false><<<grid, block, 0, s->stream>>>(a, nullptr, nullptr);
   kf_note_launch(s);
   KF_CUDA_TRY(s, cudaGetLastError());
   return KF_OK;
@@ -207,10 +209,10 @@ int kf_batch_prepare_pyramid(kf_batch* b) {
   return KF_OK;
 }
 
-int kf_batch_launch_pyramid(kf_batch* b, int n) {
+int kf_batch_launch_pyramid(kf_batch* b, int n, const uint16_t* const* d_inputs) {
   dim3 block(32, 8);
   dim3 grid((b->W1 + 31) / 32, (b->H1 + 7) / 8, n);
-  depth_mip_kernel<true><<<grid, block, 0, b->stream>>>(PyrArgs{}, static_cast<const PyrArgs*>(b->pyr_args));
+  depth_mip_kernel<true><<<grid, block, 0, b->stream>>>(PyrArgs{}, static_cast<const PyrArgs*>(b->pyr_args), d_inputs);
   KF_CUDA_TRY(b, cudaGetLastError());
   dim3 g2((b->vn_pixels + 255) / 256, n);
   vertex_normal_kernel<true><<<g2, 256, 0, b->stream>>>(VNArgs{}, static_cast<const VNArgs*>(b->vn_args));

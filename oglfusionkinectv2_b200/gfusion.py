@@ -368,6 +368,12 @@ class GFusionBatch:
                     "kf_batch_frame_step_u16_device")
         return np.array(list(t), dtype=bool)
 
+    def poses(self, n: int) -> np.ndarray:
+        """Camera-to-world poses (n x 4 x 4) of the last step's first n sessions."""
+        a = np.empty((n, 16), np.float64)
+        self._check(self.lib.kf_batch_get_poses(self._h, n, a.ctypes.data), "kf_batch_get_poses")
+        return a.reshape(n, 4, 4).transpose(0, 2, 1).copy()
+
     def stageTimes(self) -> np.ndarray:
         """Device ms of the last step: pyramid, track, integrate, recover, raycast."""
         a = (C.c_float * 5)()
@@ -378,6 +384,101 @@ class GFusionBatch:
         n = C.c_uint64()
         self._check(self.lib.kf_batch_get_launch_count(self._h, C.byref(n)), "kf_batch_get_launch_count")
         return int(n.value)
+
+
+class GFusionServer:
+    """The served form (kf_server_*): resident sessions admitted by slots and device memory,
+    frames queued as they arrive, batched steps over the sessions with a waiting frame."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_sessions: int = 128, max_batch: int = 64,
+                 storage: int = L.KF_STORAGE_F16U16, jtj: int = L.KF_JTJ_SPLIT_BF16):
+        self.lib = L.load()
+        c = L.ServerConfig()
+        L.check(self.lib.kf_server_config_default(C.byref(c)), "kf_server_config_default")
+        c.hbm_budget_bytes, c.max_sessions, c.max_batch = int(hbm_budget_bytes), int(max_sessions), int(max_batch)
+        c.storage, c.jtj = int(storage), int(jtj)
+        h = C.c_void_p()
+        L.check(self.lib.kf_server_create(C.byref(c), C.byref(h)), "kf_server_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.kf_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != L.KF_OK:
+            msg = self.lib.kf_server_last_error(self._h)
+            raise L.KfError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def now(self) -> float:
+        return float(self.lib.kf_server_now())
+
+    def open(self, config: "GFusionConfig", intrinsics: "Intrinsics", pose) -> int | None:
+        """Admit a session; None when no slot or memory is free (KF_ERR_ADMISSION)."""
+        cc = config.to_c()
+        ic = intrinsics.to_c()
+        sid = C.c_int()
+        st = self.lib.kf_server_open(self._h, C.byref(cc), C.byref(ic), _pose_to_c(pose), C.byref(sid))
+        if st == L.KF_ERR_ADMISSION:
+            return None
+        self._check(st, "kf_server_open")
+        return sid.value
+
+    def close_session(self, sid: int):
+        self._check(self.lib.kf_server_close(self._h, int(sid)), "kf_server_close")
+
+    def submit(self, sid: int, frame: np.ndarray):
+        f = np.ascontiguousarray(frame, dtype=np.uint16)
+        self._check(self.lib.kf_server_submit(self._h, int(sid), f.ctypes.data), "kf_server_submit")
+
+    def submit_device(self, sid: int, device_ptr: int):
+        self._check(self.lib.kf_server_submit_device(self._h, int(sid), C.c_void_p(int(device_ptr))),
+                    "kf_server_submit_device")
+
+    def step(self) -> int:
+        n = C.c_int()
+        self._check(self.lib.kf_server_step(self._h, C.byref(n)), "kf_server_step")
+        return n.value
+
+    def pose(self, sid: int):
+        """(camera-to-world pose, tracked, frames done) after the session's last stepped frame."""
+        a = (C.c_double * 16)()
+        t = C.c_int()
+        d = C.c_uint64()
+        self._check(self.lib.kf_server_get_pose(self._h, int(sid), a, C.byref(t), C.byref(d)), "kf_server_get_pose")
+        return _pose_from_c(a), bool(t.value), int(d.value)
+
+    def last_step(self, max_n: int = 256):
+        """(ids, poses n x 4 x 4, tracked) of the sessions in the last step."""
+        ids = np.empty(max_n, np.int32)
+        poses = np.empty((max_n, 16), np.float64)
+        tr = np.empty(max_n, np.int32)
+        n = C.c_int()
+        self._check(self.lib.kf_server_last_step(self._h, max_n, ids.ctypes.data, poses.ctypes.data,
+                                                 tr.ctypes.data, C.byref(n)), "kf_server_last_step")
+        k = n.value
+        return ids[:k].copy(), poses[:k].reshape(k, 4, 4).transpose(0, 2, 1).copy(), tr[:k].astype(bool)
+
+    def pending(self, sid: int) -> int:
+        q = C.c_int()
+        self._check(self.lib.kf_server_pending(self._h, int(sid), C.byref(q)), "kf_server_pending")
+        return q.value
+
+    def stats(self) -> dict:
+        s = L.ServerStats()
+        self._check(self.lib.kf_server_stats(self._h, C.byref(s)), "kf_server_stats")
+        return {"frames": s.frames, "steps": s.steps, "busy_s": s.busy_s, "p50_ms": s.p50_ms, "p99_ms": s.p99_ms,
+                "max_ms": s.max_ms, "bytes_in_use": s.bytes_in_use, "active_sessions": s.active_sessions}
+
+    def reset_stats(self):
+        self._check(self.lib.kf_server_reset_stats(self._h), "kf_server_reset_stats")
 
 
 class MCubes:

@@ -143,13 +143,81 @@ class Workload:
         for i in range(start, stop):
             yield self.frame(i)
 
+    def frames_torch(self, indices, device="cuda"):
+        """The same scene, trajectory and corruption model rendered with torch on `device`
+        (FP64 rays, a torch generator seeded per frame): an int16 tensor (n, H, W) holding
+        uint16 millimetres.  The noise draws differ from frame(); used where thousands of
+        frames are needed (batched and served workloads)."""
+        import torch
+        k = self.intrinsics
+        dev = torch.device(device)
+        u = torch.arange(k.width, dtype=torch.float64, device=dev)
+        v = torch.arange(k.height, dtype=torch.float64, device=dev)
+        vv, uu = torch.meshgrid(v, u, indexing="ij")
+        rays = torch.stack([(uu - k.cx) / k.fx, (vv - k.cy) / k.fy, torch.ones_like(uu)], -1).reshape(-1, 3)
+        out = torch.empty((len(indices), k.height, k.width), dtype=torch.int16, device=dev)
+        gen = torch.Generator(device=dev)
+        for j, i in enumerate(indices):
+            T = torch.as_tensor(self.poses[i], dtype=torch.float64, device=dev)
+            dirs = rays @ T[:3, :3].T
+            o = T[:3, 3]
+            t = torch.full((dirs.shape[0],), float("inf"), dtype=torch.float64, device=dev)
+            for n, d in self.scene.planes:
+                nn = torch.as_tensor(n, dtype=torch.float64, device=dev)
+                den = dirs @ nn
+                tt = (d - o @ nn) / den
+                tt = torch.where((den == 0) | ~(tt > 1e-6), torch.full_like(tt, float("inf")), tt)
+                t = torch.minimum(t, tt)
+            a = (dirs * dirs).sum(1)
+            for c, r in self.scene.spheres:
+                oc = o - torch.as_tensor(c, dtype=torch.float64, device=dev)
+                b = 2.0 * (dirs @ oc)
+                cc = oc @ oc - r * r
+                disc = b * b - 4 * a * cc
+                ok = disc >= 0
+                sq = torch.sqrt(torch.clamp(disc, min=0.0))
+                t0 = (-b - sq) / (2 * a)
+                t1 = (-b + sq) / (2 * a)
+                inf = torch.full_like(t0, float("inf"))
+                tt = torch.where(t0 > 1e-6, t0, torch.where(t1 > 1e-6, t1, inf))
+                t = torch.minimum(t, torch.where(ok, tt, inf))
+            for lo, hi in self.scene.boxes:
+                lo_t = torch.as_tensor(lo, dtype=torch.float64, device=dev)
+                hi_t = torch.as_tensor(hi, dtype=torch.float64, device=dev)
+                inv = 1.0 / dirs
+                ta = (lo_t - o) * inv
+                tb = (hi_t - o) * inv
+                tmin = torch.nan_to_num(torch.minimum(ta, tb), nan=-float("inf")).amax(1)
+                tmax = torch.nan_to_num(torch.maximum(ta, tb), nan=float("inf")).amin(1)
+                hit = (tmax >= tmin) & (tmax > 1e-6)
+                tt = torch.where(tmin > 1e-6, tmin, tmax)
+                t = torch.minimum(t, torch.where(hit, tt, torch.full_like(tt, float("inf"))))
+            z = t.reshape(k.height, k.width)
+            gen.manual_seed(splitmix64(self.seed * 1000003 + i) & 0x7FFFFFFFFFFFFFFF)
+            if self.flying_pixels:
+                zf = torch.where(torch.isfinite(z), z, torch.full_like(z, 10.0))
+                right = torch.roll(zf, -1, dims=1)
+                edge = (right - zf).abs() > 0.1
+                mix = torch.rand(z.shape, generator=gen, dtype=torch.float64, device=dev)
+                take = edge & (torch.rand(z.shape, generator=gen, dtype=torch.float64, device=dev) < 0.5)
+                z = torch.where(take, zf * mix + right * (1 - mix), z)
+            sigma = 0.0012 + 0.0019 * (z - 0.4) ** 2
+            noise = torch.randn(z.shape, generator=gen, dtype=torch.float64, device=dev)
+            zn = z + noise * torch.where(torch.isfinite(sigma), sigma, torch.zeros_like(sigma))
+            valid = torch.isfinite(zn) & (zn >= 0.5) & (zn <= 4.5)
+            mm = torch.where(valid, torch.round(zn * 1000.0), torch.zeros_like(zn))
+            drop = torch.rand(z.shape, generator=gen, dtype=torch.float64, device=dev) < self.dropout
+            mm = torch.where(drop, torch.zeros_like(mm), mm)
+            out[j] = mm.to(torch.int32).to(torch.int16)  # uint16 bits (values <= 4500)
+        return out
+
 
 def _orbit_poses(dim: float, n: int, radius: float = 1.2, deg_per_frame: float = 0.5,
-                 drift_per_frame: float = 0.002, height: float = -0.25) -> list:
+                 drift_per_frame: float = 0.002, height: float = -0.25, phase_deg: float = 0.0) -> list:
     c = np.array([dim / 2, dim / 2, dim / 2])
     poses = []
     for k in range(n):
-        th = np.deg2rad(deg_per_frame * k)
+        th = np.deg2rad(phase_deg + deg_per_frame * k)
         # orbit about the world y axis through the cube centre; drift moves the camera up
         # (towards -y) along that axis
         pos = c + np.array([radius * np.sin(th), height - drift_per_frame * k, -radius * np.cos(th)])
@@ -271,3 +339,61 @@ def ate(poses_a, poses_b) -> float:
     """RMS translation difference (m) between two trajectories."""
     d = [np.linalg.norm(np.asarray(a)[:3, 3] - np.asarray(b)[:3, 3]) for a, b in zip(poses_a, poses_b)]
     return float(np.sqrt(np.mean(np.square(d)))) if d else 0.0
+
+
+C3_SIZES = (128, 192, 256, 384)
+
+
+def session_scene(n_frames: int, seed: int, size: int, phase_deg: float = 0.0, deg_per_frame: float = 0.5) -> Workload:
+    """One session of the batched and served forms: a seeded scene in a 1.5 m cube (ground
+    plane, 6 spheres and 2 boxes near the orbit axis -- C1's three spheres alone leave some
+    seeds' tracking ill-conditioned, in the FP64 oracle as on the GPU), an orbit with a
+    seeded start angle and direction, FP16 TSDF + uint16 weight, split-BF16 J^T J."""
+    w = plain_c1(n_frames, seed=seed)
+    rng = np.random.Generator(np.random.PCG64(splitmix64(seed ^ 0x5EED)))
+    ground = 1.5 / 2 + 0.6
+    spheres, boxes = _objects(rng, 1.5, 6, 2, ground, max_axis_dist=0.7)
+    w.scene = Scene(planes=[((0.0, 1.0, 0.0), ground)], spheres=spheres, boxes=boxes)
+    w.poses = _orbit_poses(1.5, n_frames, deg_per_frame=deg_per_frame, phase_deg=phase_deg)
+    w.config.volumeSize = (size, size, size)
+    w.config.storage = L.KF_STORAGE_F16U16
+    w.config.jtj = L.KF_JTJ_SPLIT_BF16
+    return w
+
+
+def batched_c3(n_sessions: int = 64, n_frames: int = 300, seed: int = 0xC0FFEE + 3) -> list:
+    """Batched form: independent sessions (session_scene), volume size drawn uniformly from
+    {128, 192, 256, 384}^3."""
+    out = []
+    rng = np.random.Generator(np.random.PCG64(splitmix64(seed)))
+    for k in range(n_sessions):
+        sk = splitmix64(seed + k) & 0xFFFFFFFF
+        size = int(rng.choice(C3_SIZES))
+        phase = float(rng.uniform(0.0, 360.0))
+        step = 0.5 if rng.random() < 0.5 else -0.5
+        w = session_scene(n_frames, sk, size, phase, step)
+        w.name = f"c3_session{k}_{size}"
+        out.append(w)
+    return out
+
+
+@dataclass
+class Arrival:
+    t: float        # arrival time (s)
+    frames: int     # session length
+    size: int       # volume side
+    scene: int      # index of the pre-rendered sequence it streams
+
+
+def served_c4(duration_s: float, rate_per_s: float = 20.0, seed: int = 0xC0FFEE + 4,
+              n_scenes: int = 16, sizes=tuple(range(128, 513, 32))) -> list:
+    """Serving form: Poisson arrivals (rate_per_s), session length U(50, 2000) frames,
+    volume side drawn from 128..512 (multiples of 32), each session streaming one of
+    n_scenes seeded sequences at 30 Hz.  Arrivals up to duration_s."""
+    rng = np.random.Generator(np.random.PCG64(splitmix64(seed)))
+    t, out = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / rate_per_s))
+        if t > duration_s:
+            return out
+        out.append(Arrival(t, int(rng.integers(50, 2001)), int(rng.choice(sizes)), int(rng.integers(0, n_scenes))))

@@ -71,3 +71,47 @@ def test_create_without_device_fails_loudly():
     from oglfusionkinectv2_b200 import GFusion
     with pytest.raises(L.KfError):
         GFusion()
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """ctypes mirrors of the ABI structs have the C compiler's sizes and offsets."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    structs = {"kf_config": L.kf_config, "kf_intrinsics": L.kf_intrinsics, "kf_volume_view": L.kf_volume_view,
+               "kf_server_config": L.ServerConfig, "kf_server_stats_t": L.ServerStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "kf.h"', "int main(void) {"]
+    for name, py in structs.items():
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines())
+    for name, py in structs.items():
+        assert int(got[name]) == C.sizeof(py), name
+        for f, _ in py._fields_:
+            assert int(got[f"{name}.{f}"]) == getattr(py, f).offset, f"{name}.{f}"
+
+
+def test_batch_and_server_without_device_fail_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    lib = L.load()
+    h = C.c_void_p()
+    assert lib.kf_batch_create(4, C.byref(h)) == L.KF_ERR_NO_DEVICE
+    assert lib.kf_batch_create(0, C.byref(h)) == L.KF_ERR_INVALID_ARGUMENT
+    assert lib.kf_batch_create(L.KF_BATCH_MAX_SESSIONS + 1, C.byref(h)) == L.KF_ERR_INVALID_ARGUMENT
+    cfg = L.ServerConfig()
+    assert lib.kf_server_config_default(C.byref(cfg)) == L.KF_OK
+    assert (cfg.max_sessions, cfg.max_batch, cfg.storage, cfg.jtj) == (128, 64, L.KF_STORAGE_F16U16,
+                                                                      L.KF_JTJ_SPLIT_BF16)
+    assert lib.kf_server_create(C.byref(cfg), C.byref(h)) != L.KF_OK
+    t0 = lib.kf_server_now()
+    assert lib.kf_server_now() >= t0

@@ -127,3 +127,27 @@ def test_batch_rejects_bad_membership():
     assert e.value.status == L.KF_ERR_CAPACITY
     # a valid step still works after the refusals
     assert batch.frameStep(gs, [f, f]).shape == (2,)
+
+
+def test_batch_tables_follow_replaced_sessions():
+    """A destroyed session's address may come back for the next session created, and a
+    session may reallocate its buffers (Reset with delete): the batch must rebuild its
+    per-member tables rather than reuse stale ones."""
+    ws = workloads(3)
+    fr = [[w.frame(k) for k in range(3)] for w in ws]
+    batch = GFusionBatch(2)
+    a, b = fresh(ws[:2])
+    batch.frameStep([a, b], [fr[0][0], fr[1][0]])
+    a.close()
+    del a
+    c = fresh(ws[2:3])[0]  # a different volume size, possibly at a's old address
+    batch.frameStep([c, b], [fr[2][0], fr[1][1]])
+    b.Reset(ws[1].poses[0], True)  # reallocates b's volume
+    batch.frameStep([c, b], [fr[2][1], fr[1][0]])
+    ref_c = fresh(ws[2:3])[0]
+    ref_c.frameStep(fr[2][0])
+    ref_c.frameStep(fr[2][1])
+    ref_b = fresh(ws[1:2])[0]
+    ref_b.frameStep(fr[1][0])
+    assert_same(snapshot(c), snapshot(ref_c))
+    assert_same(snapshot(b), snapshot(ref_b))
