@@ -49,6 +49,7 @@ def parse():
                    help="plain: the single-session frame step (default line); batched: config 3; served: config 4")
     p.add_argument("--sessions", type=int, default=64, help="batched form: sessions per batch")
     p.add_argument("--duration", type=float, default=30.0, help="served form: seconds of arrivals")
+    p.add_argument("--slots", type=int, default=128, help="served form: resident session slots")
     return p.parse_args()
 
 
@@ -373,10 +374,17 @@ def run_served(args):
     torch.cuda.synchronize()
     gt = [(w.poses, w.config, w.intrinsics) for w in scenes]
     fbytes = 512 * 424 * 2
-    slots = 64
+    slots, batch_max = args.slots, min(args.slots, 128)
+    sizes = sorted({a.size for a in arrivals})
     results = {}
-    for name, max_batch in (("served", 64), ("plain_one_at_a_time", 1)):
+    for name, max_batch in (("served", batch_max), ("plain_one_at_a_time", 1)):
         server = GFusionServer(max_sessions=slots, max_batch=max_batch)
+        # a warm pool: sessions of every volume size created before the arrivals start
+        cfg = gt[0][1]
+        per = -(-slots // len(sizes)) + 1
+        for z in sizes:
+            cfg.volumeSize = (z, z, z)
+            server.prewarm(cfg, gt[0][2], per)
         with ClockSampler(0) as clk:
             frames, admitted, max_wait, errs = serve_pass(server, arrivals, seqs, gt, args.duration, fbytes, slots)
         st = server.stats()
@@ -396,7 +404,8 @@ def run_served(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "c4_served", "duration_s": args.duration, "arrivals": len(arrivals),
-                       "slots": slots, "max_batch": 64, "storage": "f16u16", "jtj": "bf16",
+                       "slots": slots, "max_batch": batch_max, "storage": "f16u16", "jtj": "bf16",
+                       "warm_pool": "sessions of every volume size created before the arrivals",
                        "scenes": f"{n_scenes} seeded sequences of {L_seq} frames, replayed back and forth"},
             "latency_ms": {"p50": sv["p50_ms"], "p99": sv["p99_ms"], "max": sv["max_ms"]},
             "served": sv, "plain_one_at_a_time": pl,

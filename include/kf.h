@@ -288,6 +288,11 @@ KF_API double kf_server_now(void); /* the server's clock (seconds, monotonic) */
 /* cfg's storage, jtj and tracking are replaced by the server's form. */
 KF_API int kf_server_open(kf_server* v, const kf_config* cfg, const kf_intrinsics* intr,
                           const double pose[16], int* session_id);
+/* Create `count` sessions of this configuration ahead of admissions (kept, like closed
+ * sessions, for the next admissions of the same volume size); *created receives how many
+ * fit the budget. */
+KF_API int kf_server_prewarm(kf_server* v, const kf_config* cfg, const kf_intrinsics* intr,
+                             int count, int* created);
 /* The session's slot is freed at once; its device memory is kept for the next admission of
  * the same volume size, and released when the budget needs it (or at kf_server_destroy). */
 KF_API int kf_server_close(kf_server* v, int session_id);

@@ -153,6 +153,7 @@ SIGNATURES = {
     "kf_server_now": (C.c_double, []),
     "kf_server_open": (_I, [_P, _P, _P, _P, C.POINTER(_I)]),
     "kf_server_close": (_I, [_P, _I]),
+    "kf_server_prewarm": (_I, [_P, _P, _P, _I, C.POINTER(_I)]),
     "kf_server_submit": (_I, [_P, _I, _P]),
     "kf_server_submit_device": (_I, [_P, _I, _P]),
     "kf_server_step": (_I, [_P, C.POINTER(_I)]),

@@ -224,6 +224,37 @@ int kf_server_open(kf_server* v, const kf_config* cfg, const kf_intrinsics* intr
   return KF_OK;
 }
 
+int kf_server_prewarm(kf_server* v, const kf_config* cfg, const kf_intrinsics* intr, int count, int* created) {
+  if (!v || !cfg || !intr || count < 0) return KF_ERR_INVALID_ARGUMENT;
+  if (created) *created = 0;
+  kf_config c = *cfg;
+  c.storage = v->cfg.storage;
+  c.jtj = v->cfg.jtj;
+  c.tracking = KF_TRACK_ICP;
+  uint64_t need = 0;
+  int rc = kf_session_device_bytes(&c, intr, &need);
+  if (rc) return sfail(v, rc, "invalid session configuration");
+  need += (uint64_t)kRing * intr->width * intr->height * 2;
+  const double identity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  for (int k = 0; k < count; ++k) {
+    if (v->bytes_in_use + need > v->cfg.hbm_budget_bytes) return sfail(v, KF_ERR_ADMISSION, "device memory budget full");
+    Slot sl;
+    if ((rc = kf_create(&c, intr, &sl.s))) return sfail(v, rc, "session creation failed");
+    if (cudaMalloc((void**)&sl.d_ring, (size_t)kRing * intr->width * intr->height * 2) != cudaSuccess ||
+        (rc = kf_reset(sl.s, identity, 0))) {
+      cudaGetLastError();
+      kf_destroy(sl.s);
+      cudaFree(sl.d_ring);
+      return sfail(v, rc ? rc : KF_ERR_OUT_OF_MEMORY, "session creation failed");
+    }
+    sl.bytes = need;
+    v->bytes_in_use += need;
+    v->idle.push_back(sl);
+    if (created) *created += 1;
+  }
+  return KF_OK;
+}
+
 int kf_server_close(kf_server* v, int id) {
   Slot* sl = slot_of(v, id);
   if (!sl) return KF_ERR_INVALID_ARGUMENT;

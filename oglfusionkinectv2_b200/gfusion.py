@@ -431,6 +431,14 @@ class GFusionServer:
         self._check(st, "kf_server_open")
         return sid.value
 
+    def prewarm(self, config: "GFusionConfig", intrinsics: "Intrinsics", count: int) -> int:
+        """Create `count` idle sessions of this configuration ahead of admissions."""
+        cc, ic, n = config.to_c(), intrinsics.to_c(), C.c_int()
+        st = self.lib.kf_server_prewarm(self._h, C.byref(cc), C.byref(ic), int(count), C.byref(n))
+        if st not in (L.KF_OK, L.KF_ERR_ADMISSION):
+            self._check(st, "kf_server_prewarm")
+        return n.value
+
     def close_session(self, sid: int):
         self._check(self.lib.kf_server_close(self._h, int(sid)), "kf_server_close")
 

@@ -101,3 +101,21 @@ def test_server_reuses_closed_sessions():
         v.submit(b, f2[k])
     drain(v, [b])
     np.testing.assert_array_equal(v.pose(b)[0], alone_poses(w2, f2)[-1])
+
+
+def test_server_prewarm_and_eviction():
+    """Prewarmed sessions count against the budget, serve admissions of their size, and are
+    released when another size needs the room."""
+    ws = workloads(2)
+    v = GFusionServer(hbm_budget_bytes=100 << 20, max_sessions=4, max_batch=4)
+    assert v.prewarm(ws[0].config, ws[0].intrinsics, 5) == 2  # about 38 MiB each
+    a = v.open(ws[0].config, ws[0].intrinsics, ws[0].poses[0])  # takes a warm one
+    assert a is not None
+    b = v.open(ws[1].config, ws[1].intrinsics, ws[1].poses[0])  # evicts the other warm one
+    assert b is not None
+    f = [ws[0].frame(0), ws[1].frame(0)]
+    v.submit(a, f[0])
+    v.submit(b, f[1])
+    assert v.step() == 2
+    np.testing.assert_array_equal(v.pose(a)[0], alone_poses(ws[0], f[:1])[-1])
+    np.testing.assert_array_equal(v.pose(b)[0], alone_poses(ws[1], f[1:])[-1])
