@@ -127,6 +127,9 @@ int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth,
   KF_CUDA_TRY(b, cudaEventRecord(b->ev[4], b->stream));
   if ((rc = kf_batch_launch_raycast(b, n))) return rc;
   KF_CUDA_TRY(b, cudaEventRecord(b->ev[5], b->stream));
+  // every KF_BRICK_REBUILD_EVERY integrates a member's skip flags are rebuilt exactly
+  for (int e = 0; e < n; ++e)
+    if ((rc = kf_note_integrate(ss[e], b->stream))) return bfail(b, rc, "brick flag rebuild: " + ss[e]->last_error);
   batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
   KF_CUDA_TRY(b, cudaGetLastError());
   b->launches += 2;

@@ -171,15 +171,19 @@ int alloc_volume(kf_session* s) {
   cudaFree(s->d_vol);
   s->d_vol = nullptr;
   cudaFree(s->d_bricks);
-  s->d_bricks = nullptr;
+  s->d_bricks = s->d_supers = nullptr;
   s->bx = (s->cfg.nx + KF_BRICK - 1) / KF_BRICK;
   s->by = (s->cfg.ny + KF_BRICK - 1) / KF_BRICK;
   s->bz = (s->cfg.nz + KF_BRICK - 1) / KF_BRICK;
+  s->sbx = (s->cfg.nx + KF_SUPER - 1) / KF_SUPER;
+  s->sby = (s->cfg.ny + KF_SUPER - 1) / KF_SUPER;
+  s->sbz = (s->cfg.nz + KF_SUPER - 1) / KF_SUPER;
   {
-    const size_t nb = (size_t)s->bx * s->by * s->bz;
-    int rc = dalloc(s, &s->d_bricks, nb);
+    const size_t nb = (size_t)s->bx * s->by * s->bz, ns = (size_t)s->sbx * s->sby * s->sbz;
+    int rc = dalloc(s, &s->d_bricks, nb + ns);
     if (rc) return rc;
-    KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, nb * 4, s->stream));
+    s->d_supers = s->d_bricks + nb;
+    if ((rc = kf_reset_bricks(s))) return rc;
   }
   s->vol_count = (size_t)s->cfg.nx * s->cfg.ny * s->cfg.nz;
   s->vol_value_bytes = value_bytes(s->cfg.storage);
@@ -288,6 +292,7 @@ int run_frame(kf_session* s) {
   int rc = harvest(s, slot);  // the frame that used this slot kRing frames ago
   if (rc) return rc;
   KF_CUDA_TRY(s, cudaGraphLaunch(s->frame_exec[slot], s->stream));
+  if ((rc = kf_note_integrate(s, s->stream))) return rc;
   s->ring_pending[slot] = 1;
   s->frames_run += 1;
   s->launches += (uint64_t)s->frame_kernels;
@@ -396,7 +401,9 @@ int kf_session_device_bytes(const kf_config* cfg, const kf_intrinsics* in, uint6
   const uint64_t px = (uint64_t)in->width * in->height;
   uint64_t b = vox * value_bytes(cfg->storage) * 2;
   b += (uint64_t)((cfg->nx + KF_BRICK - 1) / KF_BRICK) * ((cfg->ny + KF_BRICK - 1) / KF_BRICK) *
-       ((cfg->nz + KF_BRICK - 1) / KF_BRICK) * 4;  // brick flags
+       ((cfg->nz + KF_BRICK - 1) / KF_BRICK) * 4 +
+       (uint64_t)((cfg->nx + KF_SUPER - 1) / KF_SUPER) * ((cfg->ny + KF_SUPER - 1) / KF_SUPER) *
+       ((cfg->nz + KF_SUPER - 1) / KF_SUPER) * 4;  // brick and super-brick flags
   b += px * (2 + 4);                       // staging
   b += px * (4 + 16 + 16 + 4) * 2;         // three levels (sum < 4/3 of level 0)
   b += px * 32;                            // raycast maps
@@ -496,7 +503,7 @@ int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
     if ((rc = alloc_volume(s))) return rc;
   } else {
     KF_CUDA_TRY(s, cudaMemsetAsync(s->d_vol, 0, s->vol_bytes, s->stream));
-    KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, (size_t)s->bx * s->by * s->bz * 4, s->stream));
+    if ((rc = kf_reset_bricks(s))) return rc;
   }
   if ((rc = pull_state(s))) return rc;
   s->h_state->lib_size = 0;  // poseLibrary.resize(0)
@@ -519,7 +526,7 @@ int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
 int kf_reset_volume(kf_session* s) {
   if (!s) return KF_ERR_INVALID_ARGUMENT;
   KF_CUDA_TRY(s, cudaMemsetAsync(s->d_vol, 0, s->vol_bytes, s->stream));
-  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, (size_t)s->bx * s->by * s->bz * 4, s->stream));
+  if (int rc = kf_reset_bricks(s)) return rc;
   return KF_OK;
 }
 
@@ -654,6 +661,7 @@ int kf_integrate(kf_session* s) {
   int rc = record(s, 8);
   if (!rc) rc = kf_launch_integrate(s, 0);
   if (!rc) rc = record(s, 9);
+  if (!rc) rc = kf_note_integrate(s, s->stream);
   return rc;
 }
 
@@ -738,7 +746,7 @@ int kf_copy_volume_to_host(kf_session* s, void* dst, uint64_t bytes) {
 int kf_copy_volume_from_host(kf_session* s, const void* src, uint64_t bytes) {
   if (!s || !src || bytes != s->vol_bytes) return KF_ERR_INVALID_ARGUMENT;
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_vol, src, bytes, cudaMemcpyHostToDevice, s->stream));
-  int rc = kf_rebuild_bricks(s);
+  int rc = kf_rebuild_bricks(s, s->stream);
   if (rc) return rc;
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return KF_OK;

@@ -36,6 +36,8 @@ struct IntArgs {
   const KfDevState* st;
   uint32_t* bricks;
   int bx, by, bz;
+  uint32_t* supers;
+  int sbx, sby, sbz;
 };
 
 template <class T>
@@ -78,7 +80,9 @@ template <int S>
 __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const float* inv, int x, int y, int zb) {
   typedef typename Vox<S>::V V;
   typedef typename Vox<S>::Wt Wt;
-  uint32_t zneg = 0;
+  // bits 0-2: NEG of z-bricks zb/8 - 1 + j; bit 6: NEG of z-super-brick zb/64, bit 7: of
+  // zb/64 - 1 (a z % 64 == 0 voxel is that one's +1 layer)
+  uint32_t flags = 0;
 
   // getVolumePosition (integrate.cs:16-19) at z = zb, and delta = rotate(invTrack, (0,0,vz))
   const float cxw = (x + 0.5f) * a.dimx / a.nx;
@@ -136,17 +140,20 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
       const Wt ew = Vox<S>::encode_weight(nw);
       if (bits_of(ev) != bits_of(oldv)) vf[idx] = ev;
       if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
-      if (Vox<S>::raw_nc(&ev, 0) < 0.0f) {
+      // a non-negative nF never stores a negative value
+      if (nF < 0.0f) {
         const int z = zb + k;
-        zneg |= 1u << ((z >> 3) - (zb >> 3) + 1);
-        if ((z & 7) == 0) zneg |= 1u << ((z >> 3) - (zb >> 3));
+        const int j = (z >> 3) - (zb >> 3) + 1;
+        flags |= 1u << j;
+        if ((z & 7) == 0) flags |= 1u << (j - 1);
+        flags |= (z & 63) == 0 ? 0xc0u : 0x40u;
       }
     } else {
       vf[idx] = Vox<S>::encode_value(0.0f);
       vw[idx] = Vox<S>::encode_weight(0.0f);
     }
   }
-  return zneg;
+  return flags;
 }
 
 // A batched launch: flat block b belongs to the entry e with prefix[e] <= b < prefix[e + 1].
@@ -183,9 +190,11 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
   }
   const IntArgs& a = BATCH ? s_args : a_one;
   __shared__ int s_cull;
-  // negative-value flags of the bricks this block may touch, dilated by one voxel towards
-  // -x/-y/-z: [z: bz0-1 .. bz0+1][y: by0-1 .. by0][x: bx0-1 .. bx0+3]
+  // flags of the bricks this block may touch, its own and, for voxels on a brick's low face,
+  // the brick below whose +1 layer they are: [z: bz0-1 .. bz0+1][y: by0-1 .. by0][x: bx0-1 ..
+  // bx0+3]; and of the super-bricks: [z][y][x] = own - 1 .. own
   __shared__ uint32_t s_neg[3][2][5];
+  __shared__ uint32_t s_sup[2][2][2];
   if (a.gate && *(volatile const int*)a.gate == 0) return;
   float inv[12];  // inverse(m_pose), rows of [R^T | -R^T t] (integrate uses glm::inverse, :1242)
 #pragma unroll
@@ -201,35 +210,61 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
   {
     const int t = threadIdx.y * 32 + threadIdx.x;
     if (t < 30) (&s_neg[0][0][0])[t] = 0u;
+    else if (t < 38) (&s_sup[0][0][0])[t - 30] = 0u;
   }
   __syncthreads();
   if (s_cull) return;
   const int x = xb + threadIdx.x;
   const int y = yb + threadIdx.y;
-  uint32_t zneg = 0;  // bit j: a negative value was written in z-brick (zb/8 - 1 + j)
-  if (x < a.nx && y < a.ny) zneg = integrate_column<S>(a, inv, x, y, zb);
-  if (zneg) {
+  uint32_t flags = 0;  // integrate_column's bits
+  if (x < a.nx && y < a.ny) flags = integrate_column<S>(a, inv, x, y, zb);
+  if (flags & 0x7u) {
     // this voxel column's own brick and, at brick-low faces, the brick below (dilation)
     const int lx = (x >> 3) - (xb >> 3) + 1, ly = 1;
     for (int j = 0; j < 3; ++j) {
-      if (!(zneg & (1u << j))) continue;
-      atomicOr(&s_neg[j][ly][lx], 1u);
-      if ((x & 7) == 0) atomicOr(&s_neg[j][ly][lx - 1], 1u);
+      const uint32_t f = (flags >> j) & 1u ? KF_BRICK_NEG : 0u;
+      if (!f) continue;
+      atomicOr(&s_neg[j][ly][lx], f);
+      if ((x & 7) == 0) atomicOr(&s_neg[j][ly][lx - 1], f);
       if ((y & 7) == 0) {
-        atomicOr(&s_neg[j][ly - 1][lx], 1u);
-        if ((x & 7) == 0) atomicOr(&s_neg[j][ly - 1][lx - 1], 1u);
+        atomicOr(&s_neg[j][ly - 1][lx], f);
+        if ((x & 7) == 0) atomicOr(&s_neg[j][ly - 1][lx - 1], f);
+      }
+    }
+  }
+  if (flags & 0xc0u) {
+    // super-bricks: own (index 1) and, at super-brick-low faces, the one below (index 0)
+    for (int jz = 0; jz < 2; ++jz) {
+      if (!(flags & (jz ? 0x40u : 0x80u))) continue;
+      atomicOr(&s_sup[jz][1][1], KF_BRICK_NEG);
+      if ((x & 63) == 0) atomicOr(&s_sup[jz][1][0], KF_BRICK_NEG);
+      if ((y & 63) == 0) {
+        atomicOr(&s_sup[jz][0][1], KF_BRICK_NEG);
+        if ((x & 63) == 0) atomicOr(&s_sup[jz][0][0], KF_BRICK_NEG);
       }
     }
   }
   __syncthreads();
   {
+    // set the collected bits in global memory; most bricks near and behind surfaces have
+    // them already, so read first and skip those atomics
     const int t = threadIdx.y * 32 + threadIdx.x;
     if (t < 30) {
       const int j = t / 10, r = (t / 5) % 2, c = t % 5;
       const int gx = (xb >> 3) - 1 + c, gy = (yb >> 3) - 1 + r, gz = (zb >> 3) - 1 + j;
-      if (s_neg[j][r][c] && gx >= 0 && gy >= 0 && gz >= 0 && gx < a.bx && gy < a.by && gz < a.bz)
-        atomicOr(&a.bricks[(uint32_t)gx + (uint32_t)a.bx * ((uint32_t)gy + (uint32_t)a.by * (uint32_t)gz)],
-                 KF_BRICK_NEG);
+      const uint32_t f = s_neg[j][r][c];
+      if (f && gx >= 0 && gy >= 0 && gz >= 0 && gx < a.bx && gy < a.by && gz < a.bz) {
+        uint32_t* w = &a.bricks[(uint32_t)gx + (uint32_t)a.bx * ((uint32_t)gy + (uint32_t)a.by * (uint32_t)gz)];
+        if ((*(volatile uint32_t*)w & f) != f) atomicOr(w, f);
+      }
+    } else if (t < 38) {
+      const int q = t - 30, jz = q >> 2, jy = (q >> 1) & 1, jx = q & 1;
+      const int gx = (xb >> 6) - 1 + jx, gy = (yb >> 6) - 1 + jy, gz = (zb >> 6) - 1 + jz;
+      const uint32_t f = s_sup[jz][jy][jx];
+      if (f && gx >= 0 && gy >= 0 && gz >= 0 && gx < a.sbx && gy < a.sby && gz < a.sbz) {
+        uint32_t* w = &a.supers[(uint32_t)gx + (uint32_t)a.sbx * ((uint32_t)gy + (uint32_t)a.sby * (uint32_t)gz)];
+        if ((*(volatile uint32_t*)w & f) != f) atomicOr(w, f);
+      }
     }
   }
 }
@@ -255,6 +290,8 @@ IntArgs make_int_args(kf_session* s, int gated) {
   a.st = s->d_state;
   a.bricks = s->d_bricks;
   a.bx = s->bx; a.by = s->by; a.bz = s->bz;
+  a.supers = s->d_supers;
+  a.sbx = s->sbx; a.sby = s->sby; a.sbz = s->sbz;
   return a;
 }
 

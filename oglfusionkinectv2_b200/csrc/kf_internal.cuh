@@ -76,6 +76,11 @@ struct kf_session {
   // hold a negative TSDF value; set by integrate, cleared by reset, rebuilt on upload
   uint32_t* d_bricks = nullptr;
   int bx = 0, by = 0, bz = 0;
+  // per 64^3 super-brick (8^3 bricks; same allocation as d_bricks, after it): KF_BRICK_NEG
+  // when some brick in it is NEG
+  uint32_t* d_supers = nullptr;
+  int sbx = 0, sby = 0, sbz = 0;
+  int frames_since_rebuild = 0;  // integrates since the flags were last rebuilt exactly
 
   // volume: value plane then weight plane
   void* d_vol = nullptr;
@@ -611,9 +616,18 @@ int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy);
 int kf_launch_sdf_policy(kf_session* s);
 int kf_launch_integrate(kf_session* s, int gated);
 int kf_launch_raycast(kf_session* s);
-int kf_rebuild_bricks(kf_session* s);
+int kf_rebuild_bricks(kf_session* s, cudaStream_t stream);
+int kf_reset_bricks(kf_session* s);
+int kf_note_integrate(kf_session* s, cudaStream_t stream);
 #define KF_BRICK 8
+#define KF_SUPER 64
+// Brick flags.  A brick B covers the voxels [8B, 8B+8] on each axis (the taps of every
+// trilinear sample whose base voxel lies in B); a super-brick S covers [64S, 64S+64].
+// NEG: some value there may be negative.  Integrate only ever sets it; an exact rebuild
+// (every KF_BRICK_REBUILD_EVERY integrates, and after a volume upload) clears stale bits,
+// so a clear bit is a guarantee.
 #define KF_BRICK_NEG 1u
+#define KF_BRICK_REBUILD_EVERY 16
 int kf_mc_run(kf_session* s, float iso, int method, uint32_t* n_tri);
 int kf_scan_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* d_total,
                 cudaStream_t stream, uint32_t* d_scratch, size_t scratch_words);

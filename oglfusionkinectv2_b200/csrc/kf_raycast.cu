@@ -37,6 +37,8 @@ struct RayArgs {
   KfDevState* st_out;
   const uint32_t* bricks;
   int bx, by, bz;
+  const uint32_t* supers;
+  int sbx, sby, sbz;
 };
 
 // 32 x 4 pixel tiles: ray lengths vary a lot, and small blocks keep the SMs evenly loaded
@@ -145,36 +147,56 @@ __global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs one, const
       bool prev_known = true;  // f_t holds the sample just before t
       // bounded march: a NaN sample keeps largeStep, so cap the step count
       for (int n = 0; t < tfar && n < a.max_steps; ++n) {
-        if (fine) {
-          // empty-space skipping: a sample whose brick holds no negative value cannot be
-          // the first negative one; jump to the first sample past the brick.  The sample
-          // positions stay tb + k * step, as in the unskipped march.
+        {
+          // empty-space skipping in the fine phase.  A sample's eight taps lie in the brick
+          // (and super-brick) of its base voxel; a region without a negative value cannot
+          // hold the first negative sample.  Such samples change nothing but f_t, so jump to
+          // the first sample past the region; the positions stay tb + k * stepsize, as in
+          // the unskipped march.
           const float qx = fmaf(t, dqx, q0x), qy = fmaf(t, dqy, q0y), qz = fmaf(t, dqz, q0z);
-          const int ix = min(max((int)floorf(qx), 0), a.nx - 1) >> 3;
-          const int iy = min(max((int)floorf(qy), 0), a.ny - 1) >> 3;
-          const int iz = min(max((int)floorf(qz), 0), a.nz - 1) >> 3;
-          if (!(__ldg(a.bricks + (uint32_t)ix + (uint32_t)a.bx * ((uint32_t)iy + (uint32_t)a.by * (uint32_t)iz)) &
-                KF_BRICK_NEG)) {
-            // the brick spans [8i, 8i + 8) in voxel coordinates; the border bricks extend
-            // outwards (taps are clamped there)
+          const int vx = min(max((int)floorf(qx), 0), a.nx - 1);
+          const int vy = min(max((int)floorf(qy), 0), a.ny - 1);
+          const int vz = min(max((int)floorf(qz), 0), a.nz - 1);
+          int cell = 0;  // 0: sample it; else the side of the region to skip (64 or 8)
+          int cx = 0, cy = 0, cz = 0, ncx = 1, ncy = 1, ncz = 1;
+          if (fine) {
+            if (!(__ldg(a.supers + (uint32_t)(vx >> 6) +
+                        (uint32_t)a.sbx * ((uint32_t)(vy >> 6) + (uint32_t)a.sby * (uint32_t)(vz >> 6))) &
+                  KF_BRICK_NEG)) {
+              cell = 64;
+              cx = vx >> 6; cy = vy >> 6; cz = vz >> 6;
+              ncx = a.sbx; ncy = a.sby; ncz = a.sbz;
+            } else if (!(__ldg(a.bricks + (uint32_t)(vx >> 3) +
+                               (uint32_t)a.bx * ((uint32_t)(vy >> 3) + (uint32_t)a.by * (uint32_t)(vz >> 3))) &
+                         KF_BRICK_NEG)) {
+              cell = 8;
+              cx = vx >> 3; cy = vy >> 3; cz = vz >> 3;
+              ncx = a.bx; ncy = a.by; ncz = a.bz;
+            }
+          }
+          if (cell) {
+            // the region spans [cell*i, cell*(i+1)) in voxel coordinates; the border ones
+            // extend outwards (taps are clamped there)
+            const float c = (float)cell;
             float te = tfar;
-            if (dqx > 0.0f && ix < a.bx - 1) te = fminf(te, (float)(8 * ix + 8) * rdx - q0x * rdx);
-            if (dqx < 0.0f && ix > 0) te = fminf(te, (float)(8 * ix) * rdx - q0x * rdx);
-            if (dqy > 0.0f && iy < a.by - 1) te = fminf(te, (float)(8 * iy + 8) * rdy - q0y * rdy);
-            if (dqy < 0.0f && iy > 0) te = fminf(te, (float)(8 * iy) * rdy - q0y * rdy);
-            if (dqz > 0.0f && iz < a.bz - 1) te = fminf(te, (float)(8 * iz + 8) * rdz - q0z * rdz);
-            if (dqz < 0.0f && iz > 0) te = fminf(te, (float)(8 * iz) * rdz - q0z * rdz);
+            if (dqx > 0.0f && cx < ncx - 1) te = fminf(te, (float)(cx + 1) * c * rdx - q0x * rdx);
+            if (dqx < 0.0f && cx > 0) te = fminf(te, (float)cx * c * rdx - q0x * rdx);
+            if (dqy > 0.0f && cy < ncy - 1) te = fminf(te, (float)(cy + 1) * c * rdy - q0y * rdy);
+            if (dqy < 0.0f && cy > 0) te = fminf(te, (float)cy * c * rdy - q0y * rdy);
+            if (dqz > 0.0f && cz < ncz - 1) te = fminf(te, (float)(cz + 1) * c * rdz - q0z * rdz);
+            if (dqz < 0.0f && cz > 0) te = fminf(te, (float)cz * c * rdz - q0z * rdz);
             const float kf = ceilf((te - tb) / stepsize);
             int kn = kf < 2.0e9f ? (int)kf : k + 1;
             if (kn > k + 1) {
               // te carries rounding; the rounded sample positions are monotone in k on
-              // every axis, so if the last skipped sample is still in this brick, all of
+              // every axis, so if the last skipped sample is still in this region, all of
               // them are.  Otherwise advance by one sample.
               const float tl = fmaf((float)(kn - 1), stepsize, tb);
-              const int jx = min(max((int)floorf(fmaf(tl, dqx, q0x)), 0), a.nx - 1) >> 3;
-              const int jy = min(max((int)floorf(fmaf(tl, dqy, q0y)), 0), a.ny - 1) >> 3;
-              const int jz = min(max((int)floorf(fmaf(tl, dqz, q0z)), 0), a.nz - 1) >> 3;
-              if (jx != ix || jy != iy || jz != iz) kn = k + 1;
+              const int sh = cell == 64 ? 6 : 3;
+              const int jx = min(max((int)floorf(fmaf(tl, dqx, q0x)), 0), a.nx - 1) >> sh;
+              const int jy = min(max((int)floorf(fmaf(tl, dqy, q0y)), 0), a.ny - 1) >> sh;
+              const int jz = min(max((int)floorf(fmaf(tl, dqz, q0z)), 0), a.nz - 1) >> sh;
+              if (jx != cx || jy != cy || jz != cz) kn = k + 1;
             } else {
               kn = k + 1;
             }
@@ -261,7 +283,8 @@ __global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs one, const
   }
 }
 
-// Negative-value flag of every brick from the volume itself (after an upload).
+// Exact NEG flag of every brick from the volume itself, over the voxels [8B, 8B+8]
+// (clamped to the volume).
 template <int S>
 __global__ void __launch_bounds__(256) rebuild_bricks_kernel(const void* vol, int nx, int ny, int nz, int bx, int by,
                                                             int bz, uint32_t* bricks) {
@@ -271,33 +294,63 @@ __global__ void __launch_bounds__(256) rebuild_bricks_kernel(const void* vol, in
   const typename Vox<S>::V* f = reinterpret_cast<const typename Vox<S>::V*>(vol);
   uint32_t flag = 0;
   for (int z = 8 * iz; z <= min(8 * iz + 8, nz - 1) && !flag; ++z)
-    for (int y = 8 * iy; y <= min(8 * iy + 8, ny - 1) && !flag; ++y)
+    for (int y = 8 * iy; y <= min(8 * iy + 8, ny - 1); ++y)
       for (int x = 8 * ix; x <= min(8 * ix + 8, nx - 1); ++x)
-        if (Vox<S>::raw(f, (uint32_t)x + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z)) < 0.0f) {
+        if (Vox<S>::raw(f, (uint32_t)x + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z)) < 0.0f)
           flag = KF_BRICK_NEG;
-          break;
-        }
   bricks[b] = flag;
+}
+
+// A super-brick is NEG when one of its 8^3 bricks is (they cover [64S, 64S+64]).
+__global__ void __launch_bounds__(256) rebuild_supers_kernel(const uint32_t* bricks, int bx, int by, int bz,
+                                                            uint32_t* supers, int sbx, int sby, int sbz) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (uint32_t)sbx * sby * sbz) return;
+  const int sx = q % sbx, sy = (q / sbx) % sby, sz = q / (sbx * sby);
+  uint32_t f = 0;
+  for (int z = 8 * sz; z < min(8 * sz + 8, bz) && !f; ++z)
+    for (int y = 8 * sy; y < min(8 * sy + 8, by) && !f; ++y)
+      for (int x = 8 * sx; x < min(8 * sx + 8, bx); ++x)
+        f |= bricks[(uint32_t)x + (uint32_t)bx * ((uint32_t)y + (uint32_t)by * (uint32_t)z)] & KF_BRICK_NEG;
+  supers[q] = f;
 }
 
 }  // namespace
 
-int kf_rebuild_bricks(kf_session* s) {
+int kf_rebuild_bricks(kf_session* s, cudaStream_t stream) {
   const uint32_t nb = (uint32_t)s->bx * s->by * s->bz;
   const int g = (int)((nb + 255) / 256);
   switch (s->cfg.storage) {
     case KF_STORAGE_F32F32:
-      rebuild_bricks_kernel<KF_STORAGE_F32F32><<<g, 256, 0, s->stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      rebuild_bricks_kernel<KF_STORAGE_F32F32><<<g, 256, 0, stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
       break;
     case KF_STORAGE_F16U16:
-      rebuild_bricks_kernel<KF_STORAGE_F16U16><<<g, 256, 0, s->stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      rebuild_bricks_kernel<KF_STORAGE_F16U16><<<g, 256, 0, stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
       break;
     default:
-      rebuild_bricks_kernel<KF_STORAGE_RG16I><<<g, 256, 0, s->stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      rebuild_bricks_kernel<KF_STORAGE_RG16I><<<g, 256, 0, stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
       break;
   }
   KF_CUDA_TRY(s, cudaGetLastError());
-  kf_note_launch(s);
+  const uint32_t ns = (uint32_t)s->sbx * s->sby * s->sbz;
+  rebuild_supers_kernel<<<(ns + 255) / 256, 256, 0, stream>>>(s->d_bricks, s->bx, s->by, s->bz, s->d_supers, s->sbx,
+                                                              s->sby, s->sbz);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  kf_note_launch(s, 2);
+  s->frames_since_rebuild = 0;
+  return KF_OK;
+}
+
+int kf_note_integrate(kf_session* s, cudaStream_t stream) {
+  if (++s->frames_since_rebuild < KF_BRICK_REBUILD_EVERY) return KF_OK;
+  return kf_rebuild_bricks(s, stream);
+}
+
+int kf_reset_bricks(kf_session* s) {
+  // an all-zero volume has no negative value
+  const size_t words = (size_t)s->bx * s->by * s->bz + (size_t)s->sbx * s->sby * s->sbz;
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, words * 4, s->stream));
+  s->frames_since_rebuild = 0;
   return KF_OK;
 }
 
@@ -333,6 +386,8 @@ RayArgs make_ray_args(kf_session* s) {
   a.st_out = s->d_state;
   a.bricks = s->d_bricks;
   a.bx = s->bx; a.by = s->by; a.bz = s->bz;
+  a.supers = s->d_supers;
+  a.sbx = s->sbx; a.sby = s->sby; a.sbz = s->sbz;
   return a;
 }
 
