@@ -54,7 +54,7 @@ constexpr int kZC = 16;  // voxels per thread along z
 // integrate.cs can touch: z >= 1e-4, 0 <= u <= W-1, 0 <= v <= H-1 (u, v the +0.5-rounded
 // projection).  Conservative: a box that is not culled is tested voxel by voxel.  Called by
 // a whole warp: lane & 7 evaluates one corner, the ballots combine them.
-__device__ bool box_outside_frustum(const IntArgs& a, const float* inv, const int* b0, const int* b1) {
+__device__ __forceinline__ bool box_outside_frustum(const IntArgs& a, const float* inv, const int* b0, const int* b1) {
   const float vx = a.dimx / a.nx, vy = a.dimy / a.ny, vz = a.dimz / a.nz;
   const float kx0 = a.cx + 0.5f, kx1 = a.cx + 0.5f - (float)(a.W - 1);
   const float ky0 = a.cy + 0.5f, ky1 = a.cy + 0.5f - (float)(a.H - 1);
@@ -102,13 +102,13 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   const float fW1 = (float)(a.W - 1), fH1 = (float)(a.H - 1);
   const float ku = a.cx + 0.5f, kv = a.cy + 0.5f;
   const int zend = min(kZC, a.nz - zb);
-  for (int k = 0; k < zend; ++k, idx += slice) {
-    const float fk = (float)k;
-    const float pz = fmaf(fk, dz[2], p0[2]);
+  // the camera-space position steps by delta along z, as integrate.cs:57-62 does
+  float px = p0[0], py = p0[1], pz = p0[2];
+  for (int k = 0; k < zend; ++k, idx += slice, px += dz[0], py += dz[1], pz += dz[2]) {
     if (pz < 0.0001f) continue;
     const float iz = __fdividef(1.0f, pz);  // hardware reciprocal (2 ulp)
-    const float rx = fmaf(fk, dz[0], p0[0]) * iz;  // pos.x / pos.z
-    const float ry = fmaf(fk, dz[1], p0[1]) * iz;
+    const float rx = px * iz;  // pos.x / pos.z
+    const float ry = py * iz;
     // cameraX.x / cameraX.z + 0.5 = fx * x/z + cx + 0.5 (K has no skew, :67)
     const float u = fmaf(a.fx, rx, ku);
     const float v = fmaf(a.fy, ry, kv);
@@ -216,8 +216,13 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
   if (s_cull) return;
   const int x = xb + threadIdx.x;
   const int y = yb + threadIdx.y;
+  // the same test for this warp's own 32 x 1 x 16 voxels (blocks straddle the frustum's
+  // faces; many of their rows lie wholly outside)
+  const int w0[3] = {xb - 1, y - 1, zb - 1};
+  const int w1[3] = {xb + 32, y + 1, zb + kZC};
+  const bool warp_out = box_outside_frustum(a, inv, w0, w1);
   uint32_t flags = 0;  // integrate_column's bits
-  if (x < a.nx && y < a.ny) flags = integrate_column<S>(a, inv, x, y, zb);
+  if (!warp_out && x < a.nx && y < a.ny) flags = integrate_column<S>(a, inv, x, y, zb);
   if (flags & 0x7u) {
     // this voxel column's own brick and, at brick-low faces, the brick below (dilation)
     const int lx = (x >> 3) - (xb >> 3) + 1, ly = 1;
