@@ -216,13 +216,8 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
   if (s_cull) return;
   const int x = xb + threadIdx.x;
   const int y = yb + threadIdx.y;
-  // the same test for this warp's own 32 x 1 x 16 voxels (blocks straddle the frustum's
-  // faces; many of their rows lie wholly outside)
-  const int w0[3] = {xb - 1, y - 1, zb - 1};
-  const int w1[3] = {xb + 32, y + 1, zb + kZC};
-  const bool warp_out = box_outside_frustum(a, inv, w0, w1);
   uint32_t flags = 0;  // integrate_column's bits
-  if (!warp_out && x < a.nx && y < a.ny) flags = integrate_column<S>(a, inv, x, y, zb);
+  if (x < a.nx && y < a.ny) flags = integrate_column<S>(a, inv, x, y, zb);
   if (flags & 0x7u) {
     // this voxel column's own brick and, at brick-low faces, the brick below (dilation)
     const int lx = (x >> 3) - (xb >> 3) + 1, ly = 1;
