@@ -195,6 +195,11 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
   bool ok = true;
   int iters_run = 0;
   unsigned gi = 0;  // iterations of this launch so far: grid barrier target and sum buffer
+  // the first step's vertices and normals of the next iteration, loaded while the current
+  // iteration's system is solved (valid when pre_level is the level that runs)
+  const float4 none = make_float4(2.0f, 0.f, 0.f, 0.f), zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 pn0 = none, pv0 = zero, pn1 = none, pv1 = zero;
+  int pre_level = -1;
   for (int level = 2; level >= 0 && ok; --level) {
     const int Wl = a.W[level], Hl = a.H[level];
     const int P = Wl * Hl;
@@ -290,10 +295,12 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       const float4* Nl = a.normal[level];
       const float4* Vl = a.vertex[level];
       const int first = (local * kWarps + warp) * 32;
-      const float4 none = make_float4(2.0f, 0.f, 0.f, 0.f), zero = make_float4(0.f, 0.f, 0.f, 0.f);
-      float4 n0 = none, v0 = zero, n1 = none, v1 = zero;
-      if (first + lane < P) { n0 = __ldg(Nl + first + lane); v0 = __ldg(Vl + first + lane); }
-      if (first + stride + lane < P) { n1 = __ldg(Nl + first + stride + lane); v1 = __ldg(Vl + first + stride + lane); }
+      float4 n0 = pn0, v0 = pv0, n1 = pn1, v1 = pv1;
+      if (pre_level != level) {
+        n0 = none; v0 = zero; n1 = none; v1 = zero;
+        if (first + lane < P) { n0 = __ldg(Nl + first + lane); v0 = __ldg(Vl + first + lane); }
+        if (first + stride + lane < P) { n1 = __ldg(Nl + first + stride + lane); v1 = __ldg(Vl + first + stride + lane); }
+      }
       for (int base = first; base < P; base += 2 * stride) {
         const int i0 = base + lane, i1 = base + stride + lane;
         const float4 na = n0, va = v0, nb1 = n1, vb1 = v1;
@@ -382,6 +389,22 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       // stays warm in every SM's instruction cache.
       ok = kf_grid_sync(st, &st->barrier_count, nb * (gi + 1u), &s_flag);
       if (!ok) break;
+      {
+        // the next iteration runs this level again unless the level's iterations are used up
+        // or this solve converges; the first case is known now, the second is rare
+        const int nl = it + 1 < a.iters[level] ? level : level - 1;
+        pre_level = nl;
+        pn0 = none; pv0 = zero; pn1 = none; pv1 = zero;
+        if (nl >= 0) {
+          const int Pn = a.W[nl] * a.H[nl];
+          const int f0 = (local * kWarps + warp) * 32;
+          if (f0 + lane < Pn) { pn0 = __ldg(a.normal[nl] + f0 + lane); pv0 = __ldg(a.vertex[nl] + f0 + lane); }
+          if (f0 + stride + lane < Pn) {
+            pn1 = __ldg(a.normal[nl] + f0 + stride + lane);
+            pv1 = __ldg(a.vertex[nl] + f0 + stride + lane);
+          }
+        }
+      }
       if (tid < 32) s_sums[tid] = (double)__ldcg(accbuf + tid) * kInvFix;
       __syncthreads();
       if (warp == 0) {
