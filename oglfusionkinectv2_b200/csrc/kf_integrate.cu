@@ -189,81 +189,65 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
     bzi = blockIdx.z;
   }
   const IntArgs& a = BATCH ? s_args : a_one;
-  __shared__ int s_cull;
-  // flags of the bricks this block may touch, its own and, for voxels on a brick's low face,
-  // the brick below whose +1 layer they are: [z: bz0-1 .. bz0+1][y: by0-1 .. by0][x: bx0-1 ..
-  // bx0+3]; and of the super-bricks: [z][y][x] = own - 1 .. own
-  __shared__ uint32_t s_neg[3][2][5];
-  __shared__ uint32_t s_sup[2][2][2];
   if (a.gate && *(volatile const int*)a.gate == 0) return;
   float inv[12];  // inverse(m_pose), rows of [R^T | -R^T t] (integrate uses glm::inverse, :1242)
 #pragma unroll
   for (int k = 0; k < 12; ++k) inv[k] = a.st->inv_rows[k];
   const int xb = bxi * 32, yb = byi * 8, zb = bzi * kZC;
-  if (threadIdx.y == 0) {
-    // one voxel of margin on every side absorbs the rounding of the per-voxel tests
+  // Every warp evaluates the block's frustum test itself (the same inputs give the same
+  // answer in every warp), so no warp waits for another: the kernel has no block barrier.
+  // One voxel of margin on every side absorbs the rounding of the per-voxel tests.
+  {
     const int b0[3] = {xb - 1, yb - 1, zb - 1};
     const int b1[3] = {xb + 32, yb + 8, zb + kZC};
-    const bool out = box_outside_frustum(a, inv, b0, b1);
-    if (threadIdx.x == 0) s_cull = out ? 1 : 0;
+    if (box_outside_frustum(a, inv, b0, b1)) return;
   }
-  {
-    const int t = threadIdx.y * 32 + threadIdx.x;
-    if (t < 30) (&s_neg[0][0][0])[t] = 0u;
-    else if (t < 38) (&s_sup[0][0][0])[t - 30] = 0u;
-  }
-  __syncthreads();
-  if (s_cull) return;
-  const int x = xb + threadIdx.x;
-  const int y = yb + threadIdx.y;
+  const int lane = threadIdx.x;
+  const int x = xb + lane;
+  const int y = yb + threadIdx.y;  // uniform over the warp
   uint32_t flags = 0;  // integrate_column's bits
   if (x < a.nx && y < a.ny) flags = integrate_column<S>(a, inv, x, y, zb);
-  if (flags & 0x7u) {
-    // this voxel column's own brick and, at brick-low faces, the brick below (dilation)
-    const int lx = (x >> 3) - (xb >> 3) + 1, ly = 1;
+  if (!__any_sync(0xffffffffu, flags != 0)) return;
+  // Brick flags, merged over the warp: lanes 8c-8..8c-1 write brick column c of the block
+  // (c = 1..4) and a lane on a brick's low x face also brick column c-1 (dilation); lane c
+  // sets the merged bits of column c in global memory.  Most bricks near surfaces have the
+  // bits already, so read first and skip those atomics.
+  const int lx = (x >> 3) - (xb >> 3) + 1;
+  const uint32_t zbits = flags & 7u;
+  uint32_t mine = 0;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    const uint32_t m = (lx == c ? zbits : 0u) | (lx - 1 == c && (x & 7) == 0 ? zbits : 0u);
+    const uint32_t r = __reduce_or_sync(0xffffffffu, m);
+    if (lane == c) mine = r;
+  }
+  if (lane < 5 && mine) {
+    const int gx = (xb >> 3) - 1 + lane;
     for (int j = 0; j < 3; ++j) {
-      const uint32_t f = (flags >> j) & 1u ? KF_BRICK_NEG : 0u;
-      if (!f) continue;
-      atomicOr(&s_neg[j][ly][lx], f);
-      if ((x & 7) == 0) atomicOr(&s_neg[j][ly][lx - 1], f);
-      if ((y & 7) == 0) {
-        atomicOr(&s_neg[j][ly - 1][lx], f);
-        if ((x & 7) == 0) atomicOr(&s_neg[j][ly - 1][lx - 1], f);
+      if (!((mine >> j) & 1u)) continue;
+      const int gz = (zb >> 3) - 1 + j;
+      for (int dy = 0; dy < ((y & 7) == 0 ? 2 : 1); ++dy) {
+        const int gy = (y >> 3) - dy;
+        if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.bx && gy < a.by && gz < a.bz) {
+          uint32_t* w = &a.bricks[(uint32_t)gx + (uint32_t)a.bx * ((uint32_t)gy + (uint32_t)a.by * (uint32_t)gz)];
+          if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
+        }
       }
     }
   }
-  if (flags & 0xc0u) {
-    // super-bricks: own (index 1) and, at super-brick-low faces, the one below (index 0)
-    for (int jz = 0; jz < 2; ++jz) {
-      if (!(flags & (jz ? 0x40u : 0x80u))) continue;
-      atomicOr(&s_sup[jz][1][1], KF_BRICK_NEG);
-      if ((x & 63) == 0) atomicOr(&s_sup[jz][1][0], KF_BRICK_NEG);
-      if ((y & 63) == 0) {
-        atomicOr(&s_sup[jz][0][1], KF_BRICK_NEG);
-        if ((x & 63) == 0) atomicOr(&s_sup[jz][0][0], KF_BRICK_NEG);
-      }
-    }
-  }
-  __syncthreads();
-  {
-    // set the collected bits in global memory; most bricks near and behind surfaces have
-    // them already, so read first and skip those atomics
-    const int t = threadIdx.y * 32 + threadIdx.x;
-    if (t < 30) {
-      const int j = t / 10, r = (t / 5) % 2, c = t % 5;
-      const int gx = (xb >> 3) - 1 + c, gy = (yb >> 3) - 1 + r, gz = (zb >> 3) - 1 + j;
-      const uint32_t f = s_neg[j][r][c];
-      if (f && gx >= 0 && gy >= 0 && gz >= 0 && gx < a.bx && gy < a.by && gz < a.bz) {
-        uint32_t* w = &a.bricks[(uint32_t)gx + (uint32_t)a.bx * ((uint32_t)gy + (uint32_t)a.by * (uint32_t)gz)];
-        if ((*(volatile uint32_t*)w & f) != f) atomicOr(w, f);
-      }
-    } else if (t < 38) {
-      const int q = t - 30, jz = q >> 2, jy = (q >> 1) & 1, jx = q & 1;
-      const int gx = (xb >> 6) - 1 + jx, gy = (yb >> 6) - 1 + jy, gz = (zb >> 6) - 1 + jz;
-      const uint32_t f = s_sup[jz][jy][jx];
-      if (f && gx >= 0 && gy >= 0 && gz >= 0 && gx < a.sbx && gy < a.sby && gz < a.sbz) {
+  // super-bricks: own and, on a super-brick's low face, the one below (x, y, z)
+  const uint32_t sbits = flags & 0xc0u;
+  const uint32_t s_own = __reduce_or_sync(0xffffffffu, sbits);
+  const uint32_t s_lowx = __reduce_or_sync(0xffffffffu, (x & 63) == 0 ? sbits : 0u);
+  if (lane < 8 && (lane & 1 ? s_own : s_lowx)) {
+    const int jx = lane & 1, jy = (lane >> 1) & 1, jz = lane >> 2;
+    const uint32_t zsel = jz ? 0x40u : 0x80u;
+    const uint32_t src = jx ? s_own : s_lowx;
+    if ((src & zsel) && (jy == 1 || (y & 63) == 0)) {
+      const int gx = (xb >> 6) - 1 + jx, gy = (y >> 6) - 1 + jy, gz = (zb >> 6) - 1 + jz;
+      if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.sbx && gy < a.sby && gz < a.sbz) {
         uint32_t* w = &a.supers[(uint32_t)gx + (uint32_t)a.sbx * ((uint32_t)gy + (uint32_t)a.sby * (uint32_t)gz)];
-        if ((*(volatile uint32_t*)w & f) != f) atomicOr(w, f);
+        if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
       }
     }
   }
