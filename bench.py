@@ -475,6 +475,22 @@ def splitmix(x: int) -> int:
     return synth.splitmix64(x) & 0xFFFFFFFF
 
 
+def max_over_ranks(values, world, device):
+    """Elementwise maximum of per-rank timings over all ranks (every rank calls it, in the
+    same order); the slowest replica sets the job's time."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def aggregate_value(world, steps, ms_max):
+    """Whole-job frames/s: every rank steps its own session `steps` frames (replicas)."""
+    return world * steps / (ms_max / 1000.0)
+
+
 def run_reference(args):
     """--impl reference: the reference algorithm's CPU port on this host, same workload."""
     rank = int(os.environ.get("RANK", "0"))
@@ -617,14 +633,11 @@ def main():
         e2e = {"ms": e2e_ms, "wall_s": wall}
 
     # max over ranks of the timed durations
-    times = torch.tensor([dev_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    dev_ms_max, e2e_ms_max = float(times[0]), float(times[1])
+    dev_ms_max, e2e_ms_max = max_over_ranks([dev_ms, e2e["ms"] if e2e else 0.0], world, "cuda")
 
     out = None
     if rank == 0:
-        value = world * K / (dev_ms_max / 1000.0)
+        value = aggregate_value(world, K, dev_ms_max)
         stages = ["pyramid", "track", "integrate", "recover", "raycast"]
         per = {s: float(stage_mean[i]) for i, s in enumerate(stages)}
         dom = "integrate" if per["integrate"] >= per["raycast"] else "raycast"
