@@ -475,6 +475,17 @@ def splitmix(x: int) -> int:
     return synth.splitmix64(x) & 0xFFFFFFFF
 
 
+PLAIN_METRIC = "frames/s at 512^3 TSDF (single session, plain frame step)"
+
+
+def plain_config(w, args, world):
+    """The workload description both arms report for the plain line."""
+    return {"workload": w.name, "volume": list(w.config.volumeSize), "dim_m": 3.0,
+            "storage": args.storage, "jtj": args.jtj, "solve": "f64 cholesky",
+            "depth": "512x424 uint16", "icp_iterations": [10, 5, 4],
+            "quirks": hex(w.config.quirks), "parallelism": f"replicas x{world}", "mc_every": w.mc_every}
+
+
 def max_over_ranks(values, world, device):
     """Elementwise maximum of per-rank timings over all ranks (every rank calls it, in the
     same order); the slowest replica sets the job's time."""
@@ -513,12 +524,11 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     v = steps / dt
     cores = O.Oracle.threads()
-    line = {"impl": "reference", "metric": "frames/s at 512^3 TSDF (single session)", "value": v,
+    line = {"impl": "reference", "metric": PLAIN_METRIC, "value": v,
             "unit": "frames/s", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": 1000 * dt / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w.name, "volume": list(w.config.volumeSize), "dim_m": 3.0,
-                       "depth": "512x424 uint16", "icp_iterations": [10, 5, 4]},
+            "config": {**plain_config(w, args, 1), "sample": "the oracle steps frames only (no marching cubes)"},
             "cpu_baseline": {"value": v, "unit": "frames/s", "cores": cores, "kind": "port",
                              "sample": f"{steps} frames after {warm} untimed (requested {args.steps})"},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -645,17 +655,13 @@ def main():
         algo = algorithmic_bytes(w.config, dom)
         achieved = algo / (per[dom] / 1000.0) / 1e9 if per[dom] > 0 else None
         out = {
-            "metric": "frames/s at 512^3 TSDF (single session, plain frame step)",
+            "metric": PLAIN_METRIC,
             "value": value, "unit": "frames/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": w.name, "volume": list(w.config.volumeSize), "dim_m": 3.0,
-                       "storage": args.storage, "jtj": args.jtj, "solve": "f64 cholesky",
-                       "depth": "512x424 uint16", "icp_iterations": [10, 5, 4],
-                       "quirks": hex(w.config.quirks), "parallelism": f"replicas x{world}",
+            "config": {**plain_config(w, args, world),
                        "l2": "volume > L2 (126 MB); inputs resident",
-                       "mc_every": w.mc_every, "mc_calls": mc_calls,
-                       "mc_ms_mean": (float(np.mean(mc_ms)) if mc_ms else None)},
+                       "mc_calls": mc_calls, "mc_ms_mean": (float(np.mean(mc_ms)) if mc_ms else None)},
             "stage_ms": per, "stage_frames": stage_frames,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak if achieved else None),
