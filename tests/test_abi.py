@@ -115,3 +115,44 @@ def test_batch_and_server_without_device_fail_loudly():
     assert lib.kf_server_create(C.byref(cfg), C.byref(h)) != L.KF_OK
     t0 = lib.kf_server_now()
     assert lib.kf_server_now() >= t0
+
+
+@pytest.mark.parametrize("field,value", [
+    ("nx", 3), ("ny", 4097), ("nz", 0),
+    ("mu", 0.0), ("mu", float("nan")), ("dim_x", -1.0), ("max_weight", 0.0),
+    ("near_plane", 3.0), ("storage", 7), ("jtj", 2), ("tracking", 5),
+])
+def test_invalid_configs_are_rejected(field, value):
+    """Every bad configuration is refused with KF_ERR_INVALID_ARGUMENT before any device work
+    (checked through kf_session_device_bytes, which needs no device)."""
+    lib = L.load()
+    c = L.kf_config()
+    lib.kf_config_default(C.byref(c))
+    setattr(c, field, value)
+    i = L.kf_intrinsics(365, 365, 256, 212, 512, 424)
+    b = C.c_uint64()
+    assert lib.kf_session_device_bytes(C.byref(c), C.byref(i), C.byref(b)) == L.KF_ERR_INVALID_ARGUMENT
+
+
+def test_volume_and_image_limits():
+    lib = L.load()
+    c = L.kf_config()
+    lib.kf_config_default(C.byref(c))
+    i = L.kf_intrinsics(365, 365, 256, 212, 512, 424)
+    b = C.c_uint64()
+    # 32-bit plane offsets: fewer than 2^31 voxels
+    c.nx, c.ny, c.nz = 2048, 1024, 1024
+    assert lib.kf_session_device_bytes(C.byref(c), C.byref(i), C.byref(b)) == L.KF_ERR_INVALID_ARGUMENT
+    c.nx, c.ny, c.nz = 1024, 1024, 1024
+    assert lib.kf_session_device_bytes(C.byref(c), C.byref(i), C.byref(b)) == L.KF_OK
+    # 16-bit weights cannot hold a larger maximum weight
+    c.storage, c.max_weight = L.KF_STORAGE_RG16I, 40000.0
+    assert lib.kf_session_device_bytes(C.byref(c), C.byref(i), C.byref(b)) == L.KF_ERR_INVALID_ARGUMENT
+    c.storage, c.max_weight = L.KF_STORAGE_F32F32, 100.0
+    # three exact mip halvings
+    for w, h in ((510, 424), (512, 8), (8200, 424)):
+        bad = L.kf_intrinsics(365, 365, 256, 212, w, h)
+        assert lib.kf_session_device_bytes(C.byref(c), C.byref(bad), C.byref(b)) == L.KF_ERR_INVALID_ARGUMENT
+    iterations_bad = L.kf_config.from_buffer_copy(c)
+    iterations_bad.iterations[1] = -1
+    assert lib.kf_session_device_bytes(C.byref(iterations_bad), C.byref(i), C.byref(b)) == L.KF_ERR_INVALID_ARGUMENT
