@@ -215,6 +215,27 @@ KF_API int kf_get_volume(kf_session* s, kf_volume_view* view);
 KF_API int kf_copy_volume_to_host(kf_session* s, void* dst, uint64_t bytes);
 KF_API int kf_copy_volume_from_host(kf_session* s, const void* src, uint64_t bytes);
 KF_API int kf_get_cum_twist(kf_session* s, double twist[6]); /* getCumTwist, gFusion.h:260-265 */
+/* Volume ray-sum image (intensityProjection, gFusion.cpp:1368-1409, shaders/mip.cs) at
+ * the current pose: per pixel (sum of the positive trilinear TSDF samples taken every
+ * 0.75 mu between the slab entry/near plane and exit/far plane, 0, 0, 1); W*H*4 floats.
+ * Its device image (W*H*16 bytes) is allocated on the first call and kept. */
+KF_API int kf_intensity_projection(kf_session* s, float* rgba);
+/* Volume checkpoint (the reference keeps none; Reset, gFusion.cpp:226-240, only clears).
+ * The file is one JSON header line (format "kf-volume-checkpoint", sizes, metric volume
+ * size, mu, pose) followed by the raw volume, the session's device control block (pose,
+ * pose library, frame policy), the raycast maps and the trackSDF rows: a session loaded
+ * from it steps on exactly as the saved one would have.  Loading requires the same
+ * storage, volume size, metric size, mu and image size and a file written by this library
+ * build (KF_ERR_INVALID_ARGUMENT otherwise, KF_ERR_IO for a short or unreadable file; the
+ * session is left untouched by both).  File errors are KF_ERR_IO. */
+KF_API int kf_save_volume(kf_session* s, const char* path);
+KF_API int kf_load_volume(kf_session* s, const char* path);
+/* Self-test of the bounded device waits: one block waits at a two-block grid barrier that
+ * the other block never reaches; after budget_cycles (1e3 .. 1e9 SM clocks) the wait gives
+ * up, records the timeout in the session's device error word and the kernel ends.  Returns
+ * KF_ERR_TIMEOUT, exactly as a tracking call whose barrier timed out would, and clears the
+ * error word; the session stays usable. */
+KF_API int kf_selftest_barrier_timeout(kf_session* s, long long budget_cycles);
 KF_API int kf_get_pose_library_size(kf_session* s, int* n);
 /* Device times in milliseconds of the last call of each stage, in the order
  * pyramid, track, integrate, raycast, recover, mc. */

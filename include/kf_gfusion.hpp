@@ -115,6 +115,15 @@ class GFusion {
     Pose p = getPose();
     return {p[12], p[13], p[14]};
   }
+  // intensityProjection (gFusion.cpp:1368-1409): W*H RGBA floats, (ray sum, 0, 0, 1)
+  std::vector<float> intensityProjection() {
+    std::vector<float> m((size_t)intr_.width * intr_.height * 4);
+    check(kf_intensity_projection(s_, m.data()), "kf_intensity_projection");
+    return m;
+  }
+  // volume checkpoint: the session steps on from a loaded file exactly as it would have
+  void saveVolume(const std::string& path) { check(kf_save_volume(s_, path.c_str()), "kf_save_volume"); }
+  void loadVolume(const std::string& path) { check(kf_load_volume(s_, path.c_str()), "kf_load_volume"); }
   std::array<float, 6> getTimes() {
     std::array<float, 6> t;
     check(kf_get_stage_times(s_, t.data()), "kf_get_stage_times");

@@ -125,6 +125,10 @@ SIGNATURES = {
     "kf_copy_volume_to_host": (_I, [_P, _P, C.c_uint64]),
     "kf_copy_volume_from_host": (_I, [_P, _P, C.c_uint64]),
     "kf_get_cum_twist": (_I, [_P, _PD]),
+    "kf_intensity_projection": (_I, [_P, _P]),
+    "kf_save_volume": (_I, [_P, C.c_char_p]),
+    "kf_load_volume": (_I, [_P, C.c_char_p]),
+    "kf_selftest_barrier_timeout": (_I, [_P, C.c_longlong]),
     "kf_get_pose_library_size": (_I, [_P, C.POINTER(_I)]),
     "kf_get_stage_times": (_I, [_P, _PF]),
     "kf_get_stage_stats": (_I, [_P, _PD, C.POINTER(C.c_uint64)]),

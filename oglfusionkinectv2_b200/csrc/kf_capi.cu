@@ -108,6 +108,7 @@ void free_all(kf_session* s) {
   cudaFree(s->d_partials);
   cudaFree(s->d_state);
   cudaFree(s->d_u32_scalar);
+  cudaFree(s->d_mip);
   if (s->h_state) cudaFreeHost(s->h_state);
   if (s->h_depth_pinned) cudaFreeHost(s->h_depth_pinned);
   if (s->h_u32_scalar) cudaFreeHost(s->h_u32_scalar);
@@ -495,7 +496,7 @@ int kf_destroy(kf_session* s) {
 const char* kf_last_error(const kf_session* s) { return s ? s->last_error.c_str() : "null session"; }
 
 int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
-  if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
+  if (!s || !pose || !kf_pose_is_finite(pose)) return KF_ERR_INVALID_ARGUMENT;
   int rc;
   if (delete_flag) {
     KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
@@ -508,8 +509,11 @@ int kf_reset(kf_session* s, const double pose[16], int delete_flag) {
   if ((rc = pull_state(s))) return rc;
   s->h_state->lib_size = 0;  // poseLibrary.resize(0)
   // the ICP accumulation centre is carried from frame to frame; a new reconstruction starts
-  // from the camera origin, as a new session does
-  for (int k = 0; k < 3; ++k) s->h_state->icp_center_cam[k] = 0.0;
+  // from the one a new session has (1 m in front of the camera), so that a reset session
+  // computes exactly what a new one does
+  s->h_state->icp_center_cam[0] = 0.0;
+  s->h_state->icp_center_cam[1] = 0.0;
+  s->h_state->icp_center_cam[2] = 1.0;
   set_pose_fields(s, pose, true);
   // the app's "Reset Volume" (kinect.cpp:446-477): reset = true, counter = 0, then a
   // raycast of the empty volume, i.e. zero reference maps
@@ -531,7 +535,7 @@ int kf_reset_volume(kf_session* s) {
 }
 
 int kf_reset_pose(kf_session* s, const double pose[16]) {
-  if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
+  if (!s || !pose || !kf_pose_is_finite(pose)) return KF_ERR_INVALID_ARGUMENT;
   int rc = pull_state(s);
   if (rc) return rc;
   set_pose_fields(s, pose, true);
@@ -539,7 +543,7 @@ int kf_reset_pose(kf_session* s, const double pose[16]) {
 }
 
 int kf_set_pose(kf_session* s, const double pose[16]) {
-  if (!s || !pose) return KF_ERR_INVALID_ARGUMENT;
+  if (!s || !pose || !kf_pose_is_finite(pose)) return KF_ERR_INVALID_ARGUMENT;
   int rc = pull_state(s);
   if (rc) return rc;
   set_pose_fields(s, pose, false);
@@ -750,6 +754,219 @@ int kf_copy_volume_from_host(kf_session* s, const void* src, uint64_t bytes) {
   if (rc) return rc;
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return KF_OK;
+}
+
+// ---- volume checkpoint -------------------------------------------------------------------
+// The reference keeps no volume on disk (gFusion::Reset, src/gFusion.cpp:226-240, only
+// reallocates or zero-fills).  A checkpoint here is everything the next frame step reads:
+// one JSON header line, then the raw sections in this order: the volume (value plane, then
+// weight plane), the device control block (pose, pose library, frame-policy flags), the
+// raycast vertex and normal maps and the trackSDF rows.  A session loaded from it steps on
+// exactly as the saved one would have.
+namespace {
+
+const char kCkptFormat[] = "kf-volume-checkpoint";
+const size_t kCkptChunk = (size_t)32 << 20;
+
+struct CkptSection {
+  void* dev;
+  size_t bytes;
+};
+
+void ckpt_sections(kf_session* s, CkptSection out[4]) {
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  out[0] = {s->d_vol, s->vol_bytes};
+  out[1] = {s->d_ref_vertex, px * 16};
+  out[2] = {s->d_ref_normal, px * 16};
+  out[3] = {s->d_sdf_rows, px * 32};
+}
+
+std::string ckpt_header(kf_session* s) {
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  char buf[2048];
+  int n = std::snprintf(
+      buf, sizeof(buf),
+      "{\"format\":\"%s\",\"version\":1,\"storage\":%d,\"nx\":%d,\"ny\":%d,\"nz\":%d,"
+      "\"dim_x\":%.9g,\"dim_y\":%.9g,\"dim_z\":%.9g,\"mu\":%.9g,\"width\":%d,\"height\":%d,"
+      "\"volume_bytes\":%llu,\"state_bytes\":%llu,\"map_bytes\":%llu,\"sdf_bytes\":%llu,\"pose\":[",
+      kCkptFormat, s->cfg.storage, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->cfg.dim_x, s->cfg.dim_y, s->cfg.dim_z,
+      s->cfg.mu, s->W[0], s->H[0], (unsigned long long)s->vol_bytes, (unsigned long long)sizeof(KfDevState),
+      (unsigned long long)(px * 16), (unsigned long long)(px * 32));
+  std::string h(buf, (size_t)n);
+  for (int k = 0; k < 16; ++k) {
+    n = std::snprintf(buf, sizeof(buf), "%s%.17g", k ? "," : "", s->h_state->pose[k]);
+    h.append(buf, (size_t)n);
+  }
+  h += "]}\n";
+  return h;
+}
+
+bool json_number(const std::string& h, const char* key, double* v) {
+  const std::string k = std::string("\"") + key + "\":";
+  const size_t p = h.find(k);
+  if (p == std::string::npos) return false;
+  const char* c = h.c_str() + p + k.size();
+  char* end = nullptr;
+  *v = std::strtod(c, &end);
+  return end != c;
+}
+
+bool json_string_is(const std::string& h, const char* key, const char* want) {
+  const std::string k = std::string("\"") + key + "\":\"" + want + "\"";
+  return h.find(k) != std::string::npos;
+}
+
+int copy_section_to_file(kf_session* s, std::FILE* f, const void* dev, size_t bytes, std::vector<char>& buf) {
+  for (size_t o = 0; o < bytes; o += kCkptChunk) {
+    const size_t n = std::min(kCkptChunk, bytes - o);
+    KF_CUDA_TRY(s, cudaMemcpyAsync(buf.data(), static_cast<const char*>(dev) + o, n, cudaMemcpyDeviceToHost, s->stream));
+    KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (std::fwrite(buf.data(), 1, n, f) != n) return fail(s, KF_ERR_IO, "checkpoint write failed");
+  }
+  return KF_OK;
+}
+
+int copy_section_from_file(kf_session* s, std::FILE* f, void* dev, size_t bytes, std::vector<char>& buf) {
+  for (size_t o = 0; o < bytes; o += kCkptChunk) {
+    const size_t n = std::min(kCkptChunk, bytes - o);
+    if (std::fread(buf.data(), 1, n, f) != n) return fail(s, KF_ERR_IO, "checkpoint read failed");
+    KF_CUDA_TRY(s, cudaMemcpyAsync(static_cast<char*>(dev) + o, buf.data(), n, cudaMemcpyHostToDevice, s->stream));
+    KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  }
+  return KF_OK;
+}
+
+}  // namespace
+
+int kf_save_volume(kf_session* s, const char* path) {
+  if (!s || !path) return KF_ERR_INVALID_ARGUMENT;
+  int rc = pull_state(s);
+  if (rc) return rc;
+  std::FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(s, KF_ERR_IO, std::string("cannot open ") + path);
+  const std::string h = ckpt_header(s);
+  CkptSection sec[4];
+  ckpt_sections(s, sec);
+  std::vector<char> buf(kCkptChunk);
+  if (std::fwrite(h.data(), 1, h.size(), f) != h.size()) rc = fail(s, KF_ERR_IO, "checkpoint write failed");
+  if (!rc) rc = copy_section_to_file(s, f, sec[0].dev, sec[0].bytes, buf);
+  if (!rc && std::fwrite(s->h_state, 1, sizeof(KfDevState), f) != sizeof(KfDevState))
+    rc = fail(s, KF_ERR_IO, "checkpoint write failed");
+  for (int k = 1; k < 4 && !rc; ++k) rc = copy_section_to_file(s, f, sec[k].dev, sec[k].bytes, buf);
+  if (std::fclose(f) != 0 && !rc) rc = fail(s, KF_ERR_IO, "checkpoint close failed");
+  return rc;
+}
+
+int kf_load_volume(kf_session* s, const char* path) {
+  if (!s || !path) return KF_ERR_INVALID_ARGUMENT;
+  std::FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(s, KF_ERR_IO, std::string("cannot open ") + path);
+  // header line (bounded)
+  std::string h;
+  for (int c; h.size() < 4096 && (c = std::fgetc(f)) != EOF;) {
+    h.push_back((char)c);
+    if (c == '\n') break;
+  }
+  CkptSection sec[4];
+  ckpt_sections(s, sec);
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  double v = 0;
+  int rc = KF_OK;
+  auto need = [&](const char* key, double want) {
+    if (!rc && !(json_number(h, key, &v) && v == want))
+      rc = fail(s, KF_ERR_INVALID_ARGUMENT, std::string("checkpoint ") + key + " does not match the session");
+  };
+  // floats are written with 9 significant digits, which round-trip a float
+  auto need_f = [&](const char* key, float want) {
+    if (!rc && !(json_number(h, key, &v) && (float)v == want))
+      rc = fail(s, KF_ERR_INVALID_ARGUMENT, std::string("checkpoint ") + key + " does not match the session");
+  };
+  if (h.empty() || h.back() != '\n' || !json_string_is(h, "format", kCkptFormat))
+    rc = fail(s, KF_ERR_INVALID_ARGUMENT, "not a volume checkpoint");
+  need("version", 1);
+  need("storage", s->cfg.storage);
+  need("nx", s->cfg.nx);
+  need("ny", s->cfg.ny);
+  need("nz", s->cfg.nz);
+  need("width", s->W[0]);
+  need("height", s->H[0]);
+  // the TSDF's meaning depends on the volume's metric size and truncation distance
+  need_f("dim_x", s->cfg.dim_x);
+  need_f("dim_y", s->cfg.dim_y);
+  need_f("dim_z", s->cfg.dim_z);
+  need_f("mu", s->cfg.mu);
+  need("volume_bytes", (double)s->vol_bytes);
+  need("state_bytes", (double)sizeof(KfDevState));  // the control block of this library build
+  need("map_bytes", (double)(px * 16));
+  need("sdf_bytes", (double)(px * 32));
+  // the whole payload must be there before the session is touched
+  if (!rc) {
+    const long long payload = (long long)(s->vol_bytes + sizeof(KfDevState) + px * 64);
+    const long long at = (long long)h.size();
+    if (std::fseek(f, 0, SEEK_END) != 0 || (long long)std::ftell(f) != at + payload ||
+        std::fseek(f, (long)at, SEEK_SET) != 0)
+      rc = fail(s, KF_ERR_IO, "checkpoint has the wrong size");
+  }
+  if (rc) {
+    std::fclose(f);
+    return rc;
+  }
+  // the control block is read and checked before anything is written to the device
+  std::vector<char> state(sizeof(KfDevState));
+  std::vector<char> buf(kCkptChunk);
+  if (std::fseek(f, (long)(h.size() + s->vol_bytes), SEEK_SET) != 0 ||
+      std::fread(state.data(), 1, state.size(), f) != state.size() ||
+      std::fseek(f, (long)h.size(), SEEK_SET) != 0)
+    rc = fail(s, KF_ERR_IO, "checkpoint read failed");
+  KfDevState* st = reinterpret_cast<KfDevState*>(state.data());
+  if (!rc && (!kf_pose_is_finite(st->pose) || st->lib_size < 0 || st->lib_size > KF_MAX_LIBRARY))
+    rc = fail(s, KF_ERR_INVALID_ARGUMENT, "checkpoint control block is invalid");
+  if (!rc) {
+    KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    free_mc(s);  // a mesh of the old volume
+    rc = copy_section_from_file(s, f, sec[0].dev, sec[0].bytes, buf);
+  }
+  if (!rc && std::fseek(f, (long)sizeof(KfDevState), SEEK_CUR) != 0) rc = fail(s, KF_ERR_IO, "checkpoint read failed");
+  for (int k = 1; k < 4 && !rc; ++k) rc = copy_section_from_file(s, f, sec[k].dev, sec[k].bytes, buf);
+  std::fclose(f);
+  if (rc) return rc;
+  std::memcpy(s->h_state, st, sizeof(KfDevState));
+  s->h_state->error = 0;
+  if ((rc = push_state(s))) return rc;
+  if ((rc = kf_rebuild_bricks(s, s->stream))) return rc;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return KF_OK;
+}
+
+// ---- intensity projection (gFusion::intensityProjection, src/gFusion.cpp:1368-1409) ------
+int kf_intensity_projection(kf_session* s, float* rgba) {
+  if (!s || !rgba) return KF_ERR_INVALID_ARGUMENT;
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  int rc;
+  if (!s->d_mip && (rc = dalloc(s, &s->d_mip, px))) return rc;
+  if ((rc = kf_launch_intensity_projection(s, s->d_mip))) return rc;
+  return copy_out(s, rgba, s->d_mip, px * 16);
+}
+
+// ---- bounded-wait self-test ------------------------------------------------------------------
+namespace {
+// Block 0 waits at a two-block barrier that block 1 never reaches, so its bounded wait
+// must give up and record KF_DEV_ERR_TIMEOUT in the session's device error word.
+__global__ void barrier_timeout_selftest_kernel(unsigned* counter, int* error, long long budget) {
+  __shared__ int s_flag;
+  if (blockIdx.x != 0) return;
+  kf_grid_sync_bounded(error, counter, 2u, &s_flag, budget);
+}
+}  // namespace
+
+int kf_selftest_barrier_timeout(kf_session* s, long long budget_cycles) {
+  if (!s || budget_cycles < 1000 || budget_cycles > KF_BARRIER_SPIN_CYCLES) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_u32_scalar, 0, sizeof(uint32_t), s->stream));
+  barrier_timeout_selftest_kernel<<<2, 32, 0, s->stream>>>(s->d_u32_scalar, &s->d_state->error, budget_cycles);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  kf_note_launch(s);
+  // the host side of every tracking call: read the sticky error word, report and clear it
+  return pull_state_head(s);
 }
 
 int kf_get_cum_twist(kf_session* s, double t[6]) {

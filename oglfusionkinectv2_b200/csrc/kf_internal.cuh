@@ -5,6 +5,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -137,6 +138,8 @@ struct kf_session {
   size_t mc_scratch_words = 0;       // capacity of d_mc_scratch in bytes
   uint32_t* d_u32_scalar = nullptr;  // one device word for totals
   uint32_t* h_u32_scalar = nullptr;  // pinned
+
+  float4* d_mip = nullptr;  // intensity-projection image, allocated on first use
 };
 
 // ---------------------------------------------------------------------------------------
@@ -489,27 +492,42 @@ __device__ __forceinline__ unsigned kf_ld_acquire_gpu(const unsigned* p) {
 // of the block before it; an acquirer that observes the release sees them.
 // Grid barrier over a counter that only grows during a launch (the launcher zeroes it):
 // every block adds one and waits until `target` arrivals in total.  One release
-// reduction per block and no reset step; bounded like kf_grid_wait.
-__device__ inline bool kf_grid_sync(KfDevState* st, unsigned* counter, unsigned target, int* s_flag) {
+// reduction per block and no reset step.  The wait gives up after `budget` clock64 cycles,
+// records KF_DEV_ERR_TIMEOUT in *error and returns false; a block that sees an error
+// recorded by another block returns false as well.
+__device__ inline bool kf_grid_sync_bounded(int* error, unsigned* counter, unsigned target, int* s_flag,
+                                            long long budget) {
   __syncthreads();
   if (threadIdx.x == 0) {
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
     int ok = 1;
     const long long t0 = clock64();
     while (kf_ld_acquire_gpu(counter) < target) {
-      if (*(volatile int*)&st->error) { ok = 0; break; }
-      if (clock64() - t0 > KF_BARRIER_SPIN_CYCLES) {
-        atomicExch(&st->error, KF_DEV_ERR_TIMEOUT);
+      if (*(volatile int*)error) { ok = 0; break; }
+      if (clock64() - t0 > budget) {
+        atomicExch(error, KF_DEV_ERR_TIMEOUT);
         ok = 0;
         break;
       }
       __nanosleep(32);
     }
-    if (*(volatile int*)&st->error) ok = 0;
+    if (*(volatile int*)error) ok = 0;
     *s_flag = ok;
   }
   __syncthreads();
   return *s_flag != 0;
+}
+
+// The tracking kernels' barrier: errors go to the session's sticky device error word.
+__device__ __forceinline__ bool kf_grid_sync(KfDevState* st, unsigned* counter, unsigned target, int* s_flag) {
+  return kf_grid_sync_bounded(&st->error, counter, target, s_flag, KF_BARRIER_SPIN_CYCLES);
+}
+
+// A pose passed in by the caller must be finite (NaN or Inf would poison the device state).
+inline bool kf_pose_is_finite(const double* p) {
+  for (int k = 0; k < 16; ++k)
+    if (!std::isfinite(p[k])) return false;
+  return true;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -616,6 +634,7 @@ int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy);
 int kf_launch_sdf_policy(kf_session* s);
 int kf_launch_integrate(kf_session* s, int gated);
 int kf_launch_raycast(kf_session* s);
+int kf_launch_intensity_projection(kf_session* s, float4* out);
 int kf_rebuild_bricks(kf_session* s, cudaStream_t stream);
 int kf_reset_bricks(kf_session* s);
 int kf_note_integrate(kf_session* s, cudaStream_t stream);

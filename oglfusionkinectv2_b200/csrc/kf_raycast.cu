@@ -283,6 +283,66 @@ __global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs one, const
   }
 }
 
+// Volume ray-sum image (gFusion::intensityProjection, src/gFusion.cpp:1368-1409, and
+// shaders/mip.cs:52-104): the raycast's view, slab test and near/far clipping, then samples
+// every largeStep from tnear while t < tfar, summing the positive interpolated values into
+// x; the pixel is (sum, 0, 0, 1), misses included (mip.cs's other two branches add zero or
+// are unreachable).  Sample positions are tnear + k * largeStep (one rounding, as in the
+// raycast).  The reference dispatches it on demand, never from the frame loop; so does this.
+template <int S>
+__global__ void __launch_bounds__(kRayThreads) mip_kernel(RayArgs a, float4* out) {
+  __shared__ float s_view[12];
+  if (threadIdx.y == 0 && threadIdx.x < 12) {
+    const int r = threadIdx.x >> 2, c = threadIdx.x & 3;
+    const float* P = a.st->pose_rows;
+    float v;
+    if (c == 0) v = P[r * 4 + 0] * a.ikx;
+    else if (c == 1) v = P[r * 4 + 1] * a.iky;
+    else if (c == 2) v = fmaf(P[r * 4 + 0], a.ikcx, fmaf(P[r * 4 + 1], a.ikcy, P[r * 4 + 2]));
+    else v = P[r * 4 + 3];
+    s_view[r * 4 + c] = v;
+  }
+  __syncthreads();
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= a.W || y >= a.H) return;
+  Sampler<S> smp;
+  smp.f = reinterpret_cast<const typename Vox<S>::V*>(a.vol);
+  smp.nx = a.nx; smp.ny = a.ny; smp.nz = a.nz;
+  smp.sxy = (uint32_t)a.nx * (uint32_t)a.ny;
+
+  const float ox = s_view[3], oy = s_view[7], oz = s_view[11];
+  const float fxp = (float)x, fyp = (float)y;
+  const float dx = fmaf(s_view[0], fxp, fmaf(s_view[1], fyp, s_view[2]));
+  const float dy = fmaf(s_view[4], fxp, fmaf(s_view[5], fyp, s_view[6]));
+  const float dzv = fmaf(s_view[8], fxp, fmaf(s_view[9], fyp, s_view[10]));
+  // slab test (mip.cs:61-77, as raycast.cs:141-152)
+  const float ix = 1.0f / dx, iy = 1.0f / dy, iz = 1.0f / dzv;
+  const float tbx = -1.0f * ix * ox, tby = -1.0f * iy * oy, tbz = -1.0f * iz * oz;
+  const float ttx = ix * (a.dimx - ox), tty = iy * (a.dimy - oy), ttz = iz * (a.dimz - oz);
+  const float tminx = fminf(ttx, tbx), tminy = fminf(tty, tby), tminz = fminf(ttz, tbz);
+  const float tmaxx = fmaxf(ttx, tbx), tmaxy = fmaxf(tty, tby), tmaxz = fmaxf(ttz, tbz);
+  const float largest_tmin = fmaxf(fmaxf(tminx, tminy), fmaxf(tminx, tminz));
+  const float smallest_tmax = fminf(fminf(tmaxx, tmaxy), fminf(tmaxx, tmaxz));
+  const float tnear = fmaxf(largest_tmin, a.nearp);
+  const float tfar = fminf(smallest_tmax, a.farp);
+
+  float sum = 0.0f;
+  if (tnear < tfar) {
+    const float scale = Vox<S>::kRawToF;
+    const float q0x = fmaf(ox, a.sx, -0.5f), q0y = fmaf(oy, a.sy, -0.5f), q0z = fmaf(oz, a.sz, -0.5f);
+    const float dqx = dx * a.sx, dqy = dy * a.sy, dqz = dzv * a.sz;
+    // bounded: max_steps covers (far - near) / min(step, largeStep) samples
+    for (int k = 0; k < a.max_steps; ++k) {
+      const float t = fmaf((float)k, a.large_step, tnear);
+      if (!(t < tfar)) break;
+      const float f = smp.interp_raw(fmaf(t, dqx, q0x), fmaf(t, dqy, q0y), fmaf(t, dqz, q0z)) * scale;
+      if (f > 0.0f) sum += f;
+    }
+  }
+  out[(size_t)y * a.W + x] = make_float4(sum, 0.0f, 0.0f, 1.0f);
+}
+
 // Exact NEG flag of every brick from the volume itself, over the voxels [8B, 8B+8]
 // (clamped to the volume).
 template <int S>
@@ -407,6 +467,20 @@ int kf_launch_raycast(kf_session* s) {
   const RayArgs a = make_ray_args(s);
   dim3 grid((a.W + 31) / 32, (a.H + kRayRows - 1) / kRayRows);
   launch_ray<false>(s->cfg.storage, grid, s->stream, a, nullptr);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  kf_note_launch(s);
+  return KF_OK;
+}
+
+int kf_launch_intensity_projection(kf_session* s, float4* out) {
+  const RayArgs a = make_ray_args(s);
+  dim3 grid((a.W + 31) / 32, (a.H + kRayRows - 1) / kRayRows);
+  dim3 block(32, kRayRows);
+  switch (s->cfg.storage) {
+    case KF_STORAGE_F32F32: mip_kernel<KF_STORAGE_F32F32><<<grid, block, 0, s->stream>>>(a, out); break;
+    case KF_STORAGE_F16U16: mip_kernel<KF_STORAGE_F16U16><<<grid, block, 0, s->stream>>>(a, out); break;
+    default: mip_kernel<KF_STORAGE_RG16I><<<grid, block, 0, s->stream>>>(a, out); break;
+  }
   KF_CUDA_TRY(s, cudaGetLastError());
   kf_note_launch(s);
   return KF_OK;

@@ -146,7 +146,7 @@ const char* kf_server_last_error(const kf_server* v) { return v ? v->last_error.
 double kf_server_now(void) { return now_s(); }
 
 int kf_server_open(kf_server* v, const kf_config* cfg, const kf_intrinsics* intr, const double pose[16], int* id) {
-  if (!v || !cfg || !intr || !pose || !id) return KF_ERR_INVALID_ARGUMENT;
+  if (!v || !cfg || !intr || !pose || !id || !kf_pose_is_finite(pose)) return KF_ERR_INVALID_ARGUMENT;
   kf_config c = *cfg;
   c.storage = v->cfg.storage;
   c.jtj = v->cfg.jtj;

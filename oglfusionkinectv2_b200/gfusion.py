@@ -9,6 +9,7 @@ they cross the ABI column-major (glm layout).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -262,6 +263,25 @@ class GFusion:
         raw = np.ascontiguousarray(raw, dtype=np.uint8)
         self._check(self.lib.kf_copy_volume_from_host(self._h, raw.ctypes.data, raw.nbytes),
                     "kf_copy_volume_from_host")
+
+    def intensityProjection(self) -> np.ndarray:
+        """Volume ray-sum image at the current pose (gFusion::intensityProjection,
+        src/gFusion.cpp:1368-1409), H x W x 4: (sum of positive samples, 0, 0, 1)."""
+        m = np.empty((self.intrinsics.height, self.intrinsics.width, 4), np.float32)
+        self._check(self.lib.kf_intensity_projection(self._h, m.ctypes.data), "kf_intensity_projection")
+        return m
+
+    def saveVolume(self, path) -> None:
+        """Checkpoint the volume, pose, pose library and reference maps to `path`."""
+        self._check(self.lib.kf_save_volume(self._h, os.fsencode(path)), "kf_save_volume")
+
+    def loadVolume(self, path) -> None:
+        """Restore a checkpoint written by saveVolume into this (same-sized) session."""
+        self._check(self.lib.kf_load_volume(self._h, os.fsencode(path)), "kf_load_volume")
+
+    def selftestBarrierTimeout(self, budget_cycles: int = 2_000_000) -> int:
+        """Run the bounded-wait self-test; returns the status (KF_ERR_TIMEOUT expected)."""
+        return int(self.lib.kf_selftest_barrier_timeout(self._h, int(budget_cycles)))
 
     def getVolume(self):
         """(tsdf, weight) float32 arrays indexed [z, y, x]."""

@@ -1036,6 +1036,54 @@ void raycast(or_session* s) {
     }
 }
 
+/* ---- intensityProjection(): gFusion.cpp:1368-1409 + mip.cs:52-104 -------------------------
+ * The raycast's view, slab test and near/far clipping; samples every largeStep = 0.75 mu
+ * from tnear while t < tfar (mip.cs:82-100, t = tnear + k * largeStep here); positive
+ * samples add to x (the f == 0 branch adds zero to z, the third branch is unreachable);
+ * every pixel, misses included, is (sum, 0, 0, 1). */
+void intensity_projection(or_session* s, double* rgba) {
+  const int W = s->intr.width, H = s->intr.height;
+  double invK[16], view[16];
+  std::memset(invK, 0, sizeof(invK));
+  M(invK, 0, 0) = 1.0 / s->intr.fx; M(invK, 2, 0) = -s->intr.cx / s->intr.fx;
+  M(invK, 1, 1) = 1.0 / s->intr.fy; M(invK, 2, 1) = -s->intr.cy / s->intr.fy;
+  M(invK, 2, 2) = 1; M(invK, 3, 3) = 1;
+  mat4_mul(s->pose, invK, view);
+  const double dim[3] = {s->cfg.dim_x, s->cfg.dim_y, s->cfg.dim_z};
+  const double large_step = 0.75 * s->cfg.mu;
+  const double nearp = s->cfg.near_plane, farp = s->cfg.far_plane;
+  RaySampler rs(s);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      double o[3] = {Mc(view, 3, 0), Mc(view, 3, 1), Mc(view, 3, 2)};
+      double pix[3] = {(double)x, (double)y, 1.0};
+      double d[3];
+      xform(view, pix, 0.0, d);
+      double tmin[3], tmax[3];
+      for (int a = 0; a < 3; ++a) {
+        double inv = 1.0 / d[a];
+        double tb = -1.0 * inv * o[a], tt = inv * (dim[a] - o[a]);
+        tmin[a] = std::min(tt, tb);
+        tmax[a] = std::max(tt, tb);
+      }
+      double largest_tmin = std::max(std::max(tmin[0], tmin[1]), std::max(tmin[0], tmin[2]));
+      double smallest_tmax = std::min(std::min(tmax[0], tmax[1]), std::min(tmax[0], tmax[2]));
+      double tnear = std::max(largest_tmin, nearp), tfar = std::min(smallest_tmax, farp);
+      double sum = 0.0;
+      if (tnear < tfar)
+        for (long k = 0;; ++k) {
+          const double t = tnear + (double)k * large_step;
+          if (!(t < tfar)) break;
+          double q[3] = {o[0] + d[0] * t, o[1] + d[1] * t, o[2] + d[2] * t};
+          const double f = rs.interp(q);
+          if (f > 0) sum += f;
+        }
+      double* px = &rgba[4 * ((size_t)y * W + x)];
+      px[0] = sum; px[1] = 0.0; px[2] = 0.0; px[3] = 1.0;
+    }
+}
+
 /* ---- marching cubes: histoPyramids.cs classifyCubes/constructHPLevel + traverse ----------- */
 const int kHpOff[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 0, 1}, {1, 0, 1},
                           {0, 1, 0}, {1, 1, 0}, {0, 1, 1}, {1, 1, 1}}; /* cubeOffsets */
@@ -1319,6 +1367,12 @@ int or_sdf_reduce_once(or_session* s, int level, const double T[16], double sums
 
 int or_integrate(or_session* s) { integrate(s); return KF_OK; }
 int or_raycast(or_session* s) { raycast(s); return KF_OK; }
+
+int or_intensity_projection(or_session* s, double* rgba) {
+  if (!s || !rgba) return KF_ERR_INVALID_ARGUMENT;
+  intensity_projection(s, rgba);
+  return KF_OK;
+}
 
 int or_frame_step_u16(or_session* s, const uint16_t* depth_mm, int* tracked_out) {
   /* kinect.cpp:654-695 with trackDepthToPoint / trackDepthToVolume from cfg.tracking */

@@ -56,6 +56,8 @@ int or_sdf_reduce_once(or_session* s, int level, const double cam_to_world[16], 
 
 int or_integrate(or_session* s);
 int or_raycast(or_session* s);
+/* intensityProjection (gFusion.cpp:1368-1409, mip.cs): W*H*4 doubles, (sum, 0, 0, 1). */
+int or_intensity_projection(or_session* s, double* rgba);
 int or_frame_step_u16(or_session* s, const uint16_t* depth_mm, int* tracked);
 
 int or_get_raycast(or_session* s, double* vertex4, double* normal4);

@@ -28,7 +28,7 @@ _SIG = {
     "or_track_sdf": [_P, C.POINTER(_I)], "or_recover_pose": [_P, C.POINTER(_I)],
     "or_get_alignment_energy": [_P, _PD], "or_get_reduction": [_P, _PD],
     "or_icp_reduce_once": [_P, _I, _PD], "or_sdf_reduce_once": [_P, _I, _PD, _PD],
-    "or_integrate": [_P], "or_raycast": [_P], "or_frame_step_u16": [_P, _P, C.POINTER(_I)],
+    "or_integrate": [_P], "or_raycast": [_P], "or_intensity_projection": [_P, _P], "or_frame_step_u16": [_P, _P, C.POINTER(_I)],
     "or_get_raycast": [_P, _P, _P], "or_set_raycast": [_P, _P, _P],
     "or_get_vertex_map": [_P, _I, _P], "or_get_normal_map": [_P, _I, _P],
     "or_set_vertex_normal_map": [_P, _I, _P, _P], "or_get_depth_map": [_P, _I, _P],
@@ -155,6 +155,12 @@ class Oracle:
 
     def raycast(self):
         _ok(self.lib.or_raycast(self._h), "raycast")
+
+    def intensityProjection(self):
+        w, h = self._wh(0)
+        m = np.empty((h, w, 4))
+        _ok(self.lib.or_intensity_projection(self._h, m.ctypes.data), "intensity_projection")
+        return m
 
     def frameStep(self, depth_u16) -> bool:
         d = np.ascontiguousarray(depth_u16, np.uint16)

@@ -232,6 +232,55 @@ def test_raycast_plane_hit_depth():
     assert np.mean(nz < 1e-6) > 0.97 and nz.max() < 2e-3
 
 
+# ---- intensityProjection (mip.cs) -----------------------------------------------------
+def _mip_sample_counts(c, pose, ls):
+    """Samples tnear + k * ls < tfar per pixel, from the slab test of mip.cs:61-77."""
+    fx, fy, cx, cy = INTR.fx, INTR.fy, INTR.cx, INTR.cy
+    ys, xs = np.mgrid[0:INTR.height, 0:INTR.width].astype(np.float64)
+    d_cam = np.stack([(xs - cx) / fx, (ys - cy) / fy, np.ones_like(xs)], -1)
+    d = d_cam @ pose[:3, :3].T
+    o = pose[:3, 3]
+    dim = np.array(c.volumeDimensions, np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = 1.0 / d
+        tb = -inv * o
+        tt = inv * (dim - o)
+    tmin, tmax = np.minimum(tt, tb), np.maximum(tt, tb)
+    tnear = np.maximum(tmin.max(-1), c.nearPlane)
+    tfar = np.minimum(tmax.min(-1), c.farPlane)
+    r = (tfar - tnear) / ls
+    n = np.where(tnear < tfar, np.ceil(r), 0)
+    # where the ratio sits on an integer, rounding decides whether the last sample is in
+    on_step = (tnear < tfar) & (np.abs(r - np.rint(r)) < 1e-9)
+    return n, on_step
+
+
+@pytest.mark.parametrize("value", [0.5, -0.25])
+def test_intensity_projection_constant_volume(value):
+    """A constant TSDF c makes every trilinear sample c, so each pixel's sum is c times
+    its sample count when c > 0 and 0 otherwise; y = z = 0 and w = 1 everywhere."""
+    c = cfg(size=32, dim=1.0, mu=0.05)
+    o = O.Oracle(c, INTR)
+    pose = np.eye(4)
+    pose[:3, 3] = [0.5, 0.5, -0.2]
+    o.Reset(pose)
+    n = 32 ** 3
+    raw = np.concatenate([np.full(n, value, np.float32), np.ones(n, np.float32)])
+    o.setVolumeRaw(raw.view(np.uint8))
+    m = o.intensityProjection()
+    counts, on_step = _mip_sample_counts(c, pose, 0.75 * c.mu)
+    assert (counts > 0).mean() > 0.3 and on_step.mean() < 0.01
+    want = counts * value if value > 0 else np.zeros_like(counts)
+    err = np.abs(m[..., 0] - want)
+    assert np.all(err[~on_step] <= 1e-9 * np.maximum(1.0, np.abs(want[~on_step])))
+    assert np.all(err[on_step] <= abs(value) + 1e-9)
+    assert np.all(m[..., 1] == 0) and np.all(m[..., 2] == 0) and np.all(m[..., 3] == 1)
+    # the central ray enters at z = 0 (t = 0.2) and leaves at z = 1 (t = 1.2)
+    if value > 0:
+        cy, cx = int(INTR.cy), int(INTR.cx)
+        assert counts[cy, cx] == np.ceil(1.0 / (0.75 * c.mu))
+
+
 # ---- ICP (track.cs / reduce.cs / Track) ---------------------------------------------
 def test_icp_recovers_small_motion_on_same_frame():
     from oglfusionkinectv2_b200 import synth
