@@ -179,6 +179,29 @@ KF_API int kf_depth_to_vertex_u16(kf_session* s, const uint16_t* host_depth_mm);
 KF_API int kf_depth_to_vertex_u16_device(kf_session* s, const uint16_t* device_depth_mm);
 KF_API int kf_vertex_to_normal(kf_session* s); /* vertexToNormal, gFusion.cpp:528-547 */
 
+/* ---- depth ingest stages before the pyramid (both off by default) --------------------
+ * IR (depth) camera of the Kinect v2 as libfreenect2 describes it
+ * (Freenect2Device::IrCameraParams), set by the reference from its calibration file
+ * (src/interface.cpp:239-272, src/kinect.cpp:82-160). */
+typedef struct kf_ir_camera {
+  float fx, fy, cx, cy;
+  float k1, k2, k3; /* radial distortion */
+  float p1, p2;     /* tangential distortion */
+} kf_ir_camera;
+/* Undistort every frame before the pyramid, as libfreenect2's Registration::apply makes
+ * the `undistorted` depth the reference fuses (src/interface.cpp:290-313; libfreenect2
+ * fork at commit 0ee1ee2f): each pixel takes the raw depth at its distorted position
+ * (Brown-Conrady model in float, rounded as (int)(m + 0.5f)), 0 where that falls outside
+ * the image.  NULL turns it off.  Applies to every kf_depth_to_vertex_* and frame step of
+ * this session (not to batched steps, which refuse such sessions). */
+KF_API int kf_set_depth_undistortion(kf_session* s, const kf_ir_camera* ir);
+/* The undistortion map: W*H source pixel indices, -1 where unmapped (KF_ERR_STATE if off). */
+KF_API int kf_get_undistortion_map(kf_session* s, int32_t* map);
+/* shaders/filter3D.cs (shipped by the reference, never dispatched): an interior pixel keeps
+ * its depth when more than 6 of its 3x3 neighbours are in (5, 4000) mm and it is within
+ * 5 mm of their mean, else 0; border pixels become 0.  Runs after the undistortion. */
+KF_API int kf_set_depth_filter(kf_session* s, int enable);
+
 /* ---- tracking ------------------------------------------------------------------------ */
 /* Track() (gFusion.cpp:648-740): coarse-to-fine projective point-to-plane ICP with the
  * 27-term reduction, an on-device FP64 solve and pose update.  *tracked may be NULL (then

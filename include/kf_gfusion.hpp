@@ -74,6 +74,11 @@ class GFusion {
   }
   void depthToVertex(const uint16_t* depthMm) { check(kf_depth_to_vertex_u16(s_, depthMm), "kf_depth_to_vertex_u16"); }
   void vertexToNormal() { check(kf_vertex_to_normal(s_), "kf_vertex_to_normal"); }
+  // depth ingest before the pyramid: libfreenect2-style undistortion, filter3D.cs
+  void setDepthUndistortion(const kf_ir_camera* ir) {
+    check(kf_set_depth_undistortion(s_, ir), "kf_set_depth_undistortion");
+  }
+  void setDepthFilter(bool enable) { check(kf_set_depth_filter(s_, enable ? 1 : 0), "kf_set_depth_filter"); }
   bool Track() {
     int t = 0;
     check(kf_track_icp(s_, &t), "kf_track_icp");

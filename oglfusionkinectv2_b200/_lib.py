@@ -75,6 +75,10 @@ class kf_volume_view(C.Structure):
                 ("slice_pitch_bytes", C.c_int64)]
 
 
+class kf_ir_camera(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("fx", "fy", "cx", "cy", "k1", "k2", "k3", "p1", "p2")]
+
+
 class KfError(RuntimeError):
     def __init__(self, status: int, what: str):
         super().__init__(f"{what}: {status_string(status)} ({status})")
@@ -126,6 +130,9 @@ SIGNATURES = {
     "kf_copy_volume_from_host": (_I, [_P, _P, C.c_uint64]),
     "kf_get_cum_twist": (_I, [_P, _PD]),
     "kf_intensity_projection": (_I, [_P, _P]),
+    "kf_set_depth_undistortion": (_I, [_P, C.POINTER(kf_ir_camera)]),
+    "kf_get_undistortion_map": (_I, [_P, _P]),
+    "kf_set_depth_filter": (_I, [_P, _I]),
     "kf_save_volume": (_I, [_P, C.c_char_p]),
     "kf_load_volume": (_I, [_P, C.c_char_p]),
     "kf_selftest_barrier_timeout": (_I, [_P, C.c_longlong]),

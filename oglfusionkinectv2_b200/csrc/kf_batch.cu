@@ -52,6 +52,8 @@ int check_members(kf_batch* b, kf_session* const* ss, int n) {
     if (s->cfg.storage != s0->cfg.storage || s->cfg.jtj != s0->cfg.jtj)
       return bfail(b, KF_ERR_INVALID_ARGUMENT, "sessions of one batch step need the same storage and J^T J form");
     if (s->cfg.tracking != KF_TRACK_ICP) return bfail(b, KF_ERR_INVALID_ARGUMENT, "batched frame steps track by ICP");
+    if (s->undistort || s->depth_filter)
+      return bfail(b, KF_ERR_INVALID_ARGUMENT, "batched frame steps read raw depth (undistortion and filter off)");
     for (int f = 0; f < e; ++f)
       if (ss[f] == s) return bfail(b, KF_ERR_INVALID_ARGUMENT, "a session appears twice in one batch step");
   }

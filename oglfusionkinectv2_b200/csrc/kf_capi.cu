@@ -109,6 +109,8 @@ void free_all(kf_session* s) {
   cudaFree(s->d_state);
   cudaFree(s->d_u32_scalar);
   cudaFree(s->d_mip);
+  cudaFree(s->d_undistort_map);
+  cudaFree(s->d_depth_prep);
   if (s->h_state) cudaFreeHost(s->h_state);
   if (s->h_depth_pinned) cudaFreeHost(s->h_depth_pinned);
   if (s->h_u32_scalar) cudaFreeHost(s->h_u32_scalar);
@@ -209,7 +211,7 @@ int record(kf_session* s, int i) {
 int enqueue_frame(kf_session* s, cudaEvent_t* ev) {
   int rc;
   KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[0], s->stream, cudaEventRecordExternal));
-  if ((rc = kf_launch_pyramid(s, s->d_depth_u16, nullptr))) return rc;
+  if ((rc = kf_launch_depth_ingest(s, s->d_depth_u16, nullptr))) return rc;
   if ((rc = kf_launch_vertex_normal(s))) return rc;
   KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[1], s->stream, cudaEventRecordExternal));
   if (s->cfg.tracking == KF_TRACK_SDF) {
@@ -580,7 +582,7 @@ int kf_depth_to_vertex_f32(kf_session* s, const float* host_depth_mm) {
   if (!s || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
   const size_t px = (size_t)s->W[0] * s->H[0];
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_f32_in, host_depth_mm, px * 4, cudaMemcpyHostToDevice, s->stream));
-  int rc = kf_launch_pyramid(s, nullptr, s->d_depth_f32_in);
+  int rc = kf_launch_depth_ingest(s, nullptr, s->d_depth_f32_in);
   if (rc) return rc;
   return kf_launch_vertex(s);
 }
@@ -589,14 +591,14 @@ int kf_depth_to_vertex_u16(kf_session* s, const uint16_t* host_depth_mm) {
   if (!s || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
   const size_t px = (size_t)s->W[0] * s->H[0];
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->stream));
-  int rc = kf_launch_pyramid(s, s->d_depth_u16, nullptr);
+  int rc = kf_launch_depth_ingest(s, s->d_depth_u16, nullptr);
   if (rc) return rc;
   return kf_launch_vertex(s);
 }
 
 int kf_depth_to_vertex_u16_device(kf_session* s, const uint16_t* device_depth_mm) {
   if (!s || !device_depth_mm) return KF_ERR_INVALID_ARGUMENT;
-  int rc = kf_launch_pyramid(s, device_depth_mm, nullptr);
+  int rc = kf_launch_depth_ingest(s, device_depth_mm, nullptr);
   if (rc) return rc;
   return kf_launch_vertex(s);
 }
@@ -936,6 +938,56 @@ int kf_load_volume(kf_session* s, const char* path) {
   if ((rc = kf_rebuild_bricks(s, s->stream))) return rc;
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return KF_OK;
+}
+
+// ---- depth ingest: Kinect-v2 undistortion and filter3D.cs -----------------------------------
+namespace {
+int ensure_depth_prep(kf_session* s) {
+  if (s->d_depth_prep) return KF_OK;
+  return dalloc(s, &s->d_depth_prep, (size_t)s->W[0] * s->H[0]);
+}
+}  // namespace
+
+int kf_set_depth_undistortion(kf_session* s, const kf_ir_camera* ir) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  if (ir) {
+    const float v[9] = {ir->fx, ir->fy, ir->cx, ir->cy, ir->k1, ir->k2, ir->k3, ir->p1, ir->p2};
+    for (float f : v)
+      if (!std::isfinite(f)) return KF_ERR_INVALID_ARGUMENT;
+    if (!(ir->fx > 0) || !(ir->fy > 0)) return KF_ERR_INVALID_ARGUMENT;
+  }
+  // the captured frame graphs hold the old ingest
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  drop_graph(s);
+  if (!ir) {
+    s->undistort = 0;
+    return KF_OK;
+  }
+  int rc = ensure_depth_prep(s);
+  if (rc) return rc;
+  if (!s->d_undistort_map && (rc = dalloc(s, &s->d_undistort_map, (size_t)s->W[0] * s->H[0]))) return rc;
+  if ((rc = kf_launch_undistort_map(s, *ir))) return rc;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  s->undistort = 1;
+  return KF_OK;
+}
+
+int kf_set_depth_filter(kf_session* s, int enable) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  drop_graph(s);
+  if (enable) {
+    int rc = ensure_depth_prep(s);
+    if (rc) return rc;
+  }
+  s->depth_filter = enable ? 1 : 0;
+  return KF_OK;
+}
+
+int kf_get_undistortion_map(kf_session* s, int32_t* map) {
+  if (!s || !map) return KF_ERR_INVALID_ARGUMENT;
+  if (!s->undistort) return fail(s, KF_ERR_STATE, "undistortion is off");
+  return copy_out(s, map, s->d_undistort_map, (size_t)s->W[0] * s->H[0] * sizeof(int32_t));
 }
 
 // ---- intensity projection (gFusion::intensityProjection, src/gFusion.cpp:1368-1409) ------

@@ -140,6 +140,13 @@ struct kf_session {
   uint32_t* h_u32_scalar = nullptr;  // pinned
 
   float4* d_mip = nullptr;  // intensity-projection image, allocated on first use
+
+  // depth ingest before the pyramid (off by default): Kinect-v2 undistortion through a
+  // source-index map, and the filter3D.cs validity filter; their output is d_depth_prep
+  int undistort = 0;
+  int depth_filter = 0;
+  int32_t* d_undistort_map = nullptr;
+  float* d_depth_prep = nullptr;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -626,6 +633,8 @@ inline void kf_note_launch(kf_session* s, int n = 1) {
 // ---------------------------------------------------------------------------------------
 // launchers (one per .cu file)
 int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32);
+int kf_launch_depth_ingest(kf_session* s, const uint16_t* d_u16, const float* d_f32);
+int kf_launch_undistort_map(kf_session* s, const kf_ir_camera& ir);
 int kf_launch_vertex(kf_session* s);
 int kf_launch_normal(kf_session* s);
 int kf_launch_vertex_normal(kf_session* s);

@@ -164,7 +164,129 @@ PyrArgs make_pyr_args(kf_session* s, const uint16_t* d_u16, const float* d_f32) 
   return a;
 }
 
+// ---- depth ingest before the pyramid ----------------------------------------------------
+// Kinect-v2 undistortion: the reference fuses libfreenect2's `undistorted` frame
+// (src/interface.cpp:290-313, Registration::apply, libfreenect2 fork at commit 0ee1ee2f).
+// Registration maps every undistorted pixel to a raw pixel through the IR camera's
+// Brown-Conrady model, evaluated in float, rounds with (int)(m + 0.5f) and marks sources
+// outside the image; apply() copies the raw depth through that map (0 where unmapped).
+// The map is built once on the device with every operation explicitly rounded (no fused
+// multiply-adds), in the expression order of libfreenect2's distort().
+__global__ void __launch_bounds__(256) undistort_map_kernel(kf_ir_camera ir, int W, int H, int32_t* map) {
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const float dx = __fdiv_rn(__fsub_rn((float)x, ir.cx), ir.fx);
+  const float dy = __fdiv_rn(__fsub_rn((float)y, ir.cy), ir.fy);
+  const float dx2 = __fmul_rn(dx, dx), dy2 = __fmul_rn(dy, dy);
+  const float r2 = __fadd_rn(dx2, dy2);
+  const float dxdy2 = __fmul_rn(__fmul_rn(2.0f, dx), dy);
+  const float kr = __fadd_rn(1.0f, __fmul_rn(__fadd_rn(__fmul_rn(__fadd_rn(__fmul_rn(ir.k3, r2), ir.k2), r2), ir.k1), r2));
+  const float mx = __fadd_rn(
+      __fmul_rn(ir.fx, __fadd_rn(__fadd_rn(__fmul_rn(dx, kr), __fmul_rn(ir.p2, __fadd_rn(r2, __fmul_rn(2.0f, dx2)))),
+                                 __fmul_rn(ir.p1, dxdy2))),
+      ir.cx);
+  const float my = __fadd_rn(
+      __fmul_rn(ir.fy, __fadd_rn(__fadd_rn(__fmul_rn(dy, kr), __fmul_rn(ir.p1, __fadd_rn(r2, __fmul_rn(2.0f, dy2)))),
+                                 __fmul_rn(ir.p2, dxdy2))),
+      ir.cy);
+  const float vx = __fadd_rn(mx, 0.5f), vy = __fadd_rn(my, 0.5f);
+  // (int) truncates towards zero: the source is inside the image iff v > -1 and v < size
+  int32_t idx = -1;
+  if (vx > -1.0f && vx < (float)W && vy > -1.0f && vy < (float)H) idx = __float2int_rz(vy) * W + __float2int_rz(vx);
+  map[(size_t)y * W + x] = idx;
+}
+
+struct PrepArgs {
+  const uint16_t* in_u16;
+  const float* in_f32;
+  const int32_t* map;  // undistortion map, or null
+  float* out;
+  int W, H;
+  int filter;          // filter3D.cs
+};
+
+// filter3D.cs checkPixel (:9-21): a depth is valid when 5 < d < 4000 (millimetres)
+__device__ __forceinline__ float check_pixel(float v) { return (v > 5.0f && v < 4000.0f) ? v : 0.0f; }
+
+__device__ __forceinline__ float prep_raw(const PrepArgs& a, int x, int y) {
+  if (x < 0 || y < 0 || x >= a.W || y >= a.H) return 0.0f;
+  int i = y * a.W + x;
+  if (a.map) {
+    i = __ldg(a.map + i);
+    if (i < 0) return 0.0f;
+  }
+  return a.in_u16 ? (float)__ldg(a.in_u16 + i) : __ldg(a.in_f32 + i);
+}
+
+// One 32x8 tile per block with a one-pixel halo in shared memory (each halo value is an
+// undistortion gather).  filter3D.cs:23-86: an interior pixel (1 < x < W-1, 1 < y < H-1)
+// keeps its depth when more than 6 of its 3x3 neighbourhood are valid and it is within
+// 5 mm of their mean, else 0; the neighbourhood is summed column by column, as the
+// shader's loops do.  The shader never writes border pixels; they are 0 here.
+__global__ void __launch_bounds__(256) depth_prepare_kernel(PrepArgs a) {
+  __shared__ float s_t[10][35];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int x0 = blockIdx.x * 32 - 1, y0 = blockIdx.y * 8 - 1;
+  for (int k = tid; k < 10 * 34; k += 256) {
+    const int ty = k / 34, tx = k - ty * 34;
+    const float v = prep_raw(a, x0 + tx, y0 + ty);
+    s_t[ty][tx] = a.filter ? check_pixel(v) : v;
+  }
+  __syncthreads();
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  if (x >= a.W || y >= a.H) return;
+  float o = s_t[threadIdx.y + 1][threadIdx.x + 1];
+  if (a.filter) {
+    float r = 0.0f;
+    if (x > 1 && x < a.W - 1 && y > 1 && y < a.H - 1) {
+      float valid = 9.0f, sum = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const float t = s_t[threadIdx.y + j][threadIdx.x + i];
+          if (t == 0.0f) valid = __fsub_rn(valid, 1.0f);
+          else sum = __fadd_rn(sum, t);
+        }
+      const float mean = valid > 6.0f ? __fdiv_rn(sum, valid) : 0.0f;
+      if (mean > 0.0f && fabsf(__fsub_rn(o, mean)) < 5.0f) r = o;
+    }
+    o = r;
+  }
+  a.out[(size_t)y * a.W + x] = o;
+}
+
 }  // namespace
+
+int kf_launch_undistort_map(kf_session* s, const kf_ir_camera& ir) {
+  dim3 block(32, 8);
+  dim3 grid((s->W[0] + 31) / 32, (s->H[0] + 7) / 8);
+  undistort_map_kernel<<<grid, block, 0, s->stream>>>(ir, s->W[0], s->H[0], s->d_undistort_map);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  kf_note_launch(s);
+  return KF_OK;
+}
+
+// The pyramid of one frame, through the session's ingest stages when they are on.
+int kf_launch_depth_ingest(kf_session* s, const uint16_t* d_u16, const float* d_f32) {
+  if (!s->undistort && !s->depth_filter) return kf_launch_pyramid(s, d_u16, d_f32);
+  PrepArgs a;
+  a.in_u16 = d_u16;
+  a.in_f32 = d_u16 ? nullptr : d_f32;
+  a.map = s->undistort ? s->d_undistort_map : nullptr;
+  a.out = s->d_depth_prep;
+  a.W = s->W[0];
+  a.H = s->H[0];
+  a.filter = s->depth_filter;
+  dim3 block(32, 8);
+  dim3 grid((a.W + 31) / 32, (a.H + 7) / 8);
+  depth_prepare_kernel<<<grid, block, 0, s->stream>>>(a);
+  KF_CUDA_TRY(s, cudaGetLastError());
+  kf_note_launch(s);
+  return kf_launch_pyramid(s, nullptr, s->d_depth_prep);
+}
 
 int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32) {
   const PyrArgs a = make_pyr_args(s, d_u16, d_f32);

@@ -264,6 +264,26 @@ class GFusion:
         self._check(self.lib.kf_copy_volume_from_host(self._h, raw.ctypes.data, raw.nbytes),
                     "kf_copy_volume_from_host")
 
+    # ---- depth ingest stages (the capture side of the reference) ---------------------------
+    def setDepthUndistortion(self, ir) -> None:
+        """Undistort each frame before the pyramid as libfreenect2's Registration does
+        (src/interface.cpp:290-313).  ir: (fx, fy, cx, cy, k1, k2, k3, p1, p2) of the IR
+        camera, or None to turn it off."""
+        if ir is None:
+            self._check(self.lib.kf_set_depth_undistortion(self._h, None), "kf_set_depth_undistortion")
+            return
+        c = L.kf_ir_camera(*[float(v) for v in ir])
+        self._check(self.lib.kf_set_depth_undistortion(self._h, C.byref(c)), "kf_set_depth_undistortion")
+
+    def getUndistortionMap(self) -> np.ndarray:
+        m = np.empty((self.intrinsics.height, self.intrinsics.width), np.int32)
+        self._check(self.lib.kf_get_undistortion_map(self._h, m.ctypes.data), "kf_get_undistortion_map")
+        return m
+
+    def setDepthFilter(self, enable: bool) -> None:
+        """shaders/filter3D.cs before the pyramid (after the undistortion)."""
+        self._check(self.lib.kf_set_depth_filter(self._h, int(bool(enable))), "kf_set_depth_filter")
+
     def intensityProjection(self) -> np.ndarray:
         """Volume ray-sum image at the current pose (gFusion::intensityProjection,
         src/gFusion.cpp:1368-1409), H x W x 4: (sum of positive samples, 0, 0, 1)."""

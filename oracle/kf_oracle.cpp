@@ -445,6 +445,10 @@ struct or_session {
   double ae = 0;
   int counter = 0;
   bool reset_window = true;
+  /* depth ingest before the pyramid (libfreenect2 undistortion, filter3D.cs) */
+  bool undistort = false;
+  bool depth_filter = false;
+  std::vector<int32_t> undistort_map;
   /* marching cubes */
   std::vector<uint32_t> mc_base;                /* nx*ny*nz, numTri | ci << 16 */
   std::vector<std::vector<uint32_t>> mc_levels; /* level k>=1, (P>>k)^3 */
@@ -474,6 +478,82 @@ void level_setup(or_session* s) {
   s->ref_vertex.assign(4 * n0, 0.0);
   s->ref_normal.assign(4 * n0, 0.0);
   s->sdf_rows.assign(8 * n0, 0.0);
+}
+
+/* ---- depth ingest: Kinect-v2 undistortion (libfreenect2) and filter3D.cs ------------------
+ * The reference feeds the fusion with libfreenect2's `undistorted` depth frame
+ * (src/interface.cpp:290-313, Registration::apply; the library is philipNoonan/libfreenect2
+ * at commit 0ee1ee2f8d2331253e78aaac0a340436b14ba34e, depends/libfreenect2-nm/portfile.cmake,
+ * not part of the reference tree).  Registration's published algorithm: for every
+ * undistorted pixel (x, y), distort() applies the IR camera's Brown-Conrady model (radial
+ * k1, k2, k3; tangential p1, p2) in float, the source pixel is (int)(m + 0.5f) on each axis,
+ * and pixels whose source falls outside the image get depth 0; apply() copies the raw depth
+ * through that map.  This restatement evaluates the same float expressions in the same order
+ * (no fused multiply-adds: the oracle is built for x86-64-v2, which has none). */
+#if defined(__FMA__)
+#error "the undistortion map is specified without fused multiply-adds; build for a target without FMA"
+#endif
+int32_t undistort_index(const float ir[9], int x, int y, int W, int H) {
+  const float fx = ir[0], fy = ir[1], cx = ir[2], cy = ir[3];
+  const float k1 = ir[4], k2 = ir[5], k3 = ir[6], p1 = ir[7], p2 = ir[8];
+  const float dx = ((float)x - cx) / fx;
+  const float dy = ((float)y - cy) / fy;
+  const float dx2 = dx * dx, dy2 = dy * dy;
+  const float r2 = dx2 + dy2;
+  const float dxdy2 = 2 * dx * dy;
+  const float kr = 1 + ((k3 * r2 + k2) * r2 + k1) * r2;
+  const float mx = fx * (dx * kr + p2 * (r2 + 2 * dx2) + p1 * dxdy2) + cx;
+  const float my = fy * (dy * kr + p1 * (r2 + 2 * dy2) + p2 * dxdy2) + cy;
+  const float vx = mx + 0.5f, vy = my + 0.5f;
+  /* (int) truncates towards zero: a source index is inside the image iff v > -1 and v < size */
+  if (!(vx > -1.0f && vx < (float)W && vy > -1.0f && vy < (float)H)) return -1;
+  return (int32_t)vy * W + (int32_t)vx;
+}
+
+/* filter3D.cs:23-86: a depth is valid when 5 < d < 4000 (checkPixel); an interior pixel
+ * (1 < x < W-1, 1 < y < H-1) keeps its depth when more than 6 of its 3x3 neighbourhood are
+ * valid and it lies within 5 mm of their mean, else 0.  Float arithmetic, neighbourhood
+ * summed column by column (the shader's i (x) outer, j (y) inner loops).  The shader never
+ * writes the border pixels (its dispatch offset pix.y += 2 only moves rows inside that
+ * rule); they are 0 here. */
+inline float check_pixel(float v) { return (v > 5.0f && v < 4000.0f) ? v : 0.0f; }
+
+void filter3d(const float* in, float* out, int W, int H) {
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      float o = 0.0f;
+      if (x > 1 && x < W - 1 && y > 1 && y < H - 1) {
+        float valid = 9.0f, sum = 0.0f, curr = 0.0f;
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            const float t = check_pixel(in[(size_t)(y + j - 1) * W + (x + i - 1)]);
+            if (t == 0.0f) valid -= 1.0f;
+            else sum += t;
+            if (i == 1 && j == 1) curr = t;
+          }
+        const float mean = valid > 6.0f ? sum / valid : 0.0f;
+        if (mean > 0.0f && std::fabs(curr - mean) < 5.0f) o = curr;
+      }
+      out[(size_t)y * W + x] = o;
+    }
+}
+
+/* The level-0 depth the pyramid is built from: raw input, undistorted, then filtered. */
+void prepare_depth(or_session* s, const float* raw) {
+  Level& L = s->lv[0];
+  const int W = L.w, H = L.h;
+  const size_t n = (size_t)W * H;
+  std::vector<float> a(raw, raw + n), b(n);
+  if (s->undistort) {
+    for (size_t i = 0; i < n; ++i) b[i] = s->undistort_map[i] < 0 ? 0.0f : a[(size_t)s->undistort_map[i]];
+    a.swap(b);
+  }
+  if (s->depth_filter) {
+    filter3d(a.data(), b.data(), W, H);
+    a.swap(b);
+  }
+  for (size_t i = 0; i < n; ++i) L.depth[i] = a[i];
 }
 
 /* ---- depthToVertex: mip + depthToVert.cs:33-72 ---------------------------------------- */
@@ -1317,16 +1397,42 @@ int or_get_pose_eig(or_session* s, double pose[16]) { std::memcpy(pose, s->pose_
 int or_set_pose_eig(or_session* s, const double pose[16]) { std::memcpy(s->pose_eig, pose, 128); return KF_OK; }
 
 int or_depth_to_vertex_f32(or_session* s, const float* depth_mm) {
-  Level& L = s->lv[0];
-  for (size_t i = 0; i < L.depth.size(); ++i) L.depth[i] = depth_mm[i];
+  prepare_depth(s, depth_mm);
   depth_to_vertex(s);
   return KF_OK;
 }
 
 int or_depth_to_vertex_u16(or_session* s, const uint16_t* depth_mm) {
-  Level& L = s->lv[0];
-  for (size_t i = 0; i < L.depth.size(); ++i) L.depth[i] = depth_mm[i];
+  std::vector<float> f(s->lv[0].depth.size());
+  for (size_t i = 0; i < f.size(); ++i) f[i] = depth_mm[i];
+  prepare_depth(s, f.data());
   depth_to_vertex(s);
+  return KF_OK;
+}
+
+int or_set_depth_undistortion(or_session* s, const float ir[9]) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  if (!ir) {
+    s->undistort = false;
+    return KF_OK;
+  }
+  const int W = s->lv[0].w, H = s->lv[0].h;
+  s->undistort_map.assign((size_t)W * H, -1);
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) s->undistort_map[(size_t)y * W + x] = undistort_index(ir, x, y, W, H);
+  s->undistort = true;
+  return KF_OK;
+}
+
+int or_set_depth_filter(or_session* s, int enable) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  s->depth_filter = enable != 0;
+  return KF_OK;
+}
+
+int or_get_undistortion_map(or_session* s, int32_t* map) {
+  if (!s || !map || !s->undistort) return KF_ERR_INVALID_ARGUMENT;
+  std::memcpy(map, s->undistort_map.data(), s->undistort_map.size() * sizeof(int32_t));
   return KF_OK;
 }
 

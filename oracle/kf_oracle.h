@@ -43,6 +43,11 @@ int or_set_pose_eig(or_session* s, const double pose[16]);
 int or_depth_to_vertex_f32(or_session* s, const float* depth_mm);
 int or_depth_to_vertex_u16(or_session* s, const uint16_t* depth_mm);
 int or_vertex_to_normal(or_session* s);
+/* Depth ingest before the pyramid: libfreenect2 Registration undistortion with the IR
+ * camera (fx, fy, cx, cy, k1, k2, k3, p1, p2; NULL turns it off) and filter3D.cs. */
+int or_set_depth_undistortion(or_session* s, const float ir[9]);
+int or_set_depth_filter(or_session* s, int enable);
+int or_get_undistortion_map(or_session* s, int32_t* map);
 
 int or_track_icp(or_session* s, int* tracked);
 int or_track_sdf(or_session* s, int* tracked);

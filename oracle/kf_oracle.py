@@ -24,7 +24,8 @@ _SIG = {
     "or_set_pose": [_P, _PD], "or_get_pose": [_P, _PD], "or_get_pose_eig": [_P, _PD],
     "or_set_pose_eig": [_P, _PD],
     "or_depth_to_vertex_f32": [_P, _P], "or_depth_to_vertex_u16": [_P, _P],
-    "or_vertex_to_normal": [_P], "or_track_icp": [_P, C.POINTER(_I)],
+    "or_vertex_to_normal": [_P], "or_set_depth_undistortion": [_P, _P],
+    "or_set_depth_filter": [_P, _I], "or_get_undistortion_map": [_P, _P], "or_track_icp": [_P, C.POINTER(_I)],
     "or_track_sdf": [_P, C.POINTER(_I)], "or_recover_pose": [_P, C.POINTER(_I)],
     "or_get_alignment_energy": [_P, _PD], "or_get_reduction": [_P, _PD],
     "or_icp_reduce_once": [_P, _I, _PD], "or_sdf_reduce_once": [_P, _I, _PD, _PD],
@@ -134,6 +135,23 @@ class Oracle:
 
     def vertexToNormal(self):
         _ok(self.lib.or_vertex_to_normal(self._h), "v2n")
+
+    def setDepthUndistortion(self, ir):
+        """ir: (fx, fy, cx, cy, k1, k2, k3, p1, p2) of the IR camera, or None (off)."""
+        if ir is None:
+            _ok(self.lib.or_set_depth_undistortion(self._h, None), "undistortion")
+            return
+        a = (C.c_float * 9)(*[float(v) for v in ir])
+        _ok(self.lib.or_set_depth_undistortion(self._h, a), "undistortion")
+
+    def setDepthFilter(self, enable):
+        _ok(self.lib.or_set_depth_filter(self._h, int(bool(enable))), "depth_filter")
+
+    def getUndistortionMap(self):
+        w, h = self._wh(0)
+        m = np.empty((h, w), np.int32)
+        _ok(self.lib.or_get_undistortion_map(self._h, m.ctypes.data), "undistortion_map")
+        return m
 
     def Track(self) -> bool:
         t = C.c_int()

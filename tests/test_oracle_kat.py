@@ -232,6 +232,78 @@ def test_raycast_plane_hit_depth():
     assert np.mean(nz < 1e-6) > 0.97 and nz.max() < 2e-3
 
 
+# ---- depth ingest: libfreenect2 undistortion and filter3D.cs ----------------------------
+IR = (365.1, 364.7, 255.3, 208.9, 0.092, -0.27, 0.094, 0.0012, -0.0006)
+
+
+def _undistort_map_float32(ir, W, H):
+    """libfreenect2 Registration's map in numpy float32 (IEEE single, no fused multiply-add),
+    the same expressions in the same order."""
+    f = np.float32
+    fx, fy, cx, cy, k1, k2, k3, p1, p2 = [f(v) for v in ir]
+    ys, xs = np.mgrid[0:H, 0:W]
+    dx = (xs.astype(f) - cx) / fx
+    dy = (ys.astype(f) - cy) / fy
+    dx2, dy2 = dx * dx, dy * dy
+    r2 = dx2 + dy2
+    dxdy2 = f(2) * dx * dy
+    kr = f(1) + ((k3 * r2 + k2) * r2 + k1) * r2
+    mx = fx * (dx * kr + p2 * (r2 + f(2) * dx2) + p1 * dxdy2) + cx
+    my = fy * (dy * kr + p1 * (r2 + f(2) * dy2) + p2 * dxdy2) + cy
+    vx, vy = mx + f(0.5), my + f(0.5)
+    ok = (vx > -1) & (vx < W) & (vy > -1) & (vy < H)
+    idx = np.trunc(vy).astype(np.int64) * W + np.trunc(vx).astype(np.int64)
+    return np.where(ok, idx, -1).astype(np.int32)
+
+
+@pytest.mark.parametrize("ir", [IR, (365.0, 365.0, 256.0, 212.0, 0, 0, 0, 0, 0),
+                                (360.0, 361.0, 250.0, 205.0, 0.6, -2.0, 4.0, 0.02, -0.03)])
+def test_undistortion_map_matches_float32_model(ir):
+    o = O.Oracle(cfg(size=16), INTR)
+    o.setDepthUndistortion(ir)
+    m = o.getUndistortionMap()
+    np.testing.assert_array_equal(m, _undistort_map_float32(ir, INTR.width, INTR.height))
+    if ir[4:] == (0, 0, 0, 0, 0) and ir[:4] == (INTR.fx, INTR.fy, INTR.cx, INTR.cy):
+        np.testing.assert_array_equal(m.ravel(), np.arange(m.size))  # no distortion: identity
+    assert (m >= 0).mean() > 0.5
+
+
+def test_undistortion_gathers_raw_depth():
+    o = O.Oracle(cfg(size=16), INTR)
+    raw = (np.arange(INTR.width * INTR.height) % 3000 + 500).astype(np.uint16).reshape(INTR.height, INTR.width)
+    o.setDepthUndistortion(IR)
+    o.depthToVertex(raw)
+    m = o.getUndistortionMap()
+    want = np.where(m >= 0, raw.ravel()[np.maximum(m, 0)], 0).reshape(raw.shape)
+    np.testing.assert_array_equal(o.getDepthImage(0), want)
+    o.setDepthUndistortion(None)
+    o.depthToVertex(raw)
+    np.testing.assert_array_equal(o.getDepthImage(0), raw)
+
+
+def test_filter3d_known_answers():
+    o = O.Oracle(cfg(size=16), INTR)
+    o.setDepthFilter(True)
+    H, W = INTR.height, INTR.width
+    d = np.full((H, W), 1000, np.uint16)
+    d[100, 100] = 1010          # 8.9 mm above its neighbourhood mean (1001.1): removed
+    d[200, 200] = 1004          # 3.6 mm above its neighbourhood mean (1000.4): kept
+    d[300, 301:304] = 0         # a run of three invalid depths
+    d[50, 50] = 4000            # out of range (checkPixel keeps 5 < d < 4000): invalid
+    o.depthToVertex(d)
+    f = o.getDepthImage(0)
+    # borders (x < 2, x > W-2, y < 2, y > H-2) are never written
+    assert np.all(f[:2] == 0) and np.all(f[-1] == 0) and np.all(f[:, :2] == 0) and np.all(f[:, -1] == 0)
+    assert f[2, 2] == 1000 and f[H - 2, W - 2] == 1000
+    assert f[100, 100] == 0 and f[100, 101] == 1000
+    assert f[200, 200] == 1004
+    assert f[299, 302] == 0      # its 3x3 holds all three zeros: 6 valid, not more than 6
+    assert f[301, 302] == 0      # the same three zeros
+    assert f[299, 301] == 1000   # two of them: 7 valid, kept
+    assert f[300, 301] == 0      # an invalid depth itself is never kept
+    assert f[50, 50] == 0 and f[50, 51] == 1000
+
+
 # ---- intensityProjection (mip.cs) -----------------------------------------------------
 def _mip_sample_counts(c, pose, ls):
     """Samples tnear + k * ls < tfar per pixel, from the slab test of mip.cs:61-77."""
