@@ -38,6 +38,8 @@ def parse():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default launch shapes instead of autotuning them during warm-up")
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--size", type=int, default=512)
     p.add_argument("--storage", choices=["f16u16", "f32f32", "rg16i"], default="f16u16")
@@ -226,7 +228,13 @@ def run_batched(args):
     batch = GFusionBatch(len(gs))
     ptr = lambda i: [f.data_ptr() + i * fbytes for f in frames]
     est = [[] for _ in gs]
+    tuned = None
     for i in range(W):
+        if i == W - 1 and not args.no_autotune:
+            # brick and tile shapes for this mix (scratch copies; the sessions are untouched);
+            # one more untimed step rebuilds the batch tables with them
+            shape, tms = batch.autotune(gs, repeats=3)
+            tuned = {"integrate_z_chunk": shape[0], "raycast_rows": shape[1], "candidates_ms": tms}
         batch.frameStepDevice(gs, ptr(i))
         for j, P in enumerate(batch.poses(len(gs))):
             est[j].append(P)
@@ -285,7 +293,8 @@ def run_batched(args):
             "config": {"workload": "c3_batched", "sessions": len(gs),
                        "sizes": {str(z): sizes.count(z) for z in sorted(set(sizes))},
                        "storage": "f16u16", "jtj": "bf16", "depth": "512x424 uint16 (device-resident)",
-                       "l2": "volumes 0.5 GB-5 GB total > L2"},
+                       "l2": "volumes 0.5 GB-5 GB total > L2",
+                       "launch_shape": tuned or {"integrate_z_chunk": 16, "raycast_rows": 4, "autotune": "off"}},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "stage_ms_per_step": dict(zip(["pyramid", "track", "integrate", "recover", "raycast"],
                                           (stage / K).tolist())),
@@ -554,7 +563,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    K, W = args.steps, max(3, args.warmup)
+    # after the autotuner (at the first warm-up frame) four frames capture the ring of frame
+    # graphs, so at least five warm-up frames
+    K, W = args.steps, max(3 if args.no_autotune else 5, args.warmup)
     n_e2e = 0 if args.no_e2e else K
     n_frames = W + K + n_e2e + 1
     w = workload(args, n_frames)
@@ -590,8 +601,14 @@ def main():
             mc_ms.append(float(g.getTimes()[5]))  # device time of the extraction (CUDA events)
             mc_calls += 1
 
+    tuned = None
     for i in range(W):
         g.frameStepDevice(base + i * fbytes, sync=False)
+        if i == 0 and not args.no_autotune:
+            # brick and tile shapes for this volume and frame (scratch copies; the session is
+            # untouched); the following warm-up frames capture the frame graphs with them
+            shape, tms = g.autotune(repeats=5)
+            tuned = {"integrate_z_chunk": shape[0], "raycast_rows": shape[1], "candidates_ms": tms}
     if w.mc_every:
         mc.generateMarchingCubes(L.KF_MC_HISTOPYRAMID)  # first extraction allocates its buffers
     torch.cuda.synchronize()
@@ -661,7 +678,8 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**plain_config(w, args, world),
                        "l2": "volume > L2 (126 MB); inputs resident",
-                       "mc_calls": mc_calls, "mc_ms_mean": (float(np.mean(mc_ms)) if mc_ms else None)},
+                       "mc_calls": mc_calls, "mc_ms_mean": (float(np.mean(mc_ms)) if mc_ms else None),
+                       "launch_shape": tuned or {"integrate_z_chunk": 16, "raycast_rows": 4, "autotune": "off"}},
             "stage_ms": per, "stage_frames": stage_frames,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak if achieved else None),

@@ -271,6 +271,25 @@ KF_API int kf_reset_stage_stats(kf_session* s);
 KF_API int kf_get_launch_count(kf_session* s, uint64_t* launches);
 KF_API int kf_get_stream(kf_session* s, void** cuda_stream);
 
+/* ---- launch shapes and the autotuner (no counterpart in the reference, whose shaders
+ * fix their work-group sizes, e.g. integrate.cs local_size 32x32, raycast.cs 32x32) -----
+ * Every shape computes bit-identical results; only the time differs. */
+typedef struct kf_launch_shape {
+  int32_t integrate_z_chunk; /* voxels per thread along z: 8, 16 (default) or 32 */
+  int32_t raycast_rows;      /* raycast tile of 32 x rows pixels: 2, 4 (default) or 8 */
+  int32_t reserved[6];
+} kf_launch_shape;
+KF_API int kf_set_launch_shape(kf_session* s, const kf_launch_shape* shape);
+KF_API int kf_get_launch_shape(kf_session* s, kf_launch_shape* shape);
+/* Times every integrate z-chunk and raycast tile shape on the session's current depth
+ * frame, pose and volume (repeats launches each, twice over, into scratch copies: the
+ * session's volume, maps and pose are untouched; needs one more volume's worth of device
+ * memory meanwhile), then uses the fastest.  times_ms (optional, 6 floats) receives the
+ * mean time of integrate with z-chunk 8, 16, 32 and raycast with rows 2, 4, 8.  Sessions
+ * created later with the same device, volume size, storage and image size start with the
+ * shape chosen here. */
+KF_API int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* times_ms);
+
 /* ---- batched frame steps (the batched and served forms; no counterpart in the reference,
  * whose app runs one session) -----------------------------------------------------------
  * A batch steps several sessions' frames together, one launch per stage for all of them
@@ -298,6 +317,15 @@ KF_API int kf_batch_get_poses(kf_batch* b, int n, double* poses16);
 /* Device ms of the last step's stages: pyramid, track, integrate, recover, raycast. */
 KF_API int kf_batch_get_stage_times(kf_batch* b, float* ms5);
 KF_API int kf_batch_get_launch_count(kf_batch* b, uint64_t* launches);
+/* Launch shapes of the batched integrate and raycast (one shape per batch launch). */
+KF_API int kf_batch_set_launch_shape(kf_batch* b, const kf_launch_shape* shape);
+KF_API int kf_batch_get_launch_shape(kf_batch* b, kf_launch_shape* shape);
+/* kf_autotune for the batched launches over these sessions (the mix of one step): each
+ * candidate shape times one batched integrate and raycast over all of them, into scratch
+ * copies (one more copy of every member's volume meanwhile); the batch then uses the
+ * fastest.  times_ms as for kf_autotune. */
+KF_API int kf_batch_autotune(kf_batch* b, kf_session* const* sessions, int n, int repeats,
+                             kf_launch_shape* chosen, float* times_ms);
 
 /* ---- served form (no counterpart in the reference) --------------------------------------
  * A request loop over resident sessions: kf_server_open admits a session while a slot and

@@ -75,6 +75,10 @@ class kf_volume_view(C.Structure):
                 ("slice_pitch_bytes", C.c_int64)]
 
 
+class kf_launch_shape(C.Structure):
+    _fields_ = [("integrate_z_chunk", C.c_int32), ("raycast_rows", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
 class kf_ir_camera(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("fx", "fy", "cx", "cy", "k1", "k2", "k3", "p1", "p2")]
 
@@ -133,6 +137,12 @@ SIGNATURES = {
     "kf_set_depth_undistortion": (_I, [_P, C.POINTER(kf_ir_camera)]),
     "kf_get_undistortion_map": (_I, [_P, _P]),
     "kf_set_depth_filter": (_I, [_P, _I]),
+    "kf_set_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
+    "kf_get_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
+    "kf_autotune": (_I, [_P, _I, C.POINTER(kf_launch_shape), _PF]),
+    "kf_batch_set_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
+    "kf_batch_get_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
+    "kf_batch_autotune": (_I, [_P, _P, _I, _I, C.POINTER(kf_launch_shape), _PF]),
     "kf_save_volume": (_I, [_P, C.c_char_p]),
     "kf_load_volume": (_I, [_P, C.c_char_p]),
     "kf_selftest_barrier_timeout": (_I, [_P, C.c_longlong]),

@@ -77,8 +77,9 @@ int rebuild_tables(kf_batch* b, kf_session* const* ss, int n) {
   if (!b->states) return bfail(b, KF_ERR_CAPACITY, "batch table full");
   for (int e = 0; e < n; ++e) hs[e] = ss[e]->d_state;
   int rc;
-  if ((rc = kf_batch_prepare_pyramid(b)) || (rc = kf_batch_prepare_icp(b)) || (rc = kf_batch_prepare_integrate(b)) ||
-      (rc = kf_batch_prepare_sdf(b)) || (rc = kf_batch_prepare_raycast(b))) {
+  if ((rc = kf_batch_prepare_pyramid(b)) || (rc = kf_batch_prepare_icp(b)) ||
+      (rc = kf_batch_prepare_integrate(b, nullptr)) || (rc = kf_batch_prepare_sdf(b)) ||
+      (rc = kf_batch_prepare_raycast(b, nullptr))) {
     b->members.clear();
     b->member_keys.clear();
     return bfail(b, rc, "batch tables: too many sessions for the table or the co-resident grid");
@@ -248,6 +249,107 @@ int kf_batch_get_poses(kf_batch* b, int n, double* poses) {
 int kf_batch_get_launch_count(kf_batch* b, uint64_t* n) {
   if (!b || !n) return KF_ERR_INVALID_ARGUMENT;
   *n = b->launches;
+  return KF_OK;
+}
+
+int kf_batch_set_launch_shape(kf_batch* b, const kf_launch_shape* shape) {
+  if (!b || !shape || !kf_valid_int_zc(shape->integrate_z_chunk) || !kf_valid_ray_rows(shape->raycast_rows))
+    return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  b->int_zc = shape->integrate_z_chunk;
+  b->ray_rows = shape->raycast_rows;
+  // the integrate block prefix depends on the z-chunk: rebuild the tables at the next step
+  b->members.clear();
+  b->member_keys.clear();
+  return KF_OK;
+}
+
+int kf_batch_get_launch_shape(kf_batch* b, kf_launch_shape* shape) {
+  if (!b || !shape) return KF_ERR_INVALID_ARGUMENT;
+  std::memset(shape, 0, sizeof(*shape));
+  shape->integrate_z_chunk = b->int_zc;
+  shape->raycast_rows = b->ray_rows;
+  return KF_OK;
+}
+
+int kf_batch_autotune(kf_batch* b, kf_session* const* ss, int n, int repeats, kf_launch_shape* chosen,
+                      float* times_ms) {
+  if (!b || !ss || n < 1 || n > b->cap || repeats < 1 || repeats > 1000) return KF_ERR_INVALID_ARGUMENT;
+  int rc = check_members(b, ss, n);
+  if (rc) return rc;
+  int cur = 0;
+  KF_CUDA_TRY(b, cudaGetDevice(&cur));
+  if (cur != b->device) KF_CUDA_TRY(b, cudaSetDevice(b->device));
+  KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  std::vector<kf_scratch_target> t(n);
+  for (int e = 0; e < n && !rc; ++e) {
+    if (cudaStreamSynchronize(ss[e]->stream) != cudaSuccess) {
+      rc = bfail(b, KF_ERR_CUDA, "autotune: a member's stream failed");
+      break;
+    }
+    if ((rc = kf_scratch_alloc(ss[e], &t[e]))) {
+      bfail(b, rc, "autotune scratch: " + ss[e]->last_error);
+      break;
+    }
+    if (cudaStreamSynchronize(ss[e]->stream) != cudaSuccess) rc = bfail(b, KF_ERR_CUDA, "autotune scratch copy");
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    rc = bfail(b, KF_ERR_CUDA, "autotune events");
+  // the tables are rebuilt here with scratch targets, one candidate at a time
+  b->members.assign(ss, ss + n);
+  b->member_keys.clear();
+  const int zc0 = b->int_zc, rows0 = b->ray_rows;
+  float best[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+  for (int round = 0; round < 2 && !rc; ++round)
+    for (int c = 0; c < 6 && !rc; ++c) {
+      const bool ray = c >= 3;
+      if (cudaStreamSynchronize(b->stream) != cudaSuccess) { rc = bfail(b, KF_ERR_CUDA, "autotune"); break; }
+      b->table_used = 0;
+      if (ray) {
+        b->ray_rows = kf_tune_ray_rows[c - 3];
+        rc = kf_batch_prepare_raycast(b, t.data());
+      } else {
+        b->int_zc = kf_tune_int_zc[c];
+        rc = kf_batch_prepare_integrate(b, t.data());
+      }
+      if (rc) { bfail(b, rc, "autotune tables"); break; }
+      if (cudaMemcpyAsync(b->d_table, b->h_table, b->table_used, cudaMemcpyHostToDevice, b->stream) != cudaSuccess) {
+        rc = bfail(b, KF_ERR_CUDA, "autotune tables");
+        break;
+      }
+      auto launch = [&]() { return ray ? kf_batch_launch_raycast(b, n) : kf_batch_launch_integrate(b); };
+      if ((rc = launch())) break;
+      if (cudaEventRecord(e0, b->stream) != cudaSuccess) { rc = bfail(b, KF_ERR_CUDA, "autotune timing"); break; }
+      for (int r = 0; r < repeats && !rc; ++r) rc = launch();
+      if (rc) break;
+      float ms = 0.0f;
+      if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = bfail(b, KF_ERR_CUDA, "autotune timing");
+        break;
+      }
+      best[c] = std::min(best[c], ms / (float)repeats);
+    }
+  cudaStreamSynchronize(b->stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (auto& x : t) kf_scratch_free(&x);
+  // the next step rebuilds the real tables
+  b->members.clear();
+  b->member_keys.clear();
+  b->int_zc = zc0;
+  b->ray_rows = rows0;
+  if (rc) return rc;
+  int zi = 1, ri = 4;  // the defaults win ties
+  for (int c = 0; c < 3; ++c)
+    if (best[c] < best[zi]) zi = c;
+  for (int c = 3; c < 6; ++c)
+    if (best[c] < best[ri]) ri = c;
+  b->int_zc = kf_tune_int_zc[zi];
+  b->ray_rows = kf_tune_ray_rows[ri - 3];
+  if (chosen) kf_batch_get_launch_shape(b, chosen);
+  if (times_ms) std::memcpy(times_ms, best, sizeof(best));
   return KF_OK;
 }
 

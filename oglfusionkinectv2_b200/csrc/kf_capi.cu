@@ -7,6 +7,7 @@
 // The first kf_frame_step_* call captures the device part of a frame into a CUDA graph;
 // later calls replay it.
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -313,7 +314,61 @@ int finish_step(kf_session* s, int* tracked) {
 std::mutex g_occ_mu;
 std::map<std::pair<const void*, int>, int> g_occ;
 
+// tuned launch shapes by (device, nx, ny, nz, storage, width, height)
+typedef std::array<int, 7> TuneKey;
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, int>> g_tune;
+
+TuneKey tune_key(const kf_session* s) {
+  return TuneKey{s->device, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->cfg.storage, s->intr.width, s->intr.height};
+}
+
+void tune_cache_apply(kf_session* s) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(s));
+  if (it == g_tune.end()) return;
+  s->int_zc = it->second.first;
+  s->ray_rows = it->second.second;
+}
+
 }  // namespace
+
+void kf_tune_cache_put(const kf_session* s, int zc, int rows) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[tune_key(s)] = std::make_pair(zc, rows);
+}
+
+void kf_scratch_free(kf_scratch_target* t) {
+  cudaFree(t->vol);
+  cudaFree(t->bricks);
+  cudaFree(t->out_v);
+  cudaFree(t->st_out);
+  *t = kf_scratch_target{};
+}
+
+int kf_scratch_alloc(kf_session* s, kf_scratch_target* t) {
+  *t = kf_scratch_target{};
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  const size_t nflags = (size_t)s->bx * s->by * s->bz + (size_t)s->sbx * s->sby * s->sbz;
+  int rc = KF_OK;
+  char* vol = nullptr;
+  float4* maps = nullptr;
+  if ((rc = dalloc(s, &vol, s->vol_bytes)) || (rc = dalloc(s, &t->bricks, nflags)) || (rc = dalloc(s, &maps, 2 * px)) ||
+      (rc = dalloc(s, &t->st_out, 1))) {
+    t->vol = vol;
+    t->out_v = maps;
+    kf_scratch_free(t);
+    return rc;
+  }
+  t->vol = vol;
+  t->supers = t->bricks + (size_t)s->bx * s->by * s->bz;
+  t->out_v = maps;
+  t->out_n = maps + px;
+  KF_CUDA_TRY(s, cudaMemcpyAsync(t->vol, s->d_vol, s->vol_bytes, cudaMemcpyDeviceToDevice, s->stream));
+  KF_CUDA_TRY(s, cudaMemcpyAsync(t->bricks, s->d_bricks, nflags * 4, cudaMemcpyDeviceToDevice, s->stream));
+  KF_CUDA_TRY(s, cudaMemcpyAsync(t->st_out, s->d_state, sizeof(KfDevState), cudaMemcpyDeviceToDevice, s->stream));
+  return KF_OK;
+}
 
 // SDF tracking in the frame step: TrackSDF's result drives the same policy flags as ICP.
 __global__ void kf_sdf_policy_kernel(KfDevState* st, int every) {
@@ -435,6 +490,7 @@ int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out)
   s->intr = *intr;
   cudaGetDevice(&s->device);
   cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
+  tune_cache_apply(s);
   auto bail = [&](int code) {
     free_all(s);
     delete s;
@@ -1075,6 +1131,75 @@ int kf_get_launch_count(kf_session* s, uint64_t* launches) {
 int kf_get_stream(kf_session* s, void** stream) {
   if (!s || !stream) return KF_ERR_INVALID_ARGUMENT;
   *stream = (void*)s->stream;
+  return KF_OK;
+}
+
+// ---- launch shapes and the autotuner ------------------------------------------------------
+int kf_set_launch_shape(kf_session* s, const kf_launch_shape* shape) {
+  if (!s || !shape || !kf_valid_int_zc(shape->integrate_z_chunk) || !kf_valid_ray_rows(shape->raycast_rows))
+    return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  drop_graph(s);  // the captured frames hold the old shapes
+  s->int_zc = shape->integrate_z_chunk;
+  s->ray_rows = shape->raycast_rows;
+  return KF_OK;
+}
+
+int kf_get_launch_shape(kf_session* s, kf_launch_shape* shape) {
+  if (!s || !shape) return KF_ERR_INVALID_ARGUMENT;
+  std::memset(shape, 0, sizeof(*shape));
+  shape->integrate_z_chunk = s->int_zc;
+  shape->raycast_rows = s->ray_rows;
+  return KF_OK;
+}
+
+int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* times_ms) {
+  if (!s || repeats < 1 || repeats > 1000) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  kf_scratch_target t;
+  int rc = kf_scratch_alloc(s, &t);
+  if (rc) return rc;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(s, KF_ERR_CUDA, "autotune events");
+  // each candidate: one untimed launch, then `repeats` launches between two events; two
+  // rounds over all candidates, the better mean kept (clock and cache drift even out)
+  float best[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+  for (int round = 0; round < 2 && !rc; ++round)
+    for (int c = 0; c < 6 && !rc; ++c) {
+      const bool ray = c >= 3;
+      const int v = ray ? kf_tune_ray_rows[c - 3] : kf_tune_int_zc[c];
+      auto launch = [&]() {
+        return ray ? kf_launch_raycast_shape(s, v, &t) : kf_launch_integrate_shape(s, 0, v, &t);
+      };
+      if ((rc = launch())) break;
+      if (cudaEventRecord(e0, s->stream) != cudaSuccess) { rc = fail(s, KF_ERR_CUDA, "autotune timing failed"); break; }
+      for (int r = 0; r < repeats && !rc; ++r) rc = launch();
+      if (rc) break;
+      float ms = 0.0f;
+      if (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = fail(s, KF_ERR_CUDA, "autotune timing failed");
+        break;
+      }
+      best[c] = std::min(best[c], ms / (float)repeats);
+    }
+  cudaStreamSynchronize(s->stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  kf_scratch_free(&t);
+  if (rc) return rc;
+  int zi = 1, ri = 4;  // the defaults win ties
+  for (int c = 0; c < 3; ++c)
+    if (best[c] < best[zi]) zi = c;
+  for (int c = 3; c < 6; ++c)
+    if (best[c] < best[ri]) ri = c;
+  kf_launch_shape sh{};
+  sh.integrate_z_chunk = kf_tune_int_zc[zi];
+  sh.raycast_rows = kf_tune_ray_rows[ri - 3];
+  if ((rc = kf_set_launch_shape(s, &sh))) return rc;
+  kf_tune_cache_put(s, sh.integrate_z_chunk, sh.raycast_rows);
+  if (chosen) *chosen = sh;
+  if (times_ms) std::memcpy(times_ms, best, sizeof(best));
   return KF_OK;
 }
 

@@ -8,10 +8,10 @@
 // below 0.2, clamped to [-0.1, 0.2] with w = min(w + 1, maxWeight); otherwise (and for
 // eta <= -mu) value and weight are zeroed (Q8).
 //
-// B200 design: a block owns 32 x 8 columns by 16 z (one warp = 32 consecutive x: 64 B
+// B200 design: a block owns 32 x 8 columns by ZC z (one warp = 32 consecutive x: 64 B
 // per plane per z-step for 2-byte storage, fully used sectors); splitting the z-march
-// over 16-voxel chunks gives the SMs enough independent warps to hide the depth-gather and
-// volume latencies.  A block whose voxel box lies outside one of the five frustum
+// over ZC-voxel chunks (8, 16 or 32, tuned per volume) gives the SMs enough independent
+// warps to hide the depth-gather and volume latencies.  A block whose voxel box lies outside one of the five frustum
 // half-spaces returns at once, so voxels that cannot project into the image cost nothing;
 // inside, every voxel runs the reference's tests.  Per voxel one reciprocal replaces the
 // shader's divisions by z (u = fx * x/z + cx + 0.5 is the reference's (fx x + cx z)/z + 0.5
@@ -47,7 +47,9 @@ __device__ __forceinline__ uint32_t bits_of(const T& v) {
   return b;
 }
 
-constexpr int kZC = 16;  // voxels per thread along z
+// Voxels per thread along z (the block's brick of columns is 32 x 8 x ZC): one of
+// KF_INT_ZCHUNKS, chosen per session (default 16, or the autotuner's pick).  Every choice
+// computes the same volume.
 
 // True when the box of voxel centres [b0, b1] (index space, inclusive) lies entirely on the
 // outside of one of the five half-spaces whose intersection is the set of voxels
@@ -74,25 +76,28 @@ __device__ __forceinline__ bool box_outside_frustum(const IntArgs& a, const floa
          (o3 & 0xffu) == 0xffu || (o4 & 0xffu) == 0xffu;
 }
 
-// The z-chunk [zb, zb + kZC) of column (x, y); returns which z-bricks received a negative
+// The z-chunk [zb, zb + ZC) of column (x, y); returns which z-bricks received a negative
 // value (bit j = brick zb/8 - 1 + j, bit 0 for the dilation of a z % 8 == 0 voxel).
-template <int S>
+template <int S, int ZC>
 __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const float* inv, int x, int y, int zb) {
   typedef typename Vox<S>::V V;
   typedef typename Vox<S>::Wt Wt;
-  // bits 0-2: NEG of z-bricks zb/8 - 1 + j; bit 6: NEG of z-super-brick zb/64, bit 7: of
-  // zb/64 - 1 (a z % 64 == 0 voxel is that one's +1 layer)
+  // bits 0..ZC/8: NEG of z-bricks zb/8 - 1 + j; bit 6: NEG of z-super-brick zb/64, bit 7:
+  // of zb/64 - 1 (a z % 64 == 0 voxel is that one's +1 layer)
+  static_assert(ZC == 8 || ZC == 16 || ZC == 32, "z chunk: 8, 16 or 32 voxels");
   uint32_t flags = 0;
 
-  // getVolumePosition (integrate.cs:16-19) at z = zb, and delta = rotate(invTrack, (0,0,vz))
+  // getVolumePosition (integrate.cs:16-19) and delta = rotate(invTrack, (0,0,vz)): the
+  // camera-space position is computed directly at every z % 8 == 0 voxel and stepped by
+  // delta in between, so it does not depend on where a chunk starts (every z-chunk size
+  // gives the same volume)
   const float cxw = (x + 0.5f) * a.dimx / a.nx;
   const float cyw = (y + 0.5f) * a.dimy / a.ny;
-  const float czw = (zb + 0.5f) * a.dimz / a.nz;
   const float vz = a.dimz / a.nz;
-  float p0[3], dz[3];
+  float pxy[3], dz[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    p0[r] = fmaf(inv[r * 4 + 0], cxw, fmaf(inv[r * 4 + 1], cyw, fmaf(inv[r * 4 + 2], czw, inv[r * 4 + 3])));
+    pxy[r] = fmaf(inv[r * 4 + 0], cxw, fmaf(inv[r * 4 + 1], cyw, inv[r * 4 + 3]));
     dz[r] = inv[r * 4 + 2] * vz;
   }
   V* vf = reinterpret_cast<V*>(a.vol);
@@ -101,10 +106,16 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   uint32_t idx = (uint32_t)x + (uint32_t)a.nx * (uint32_t)y + (uint32_t)zb * slice;
   const float fW1 = (float)(a.W - 1), fH1 = (float)(a.H - 1);
   const float ku = a.cx + 0.5f, kv = a.cy + 0.5f;
-  const int zend = min(kZC, a.nz - zb);
-  // the camera-space position steps by delta along z, as integrate.cs:57-62 does
-  float px = p0[0], py = p0[1], pz = p0[2];
+  const int zend = min(ZC, a.nz - zb);
+  // between anchors the position steps by delta along z, as integrate.cs:57-62 does
+  float px = 0.0f, py = 0.0f, pz = 0.0f;
   for (int k = 0; k < zend; ++k, idx += slice, px += dz[0], py += dz[1], pz += dz[2]) {
+    if ((k & 7) == 0) {
+      const float czw = (zb + k + 0.5f) * a.dimz / a.nz;
+      px = fmaf(inv[2], czw, pxy[0]);
+      py = fmaf(inv[6], czw, pxy[1]);
+      pz = fmaf(inv[10], czw, pxy[2]);
+    }
     if (pz < 0.0001f) continue;
     const float iz = __fdividef(1.0f, pz);  // hardware reciprocal (2 ulp)
     const float rx = px * iz;  // pos.x / pos.z
@@ -163,7 +174,7 @@ struct IntBatch {
   int n;
 };
 
-template <int S, bool BATCH>
+template <int S, bool BATCH, int ZC>
 __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBatch batch) {
   __shared__ IntArgs s_args;
   int bxi, byi, bzi;  // this block's position in its volume's block grid
@@ -193,27 +204,28 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
   float inv[12];  // inverse(m_pose), rows of [R^T | -R^T t] (integrate uses glm::inverse, :1242)
 #pragma unroll
   for (int k = 0; k < 12; ++k) inv[k] = a.st->inv_rows[k];
-  const int xb = bxi * 32, yb = byi * 8, zb = bzi * kZC;
+  const int xb = bxi * 32, yb = byi * 8, zb = bzi * ZC;
   // Every warp evaluates the block's frustum test itself (the same inputs give the same
   // answer in every warp), so no warp waits for another: the kernel has no block barrier.
   // One voxel of margin on every side absorbs the rounding of the per-voxel tests.
   {
     const int b0[3] = {xb - 1, yb - 1, zb - 1};
-    const int b1[3] = {xb + 32, yb + 8, zb + kZC};
+    const int b1[3] = {xb + 32, yb + 8, zb + ZC};
     if (box_outside_frustum(a, inv, b0, b1)) return;
   }
   const int lane = threadIdx.x;
   const int x = xb + lane;
   const int y = yb + threadIdx.y;  // uniform over the warp
   uint32_t flags = 0;  // integrate_column's bits
-  if (x < a.nx && y < a.ny) flags = integrate_column<S>(a, inv, x, y, zb);
+  if (x < a.nx && y < a.ny) flags = integrate_column<S, ZC>(a, inv, x, y, zb);
   if (!__any_sync(0xffffffffu, flags != 0)) return;
   // Brick flags, merged over the warp: lanes 8c-8..8c-1 write brick column c of the block
   // (c = 1..4) and a lane on a brick's low x face also brick column c-1 (dilation); lane c
   // sets the merged bits of column c in global memory.  Most bricks near surfaces have the
   // bits already, so read first and skip those atomics.
   const int lx = (x >> 3) - (xb >> 3) + 1;
-  const uint32_t zbits = flags & 7u;
+  constexpr int kZBits = ZC / 8 + 1;  // z-bricks a chunk touches, with the dilation one
+  const uint32_t zbits = flags & ((1u << kZBits) - 1u);
   uint32_t mine = 0;
 #pragma unroll
   for (int c = 0; c < 5; ++c) {
@@ -223,7 +235,7 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
   }
   if (lane < 5 && mine) {
     const int gx = (xb >> 3) - 1 + lane;
-    for (int j = 0; j < 3; ++j) {
+    for (int j = 0; j < kZBits; ++j) {
       if (!((mine >> j) & 1u)) continue;
       const int gz = (zb >> 3) - 1 + j;
       for (int dy = 0; dy < ((y & 7) == 0 ? 2 : 1); ++dy) {
@@ -279,29 +291,47 @@ IntArgs make_int_args(kf_session* s, int gated) {
   return a;
 }
 
-template <bool BATCH>
-void launch_int(int storage, dim3 grid, cudaStream_t st, const IntArgs& a, const IntBatch& b) {
+template <bool BATCH, int ZC>
+void launch_int_zc(int storage, dim3 grid, cudaStream_t st, const IntArgs& a, const IntBatch& b) {
   dim3 block(32, 8);
   switch (storage) {
-    case KF_STORAGE_F32F32: integrate_kernel<KF_STORAGE_F32F32, BATCH><<<grid, block, 0, st>>>(a, b); break;
-    case KF_STORAGE_F16U16: integrate_kernel<KF_STORAGE_F16U16, BATCH><<<grid, block, 0, st>>>(a, b); break;
-    default: integrate_kernel<KF_STORAGE_RG16I, BATCH><<<grid, block, 0, st>>>(a, b); break;
+    case KF_STORAGE_F32F32: integrate_kernel<KF_STORAGE_F32F32, BATCH, ZC><<<grid, block, 0, st>>>(a, b); break;
+    case KF_STORAGE_F16U16: integrate_kernel<KF_STORAGE_F16U16, BATCH, ZC><<<grid, block, 0, st>>>(a, b); break;
+    default: integrate_kernel<KF_STORAGE_RG16I, BATCH, ZC><<<grid, block, 0, st>>>(a, b); break;
   }
+}
+
+template <bool BATCH>
+void launch_int(int storage, int zc, dim3 grid, cudaStream_t st, const IntArgs& a, const IntBatch& b) {
+  if (zc == 8) launch_int_zc<BATCH, 8>(storage, grid, st, a, b);
+  else if (zc == 32) launch_int_zc<BATCH, 32>(storage, grid, st, a, b);
+  else launch_int_zc<BATCH, 16>(storage, grid, st, a, b);
+}
+
+IntArgs retarget(IntArgs a, const kf_scratch_target* t) {
+  if (t) {
+    a.vol = t->vol;
+    a.bricks = t->bricks;
+    a.supers = t->supers;
+  }
+  return a;
 }
 
 }  // namespace
 
-int kf_launch_integrate(kf_session* s, int gated) {
-  const IntArgs a = make_int_args(s, gated);
-  dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + kZC - 1) / kZC);
-  launch_int<false>(s->cfg.storage, grid, s->stream, a, IntBatch{nullptr, nullptr, 0});
+int kf_launch_integrate_shape(kf_session* s, int gated, int zc, const kf_scratch_target* t) {
+  const IntArgs a = retarget(make_int_args(s, gated), t);
+  dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + zc - 1) / zc);
+  launch_int<false>(s->cfg.storage, zc, grid, s->stream, a, IntBatch{nullptr, nullptr, 0});
   KF_CUDA_TRY(s, cudaGetLastError());
   kf_note_launch(s);
   return KF_OK;
 }
 
+int kf_launch_integrate(kf_session* s, int gated) { return kf_launch_integrate_shape(s, gated, s->int_zc, nullptr); }
+
 // ---- batched: every member's gated frame-step integrate in one launch ----
-int kf_batch_prepare_integrate(kf_batch* b) {
+int kf_batch_prepare_integrate(kf_batch* b, const kf_scratch_target* over) {
   const int n = (int)b->members.size();
   IntArgs* h = nullptr;
   uint32_t* hp = nullptr;
@@ -309,10 +339,12 @@ int kf_batch_prepare_integrate(kf_batch* b) {
   b->int_prefix = static_cast<const uint32_t*>(kf_batch_table(b, 4 * (size_t)(n + 1), reinterpret_cast<void**>(&hp)));
   if (!b->int_args || !b->int_prefix) return KF_ERR_CAPACITY;
   uint64_t total = 0;
+  const int zc = b->int_zc;
   for (int e = 0; e < n; ++e) {
-    h[e] = make_int_args(b->members[e], 1);
+    // the autotuner's timing runs ungated into scratch copies
+    h[e] = over ? retarget(make_int_args(b->members[e], 0), over + e) : make_int_args(b->members[e], 1);
     hp[e] = (uint32_t)total;
-    total += (uint64_t)((h[e].nx + 31) / 32) * ((h[e].ny + 7) / 8) * ((h[e].nz + kZC - 1) / kZC);
+    total += (uint64_t)((h[e].nx + 31) / 32) * ((h[e].ny + 7) / 8) * ((h[e].nz + zc - 1) / zc);
   }
   if (total >= (1ull << 31)) return KF_ERR_CAPACITY;
   hp[n] = (uint32_t)total;
@@ -322,7 +354,7 @@ int kf_batch_prepare_integrate(kf_batch* b) {
 
 int kf_batch_launch_integrate(kf_batch* b) {
   const IntBatch batch = {static_cast<const IntArgs*>(b->int_args), b->int_prefix, (int)b->members.size()};
-  launch_int<true>(b->members[0]->cfg.storage, dim3(b->int_blocks), b->stream, IntArgs{}, batch);
+  launch_int<true>(b->members[0]->cfg.storage, b->int_zc, dim3(b->int_blocks), b->stream, IntArgs{}, batch);
   KF_CUDA_TRY(b, cudaGetLastError());
   b->launches += 1;
   return KF_OK;

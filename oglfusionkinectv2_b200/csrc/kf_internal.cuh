@@ -60,6 +60,16 @@ struct KfDevState {
 #define KF_STATE_RESULT_BYTES (offsetof(KfDevState, pose_rows))
 static_assert(KF_STATE_RESULT_BYTES == 144, "frame result head: pose, tracked, error, recover_found, counter");
 
+// Where the autotuner's timing launches write instead of the session's own buffers.
+struct kf_scratch_target {
+  void* vol;             // integrate: a copy of the volume
+  uint32_t* bricks;      // and of the brick / super-brick flags
+  uint32_t* supers;
+  float4* out_v;         // raycast: vertex and normal maps
+  float4* out_n;
+  KfDevState* st_out;    // raycast: the control block that receives raycast_pose
+};
+
 struct kf_session {
   kf_config cfg{};
   kf_intrinsics intr{};
@@ -140,6 +150,10 @@ struct kf_session {
   uint32_t* h_u32_scalar = nullptr;  // pinned
 
   float4* d_mip = nullptr;  // intensity-projection image, allocated on first use
+
+  // launch shapes (kf_set_launch_shape / kf_autotune); every choice computes the same result
+  int int_zc = 16;   // integrate: voxels per thread along z (8, 16, 32)
+  int ray_rows = 4;  // raycast: tile rows of 32 pixels (2, 4, 8)
 
   // depth ingest before the pyramid (off by default): Kinect-v2 undistortion through a
   // source-index map, and the filter3D.cs validity filter; their output is d_depth_prep
@@ -568,6 +582,10 @@ struct kf_batch {
   const uint32_t* int_prefix = nullptr;
   uint32_t int_blocks = 0;
   const void* ray_args = nullptr;
+  // launch shapes of the batched integrate and raycast (kf_batch_set_launch_shape /
+  // kf_batch_autotune); the integrate block prefix in the tables depends on int_zc
+  int int_zc = 16;
+  int ray_rows = 4;
   // gathered frame results: [cap][KF_STATE_RESULT_BYTES]
   char* d_heads = nullptr;
   char* h_heads = nullptr;
@@ -610,8 +628,9 @@ inline int kf_batch_block_map(kf_batch* b, int total, const uint32_t** d_map) {
 int kf_batch_prepare_pyramid(kf_batch* b);
 int kf_batch_prepare_icp(kf_batch* b);
 int kf_batch_prepare_sdf(kf_batch* b);
-int kf_batch_prepare_integrate(kf_batch* b);
-int kf_batch_prepare_raycast(kf_batch* b);
+// `over` (one per member, or null): the autotuner's scratch targets (ungated integrate)
+int kf_batch_prepare_integrate(kf_batch* b, const kf_scratch_target* over);
+int kf_batch_prepare_raycast(kf_batch* b, const kf_scratch_target* over);
 int kf_batch_launch_pyramid(kf_batch* b, int n, const uint16_t* const* d_inputs);
 int kf_batch_launch_icp(kf_batch* b);
 int kf_batch_launch_sdf_recover(kf_batch* b);
@@ -643,6 +662,18 @@ int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy);
 int kf_launch_sdf_policy(kf_session* s);
 int kf_launch_integrate(kf_session* s, int gated);
 int kf_launch_raycast(kf_session* s);
+int kf_launch_integrate_shape(kf_session* s, int gated, int zc, const kf_scratch_target* t);
+int kf_launch_raycast_shape(kf_session* s, int rows, const kf_scratch_target* t);
+inline bool kf_valid_int_zc(int zc) { return zc == 8 || zc == 16 || zc == 32; }
+inline bool kf_valid_ray_rows(int r) { return r == 2 || r == 4 || r == 8; }
+constexpr int kf_tune_int_zc[3] = {8, 16, 32};
+constexpr int kf_tune_ray_rows[3] = {2, 4, 8};
+// Scratch copies of a session's volume, brick flags and control block plus scratch maps,
+// for timing launches without touching the session (kf_capi.cu).
+int kf_scratch_alloc(kf_session* s, kf_scratch_target* t);
+void kf_scratch_free(kf_scratch_target* t);
+// Tuned shapes remembered per (device, volume size, storage, image size) for new sessions.
+void kf_tune_cache_put(const kf_session* s, int zc, int rows);
 int kf_launch_intensity_projection(kf_session* s, float4* out);
 int kf_rebuild_bricks(kf_session* s, cudaStream_t stream);
 int kf_reset_bricks(kf_session* s);

@@ -10,7 +10,7 @@
 // central-difference trilinear gradient (getGradient :229-276), zero when its length is
 // zero.  Misses write zero vertex and normal.
 //
-// B200 design: one thread per pixel, 32x4 tiles so a warp's rays stay coherent and its
+// B200 design: one thread per pixel, 32-wide tiles so a warp's rays stay coherent and its
 // trilinear taps share L1 lines; the value plane alone is read (2 B per tap for the
 // 16-bit storages).  The march position is t0 + k * step (one rounding) rather than the
 // reference's repeated float addition.  Once the march is in its fine-step phase it
@@ -41,10 +41,10 @@ struct RayArgs {
   int sbx, sby, sbz;
 };
 
-// 32 x 4 pixel tiles: ray lengths vary a lot, and small blocks keep the SMs evenly loaded
-// to the end of the launch (512 x 424 gives 1,696 blocks)
-constexpr int kRayRows = 4;
-constexpr int kRayThreads = 32 * kRayRows;
+// 32 x ROWS pixel tiles (ROWS one of KF_RAY_ROWS, chosen per session: default 4, or the
+// autotuner's pick): ray lengths vary a lot, and small blocks keep the SMs evenly loaded to
+// the end of the launch (512 x 424 in 32 x 4 tiles gives 1,696 blocks).  Every choice
+// computes the same maps.
 
 template <int S>
 struct Sampler {
@@ -76,14 +76,15 @@ struct Sampler {
 };
 
 // BATCH: blockIdx.z selects the session's arguments in `many`.
-template <int S, bool BATCH>
-__global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs one, const RayArgs* many) {
+template <int S, bool BATCH, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS) raycast_kernel(RayArgs one, const RayArgs* many) {
+  static_assert(ROWS == 2 || ROWS == 4 || ROWS == 8, "raycast tile rows: 2, 4 or 8");
   __shared__ RayArgs s_args;
   __shared__ float s_view[12];  // rows of m_pose * invK: (R K^-1 | t)
   if constexpr (BATCH) {
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int* src = reinterpret_cast<const int*>(many + blockIdx.z);
-    for (int k = tid; k < (int)(sizeof(RayArgs) / 4); k += kRayThreads) reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
+    for (int k = tid; k < (int)(sizeof(RayArgs) / 4); k += 32 * ROWS) reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
     __syncthreads();
   }
   const RayArgs& a = BATCH ? s_args : one;
@@ -290,7 +291,7 @@ __global__ void __launch_bounds__(kRayThreads) raycast_kernel(RayArgs one, const
 // are unreachable).  Sample positions are tnear + k * largeStep (one rounding, as in the
 // raycast).  The reference dispatches it on demand, never from the frame loop; so does this.
 template <int S>
-__global__ void __launch_bounds__(kRayThreads) mip_kernel(RayArgs a, float4* out) {
+__global__ void __launch_bounds__(128) mip_kernel(RayArgs a, float4* out) {
   __shared__ float s_view[12];
   if (threadIdx.y == 0 && threadIdx.x < 12) {
     const int r = threadIdx.x >> 2, c = threadIdx.x & 3;
@@ -451,31 +452,49 @@ RayArgs make_ray_args(kf_session* s) {
   return a;
 }
 
-template <bool BATCH>
-void launch_ray(int storage, dim3 grid, cudaStream_t st, const RayArgs& a, const RayArgs* many) {
-  dim3 block(32, kRayRows);
+template <bool BATCH, int ROWS>
+void launch_ray_rows(int storage, dim3 grid, cudaStream_t st, const RayArgs& a, const RayArgs* many) {
+  dim3 block(32, ROWS);
   switch (storage) {
-    case KF_STORAGE_F32F32: raycast_kernel<KF_STORAGE_F32F32, BATCH><<<grid, block, 0, st>>>(a, many); break;
-    case KF_STORAGE_F16U16: raycast_kernel<KF_STORAGE_F16U16, BATCH><<<grid, block, 0, st>>>(a, many); break;
-    default: raycast_kernel<KF_STORAGE_RG16I, BATCH><<<grid, block, 0, st>>>(a, many); break;
+    case KF_STORAGE_F32F32: raycast_kernel<KF_STORAGE_F32F32, BATCH, ROWS><<<grid, block, 0, st>>>(a, many); break;
+    case KF_STORAGE_F16U16: raycast_kernel<KF_STORAGE_F16U16, BATCH, ROWS><<<grid, block, 0, st>>>(a, many); break;
+    default: raycast_kernel<KF_STORAGE_RG16I, BATCH, ROWS><<<grid, block, 0, st>>>(a, many); break;
   }
+}
+
+template <bool BATCH>
+void launch_ray(int storage, int rows, dim3 grid, cudaStream_t st, const RayArgs& a, const RayArgs* many) {
+  if (rows == 2) launch_ray_rows<BATCH, 2>(storage, grid, st, a, many);
+  else if (rows == 8) launch_ray_rows<BATCH, 8>(storage, grid, st, a, many);
+  else launch_ray_rows<BATCH, 4>(storage, grid, st, a, many);
+}
+
+RayArgs retarget(RayArgs a, const kf_scratch_target* t) {
+  if (t) {
+    a.out_v = t->out_v;
+    a.out_n = t->out_n;
+    a.st_out = t->st_out;
+  }
+  return a;
 }
 
 }  // namespace
 
-int kf_launch_raycast(kf_session* s) {
-  const RayArgs a = make_ray_args(s);
-  dim3 grid((a.W + 31) / 32, (a.H + kRayRows - 1) / kRayRows);
-  launch_ray<false>(s->cfg.storage, grid, s->stream, a, nullptr);
+int kf_launch_raycast_shape(kf_session* s, int rows, const kf_scratch_target* t) {
+  const RayArgs a = retarget(make_ray_args(s), t);
+  dim3 grid((a.W + 31) / 32, (a.H + rows - 1) / rows);
+  launch_ray<false>(s->cfg.storage, rows, grid, s->stream, a, nullptr);
   KF_CUDA_TRY(s, cudaGetLastError());
   kf_note_launch(s);
   return KF_OK;
 }
 
+int kf_launch_raycast(kf_session* s) { return kf_launch_raycast_shape(s, s->ray_rows, nullptr); }
+
 int kf_launch_intensity_projection(kf_session* s, float4* out) {
   const RayArgs a = make_ray_args(s);
-  dim3 grid((a.W + 31) / 32, (a.H + kRayRows - 1) / kRayRows);
-  dim3 block(32, kRayRows);
+  dim3 grid((a.W + 31) / 32, (a.H + 3) / 4);
+  dim3 block(32, 4);
   switch (s->cfg.storage) {
     case KF_STORAGE_F32F32: mip_kernel<KF_STORAGE_F32F32><<<grid, block, 0, s->stream>>>(a, out); break;
     case KF_STORAGE_F16U16: mip_kernel<KF_STORAGE_F16U16><<<grid, block, 0, s->stream>>>(a, out); break;
@@ -487,19 +506,20 @@ int kf_launch_intensity_projection(kf_session* s, float4* out) {
 }
 
 // ---- batched: every member's raycast in one launch (blockIdx.z = member) ----
-int kf_batch_prepare_raycast(kf_batch* b) {
+int kf_batch_prepare_raycast(kf_batch* b, const kf_scratch_target* over) {
   const int n = (int)b->members.size();
   RayArgs* h = nullptr;
   b->ray_args = kf_batch_table(b, sizeof(RayArgs) * n, reinterpret_cast<void**>(&h));
   if (!b->ray_args) return KF_ERR_CAPACITY;
-  for (int e = 0; e < n; ++e) h[e] = make_ray_args(b->members[e]);
+  for (int e = 0; e < n; ++e) h[e] = retarget(make_ray_args(b->members[e]), over ? over + e : nullptr);
   return KF_OK;
 }
 
 int kf_batch_launch_raycast(kf_batch* b, int n) {
   kf_session* s0 = b->members[0];
-  dim3 grid((s0->W[0] + 31) / 32, (s0->H[0] + kRayRows - 1) / kRayRows, n);
-  launch_ray<true>(s0->cfg.storage, grid, b->stream, RayArgs{}, static_cast<const RayArgs*>(b->ray_args));
+  const int rows = b->ray_rows;
+  dim3 grid((s0->W[0] + 31) / 32, (s0->H[0] + rows - 1) / rows, n);
+  launch_ray<true>(s0->cfg.storage, rows, grid, b->stream, RayArgs{}, static_cast<const RayArgs*>(b->ray_args));
   KF_CUDA_TRY(b, cudaGetLastError());
   b->launches += 1;
   return KF_OK;

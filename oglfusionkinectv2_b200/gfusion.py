@@ -17,6 +17,11 @@ import numpy as np
 from . import _lib as L
 
 
+def _tune_times(t) -> dict:
+    names = ["integrate_z8", "integrate_z16", "integrate_z32", "raycast_rows2", "raycast_rows4", "raycast_rows8"]
+    return {n: float(v) for n, v in zip(names, t)}
+
+
 def _pose_to_c(pose) -> C.Array:
     m = np.asarray(pose, dtype=np.float64).reshape(4, 4)
     return (C.c_double * 16)(*m.flatten(order="F"))
@@ -284,6 +289,24 @@ class GFusion:
         """shaders/filter3D.cs before the pyramid (after the undistortion)."""
         self._check(self.lib.kf_set_depth_filter(self._h, int(bool(enable))), "kf_set_depth_filter")
 
+    # ---- launch shapes and the autotuner -----------------------------------------------
+    def setLaunchShape(self, integrate_z_chunk: int, raycast_rows: int) -> None:
+        sh = L.kf_launch_shape(int(integrate_z_chunk), int(raycast_rows))
+        self._check(self.lib.kf_set_launch_shape(self._h, C.byref(sh)), "kf_set_launch_shape")
+
+    def launchShape(self) -> tuple:
+        sh = L.kf_launch_shape()
+        self._check(self.lib.kf_get_launch_shape(self._h, C.byref(sh)), "kf_get_launch_shape")
+        return sh.integrate_z_chunk, sh.raycast_rows
+
+    def autotune(self, repeats: int = 5):
+        """Time every integrate z-chunk and raycast tile shape on the current frame and use
+        the fastest.  Returns ((z_chunk, rows), {shape name: mean ms})."""
+        sh = L.kf_launch_shape()
+        t = (C.c_float * 6)()
+        self._check(self.lib.kf_autotune(self._h, int(repeats), C.byref(sh), t), "kf_autotune")
+        return (sh.integrate_z_chunk, sh.raycast_rows), _tune_times(t)
+
     def intensityProjection(self) -> np.ndarray:
         """Volume ray-sum image at the current pose (gFusion::intensityProjection,
         src/gFusion.cpp:1368-1409), H x W x 4: (sum of positive samples, 0, 0, 1)."""
@@ -424,6 +447,24 @@ class GFusionBatch:
         n = C.c_uint64()
         self._check(self.lib.kf_batch_get_launch_count(self._h, C.byref(n)), "kf_batch_get_launch_count")
         return int(n.value)
+
+    def setLaunchShape(self, integrate_z_chunk: int, raycast_rows: int) -> None:
+        sh = L.kf_launch_shape(int(integrate_z_chunk), int(raycast_rows))
+        self._check(self.lib.kf_batch_set_launch_shape(self._h, C.byref(sh)), "kf_batch_set_launch_shape")
+
+    def launchShape(self) -> tuple:
+        sh = L.kf_launch_shape()
+        self._check(self.lib.kf_batch_get_launch_shape(self._h, C.byref(sh)), "kf_batch_get_launch_shape")
+        return sh.integrate_z_chunk, sh.raycast_rows
+
+    def autotune(self, sessions, repeats: int = 3):
+        """kf_batch_autotune over this mix of sessions; returns ((z_chunk, rows), times)."""
+        n = len(sessions)
+        hs = (C.c_void_p * n)(*[s.handle.value for s in sessions])
+        sh = L.kf_launch_shape()
+        t = (C.c_float * 6)()
+        self._check(self.lib.kf_batch_autotune(self._h, hs, n, int(repeats), C.byref(sh), t), "kf_batch_autotune")
+        return (sh.integrate_z_chunk, sh.raycast_rows), _tune_times(t)
 
 
 class GFusionServer:

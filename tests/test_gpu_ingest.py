@@ -69,7 +69,10 @@ def test_ingest_level0_is_bit_exact(undistort, filt):
 
 def test_frame_loop_with_ingest_matches_oracle():
     """Undistortion and filter on in the captured frame graph: same tracked flags as the
-    oracle, poses within 1 mm, and the same frames as the step-by-step entry points."""
+    oracle, poses within 1 mm, and the same frames as the step-by-step entry points.  The
+    frames carry the workload's own sensor noise and dropouts (with the harsher noise of
+    _noisy_frame the 5 mm filter leaves too few pixels for a well-conditioned ICP, and the
+    FP64 and FP32 trackers wander apart by millimetres)."""
     w = small_workload(6, size=128)
     g, o = pair(w)
     h = GFusion(w.config, w.intrinsics)
@@ -78,7 +81,7 @@ def test_frame_loop_with_ingest_matches_oracle():
         s.setDepthUndistortion(IRS[0])
         s.setDepthFilter(True)
     for k in range(w.n_frames):
-        f = _noisy_frame(w, k, 100 + k)
+        f = w.frame(k)
         tg, to = g.frameStep(f), o.frameStep(f)
         assert tg == to, k
         assert np.linalg.norm(g.getPose()[:3, 3] - o.getPose()[:3, 3]) < 1e-3
