@@ -66,11 +66,14 @@ struct IcpBatch {
 constexpr float kFix = 4294967296.0f;       // 2^32
 constexpr double kInvFix = 1.0 / 4294967296.0;
 
-// ---- track.cs:53-133 for one pixel ------------------------------------------------------
-// n, v: the pixel's normal and vertex (loaded one pass ahead by the caller)
-__device__ __forceinline__ int track_pixel(const IcpArgs& a, const float4 n, const float4 v,
-                                           const float* T, const float* V, const float* c,
-                                           float* f, float* pw) {
+// ---- track.cs:53-133 for one pixel, in two phases -----------------------------------------
+// The caller projects its pixels first, then issues every reference gather (normal and
+// vertex together, for all of its pixels) and only then finishes them: the gathers are the
+// latency of this kernel, and none of them waits for another.
+// n, v: the pixel's normal and vertex.  Returns the status for a pixel that stops here, or
+// 0 with the transformed vertex pv and the reference index *ri.
+__device__ __forceinline__ int track_project(const IcpArgs& a, const float4 n, const float4 v, const float* T,
+                                             const float* V, float* pv, int* ri) {
   if (n.x == 2.0f) return -1;
   // z == 0 with a valid normal projects (0,0,0) -> 0/0 in track.cs:72 (undefined in
   // GLSL); treated as "outside the image"
@@ -86,10 +89,19 @@ __device__ __forceinline__ int track_pixel(const IcpArgs& a, const float4 n, con
   const float px = ppx / ppz + 0.5f, py = ppy / ppz + 0.5f;
   if (!(px >= 0.0f) || px > (float)(a.W0 - 1) || !(py >= 0.0f) || py > (float)(a.H0 - 1))
     return -2;
-  const size_t ri = (size_t)(int)py * a.W0 + (int)px;
-  const float4 rn = __ldg(&a.ref_normal[ri]);
+  *ri = (int)py * a.W0 + (int)px;
+  pv[0] = pvx;
+  pv[1] = pvy;
+  pv[2] = pvz;
+  return 0;
+}
+
+// The rest of track.cs for a pixel that track_project passed, with its reference normal rn
+// and vertex rv.
+__device__ __forceinline__ int track_finish(const IcpArgs& a, const float4 n, const float* pv, const float4 rn,
+                                            const float4 rv, const float* T, const float* c, float* f, float* pw) {
   if (rn.x == -2.0f) return -3;
-  const float4 rv = __ldg(&a.ref_vertex[ri]);
+  const float pvx = pv[0], pvy = pv[1], pvz = pv[2];
   const float dx = rv.x - pvx, dy = rv.y - pvy, dz = rv.z - pvz;
   // projectedNormal = rotate(Ttrack, normal)
   const float pnx = T[0] * n.x + T[4] * n.y + T[8] * n.z;
@@ -309,9 +321,16 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
         if (i1 + 2 * stride < P) { n1 = __ldg(Nl + i1 + 2 * stride); v1 = __ldg(Vl + i1 + 2 * stride); }
         float f0[7] = {0, 0, 0, 0, 0, 0, 0}, f1[7] = {0, 0, 0, 0, 0, 0, 0};
         float pw0[3] = {0, 0, 0}, pw1[3] = {0, 0, 0};
-        int st0 = 0, st1 = 0;
-        if (i0 < P) st0 = track_pixel(a, na, va, s_T, s_V, c, f0, pw0);
-        if (i1 < P) st1 = track_pixel(a, nb1, vb1, s_T, s_V, c, f1, pw1);
+        float q0[3], q1[3];
+        int st0 = 0, st1 = 0, r0 = 0, r1 = 0;
+        if (i0 < P) st0 = track_project(a, na, va, s_T, s_V, q0, &r0);
+        if (i1 < P) st1 = track_project(a, nb1, vb1, s_T, s_V, q1, &r1);
+        const bool g0 = i0 < P && st0 == 0, g1 = i1 < P && st1 == 0;
+        float4 rn0 = zero, rv0 = zero, rn1 = zero, rv1 = zero;
+        if (g0) { rn0 = __ldg(&a.ref_normal[r0]); rv0 = __ldg(&a.ref_vertex[r0]); }
+        if (g1) { rn1 = __ldg(&a.ref_normal[r1]); rv1 = __ldg(&a.ref_vertex[r1]); }
+        if (g0) st0 = track_finish(a, na, q0, rn0, rv0, s_T, c, f0, pw0);
+        if (g1) st1 = track_finish(a, nb1, q1, rn1, rv1, s_T, c, f1, pw1);
         if (i0 < P) {
           a.status[level][i0] = st0;
           if (a.q1 && ((i0 / Wl) & 7) != 7) st0 = 0;  // only work group 7 reaches the solver
