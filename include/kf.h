@@ -317,6 +317,18 @@ KF_API int kf_batch_get_poses(kf_batch* b, int n, double* poses16);
 /* Device ms of the last step's stages: pyramid, track, integrate, recover, raycast. */
 KF_API int kf_batch_get_stage_times(kf_batch* b, float* ms5);
 KF_API int kf_batch_get_launch_count(kf_batch* b, uint64_t* launches);
+/* Asynchronous batched step (device-resident frames): enqueues the step and returns once
+ * the PREVIOUS step's results are read (waiting for that one only), so the device runs one
+ * step while the host prepares the next.  After it, kf_batch_get_poses / kf_batch_get_tracked
+ * describe the previous step; its error status (e.g. KF_ERR_TIMEOUT of a member) is this
+ * call's return value.  kf_batch_sync waits for and reads the step still in flight.  Until
+ * then the step's sessions must not be used on their own.  Every other batch call finishes
+ * the step in flight first. */
+KF_API int kf_batch_frame_step_u16_device_async(kf_batch* b, kf_session* const* sessions,
+                                                const uint16_t* const* device_depth_mm, int n);
+KF_API int kf_batch_sync(kf_batch* b);
+/* Tracked flags of the last step whose results were read (as kf_batch_get_poses). */
+KF_API int kf_batch_get_tracked(kf_batch* b, int n, int32_t* tracked);
 /* Launch shapes of the batched integrate and raycast (one shape per batch launch). */
 KF_API int kf_batch_set_launch_shape(kf_batch* b, const kf_launch_shape* shape);
 KF_API int kf_batch_get_launch_shape(kf_batch* b, kf_launch_shape* shape);

@@ -140,6 +140,9 @@ SIGNATURES = {
     "kf_set_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
     "kf_get_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
     "kf_autotune": (_I, [_P, _I, C.POINTER(kf_launch_shape), _PF]),
+    "kf_batch_frame_step_u16_device_async": (_I, [_P, _P, _P, _I]),
+    "kf_batch_sync": (_I, [_P]),
+    "kf_batch_get_tracked": (_I, [_P, _I, _P]),
     "kf_batch_set_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
     "kf_batch_get_launch_shape": (_I, [_P, C.POINTER(kf_launch_shape)]),
     "kf_batch_autotune": (_I, [_P, _P, _I, _I, C.POINTER(kf_launch_shape), _PF]),

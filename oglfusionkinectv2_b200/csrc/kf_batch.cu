@@ -88,65 +88,25 @@ int rebuild_tables(kf_batch* b, kf_session* const* ss, int n) {
   return KF_OK;
 }
 
-int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth, int n, int32_t* tracked,
-               cudaMemcpyKind kind) {
-  if (!b || !ss || !depth || n <= 0) return KF_ERR_INVALID_ARGUMENT;
-  if (n > b->cap) return bfail(b, KF_ERR_CAPACITY, "more sessions than the batch was created for");
-  int rc = check_members(b, ss, n);
-  if (rc) return rc;
-  for (int e = 0; e < n; ++e)
-    if (!depth[e]) return bfail(b, KF_ERR_INVALID_ARGUMENT, "null depth frame");
-  int cur = 0;
-  KF_CUDA_TRY(b, cudaGetDevice(&cur));
-  if (cur != b->device) KF_CUDA_TRY(b, cudaSetDevice(b->device));
-  // a destroyed session's address may come back for a new one, and a session may
-  // reallocate its buffers: the tables are keyed by (address, uid, layout)
-  if (!same_members(b, ss, n) && (rc = rebuild_tables(b, ss, n))) return rc;
-  // a member's own stream may still hold work (an asynchronous frame step)
-  for (int e = 0; e < n; ++e)
-    if (cudaStreamQuery(ss[e]->stream) != cudaSuccess) KF_CUDA_TRY(b, cudaStreamSynchronize(ss[e]->stream));
-  const uint16_t* const* inputs = nullptr;
-  if (kind == cudaMemcpyHostToDevice) {
-    const size_t px = (size_t)ss[0]->W[0] * ss[0]->H[0];
-    for (int e = 0; e < n; ++e)
-      KF_CUDA_TRY(b, cudaMemcpyAsync(ss[e]->d_depth_u16, depth[e], px * 2, kind, b->stream));
-  } else {
-    // device frames are read in place: one small upload of their addresses
-    for (int e = 0; e < n; ++e) b->h_inputs[e] = depth[e];
-    KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_inputs, b->h_inputs, n * sizeof(uint16_t*), cudaMemcpyHostToDevice,
-                                   b->stream));
-    inputs = b->d_inputs;
-  }
-  KF_CUDA_TRY(b, cudaEventRecord(b->ev[0], b->stream));
-  batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
-  KF_CUDA_TRY(b, cudaGetLastError());
-  if ((rc = kf_batch_launch_pyramid(b, n, inputs))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(b->ev[1], b->stream));
-  if ((rc = kf_batch_launch_icp(b))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(b->ev[2], b->stream));
-  if ((rc = kf_batch_launch_integrate(b))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(b->ev[3], b->stream));
-  if ((rc = kf_batch_launch_sdf_recover(b))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(b->ev[4], b->stream));
-  if ((rc = kf_batch_launch_raycast(b, n))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(b->ev[5], b->stream));
-  // every KF_BRICK_REBUILD_EVERY integrates a member's skip flags are rebuilt exactly
-  for (int e = 0; e < n; ++e)
-    if ((rc = kf_note_integrate(ss[e], b->stream))) return bfail(b, rc, "brick flag rebuild: " + ss[e]->last_error);
-  batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
-  KF_CUDA_TRY(b, cudaGetLastError());
-  b->launches += 2;
-  KF_CUDA_TRY(b, cudaMemcpyAsync(b->h_heads, b->d_heads, (size_t)n * KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost,
-                                 b->stream));
-  KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
-  for (int i = 0; i < 5; ++i) KF_CUDA_TRY(b, cudaEventElapsedTime(&b->stage_ms[i], b->ev[i], b->ev[i + 1]));
-  b->steps += 1;
+// Reads the results of the pending step (waits for it): each member's frame result into
+// its host state, the stage times, the tracked flags; a member's device timeout is
+// reported and cleared.
+int harvest(kf_batch* b) {
+  const int slot = b->pend_slot;
+  if (slot < 0) return KF_OK;
+  b->pend_slot = -1;
+  KF_CUDA_TRY(b, cudaEventSynchronize(b->ev[slot][6]));  // this step's results are copied
+  for (int i = 0; i < 5; ++i) KF_CUDA_TRY(b, cudaEventElapsedTime(&b->stage_ms[i], b->ev[slot][i], b->ev[slot][i + 1]));
+  const int n = (int)b->pend_members.size();
+  const char* heads = b->h_heads + (size_t)slot * b->cap * KF_STATE_RESULT_BYTES;
+  b->last_slot = slot;
   b->last_n = n;
+  b->last_tracked.assign(n, 0);
   int first_err = KF_OK;
   for (int e = 0; e < n; ++e) {
-    kf_session* s = ss[e];
-    std::memcpy(s->h_state, b->h_heads + (size_t)e * KF_STATE_RESULT_BYTES, KF_STATE_RESULT_BYTES);
-    if (tracked) tracked[e] = s->h_state->tracked;
+    kf_session* s = b->pend_members[e];
+    std::memcpy(s->h_state, heads + (size_t)e * KF_STATE_RESULT_BYTES, KF_STATE_RESULT_BYTES);
+    b->last_tracked[e] = s->h_state->tracked;
     if (s->h_state->error) {
       const int err = s->h_state->error;
       s->h_state->error = 0;
@@ -159,6 +119,85 @@ int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth,
   return first_err;
 }
 
+// Enqueues one step into the next slot (the previous step may still be running).
+int enqueue_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth, int n, cudaMemcpyKind kind) {
+  if (!b || !ss || !depth || n <= 0) return KF_ERR_INVALID_ARGUMENT;
+  if (n > b->cap) return bfail(b, KF_ERR_CAPACITY, "more sessions than the batch was created for");
+  int rc = check_members(b, ss, n);
+  if (rc) return rc;
+  for (int e = 0; e < n; ++e)
+    if (!depth[e]) return bfail(b, KF_ERR_INVALID_ARGUMENT, "null depth frame");
+  int cur = 0;
+  KF_CUDA_TRY(b, cudaGetDevice(&cur));
+  if (cur != b->device) KF_CUDA_TRY(b, cudaSetDevice(b->device));
+  // a destroyed session's address may come back for a new one, and a session may
+  // reallocate its buffers: the tables are keyed by (address, uid, layout).  The host
+  // table is rewritten only once the pending step (whose copy may read it) is done.
+  if (!same_members(b, ss, n)) {
+    if ((rc = harvest(b))) return rc;
+    KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    if ((rc = rebuild_tables(b, ss, n))) return rc;
+  }
+  // a member's own stream may still hold work (an asynchronous frame step)
+  for (int e = 0; e < n; ++e)
+    if (cudaStreamQuery(ss[e]->stream) != cudaSuccess) KF_CUDA_TRY(b, cudaStreamSynchronize(ss[e]->stream));
+  const int slot = (int)(b->steps & 1u);
+  cudaEvent_t* ev = b->ev[slot];
+  const uint16_t* const* inputs = nullptr;
+  if (kind == cudaMemcpyHostToDevice) {
+    const size_t px = (size_t)ss[0]->W[0] * ss[0]->H[0];
+    for (int e = 0; e < n; ++e)
+      KF_CUDA_TRY(b, cudaMemcpyAsync(ss[e]->d_depth_u16, depth[e], px * 2, kind, b->stream));
+  } else {
+    // device frames are read in place: one small upload of their addresses
+    const uint16_t** hin = b->h_inputs + (size_t)slot * b->cap;
+    for (int e = 0; e < n; ++e) hin[e] = depth[e];
+    KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_inputs, hin, n * sizeof(uint16_t*), cudaMemcpyHostToDevice, b->stream));
+    inputs = b->d_inputs;
+  }
+  KF_CUDA_TRY(b, cudaEventRecord(ev[0], b->stream));
+  batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
+  KF_CUDA_TRY(b, cudaGetLastError());
+  if ((rc = kf_batch_launch_pyramid(b, n, inputs))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(ev[1], b->stream));
+  if ((rc = kf_batch_launch_icp(b))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(ev[2], b->stream));
+  if ((rc = kf_batch_launch_integrate(b))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(ev[3], b->stream));
+  if ((rc = kf_batch_launch_sdf_recover(b))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(ev[4], b->stream));
+  if ((rc = kf_batch_launch_raycast(b, n))) return rc;
+  KF_CUDA_TRY(b, cudaEventRecord(ev[5], b->stream));
+  // every KF_BRICK_REBUILD_EVERY integrates a member's skip flags are rebuilt exactly
+  for (int e = 0; e < n; ++e)
+    if ((rc = kf_note_integrate(ss[e], b->stream))) return bfail(b, rc, "brick flag rebuild: " + ss[e]->last_error);
+  batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
+  KF_CUDA_TRY(b, cudaGetLastError());
+  b->launches += 2;
+  KF_CUDA_TRY(b, cudaMemcpyAsync(b->h_heads + (size_t)slot * b->cap * KF_STATE_RESULT_BYTES, b->d_heads,
+                                 (size_t)n * KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost, b->stream));
+  KF_CUDA_TRY(b, cudaEventRecord(ev[6], b->stream));
+  b->steps += 1;
+  // the previous step's results are read now, while this one runs
+  const int prev = harvest(b);
+  b->pend_slot = slot;
+  b->pend_members.assign(ss, ss + n);
+  return prev;
+}
+
+int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth, int n, int32_t* tracked,
+               cudaMemcpyKind kind) {
+  int rc = enqueue_step(b, ss, depth, n, kind);
+  if (rc) {
+    harvest(b);
+    return rc;
+  }
+  if ((rc = harvest(b))) return rc;
+  if (tracked)
+    for (int e = 0; e < n; ++e) tracked[e] = b->last_tracked[e];
+  return KF_OK;
+}
+
 void free_batch(kf_batch* b) {
   cudaFree(b->d_table);
   cudaFreeHost(b->h_table);
@@ -166,8 +205,9 @@ void free_batch(kf_batch* b) {
   cudaFreeHost(b->h_heads);
   cudaFree(b->d_inputs);
   cudaFreeHost(b->h_inputs);
-  for (auto& e : b->ev)
-    if (e) cudaEventDestroy(e);
+  for (auto& row : b->ev)
+    for (auto& e : row)
+      if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -195,16 +235,17 @@ int kf_batch_create(int max_sessions, kf_batch** out) {
   if (cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess)
     return bail(KF_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(KF_ERR_CUDA);
-  for (auto& e : b->ev)
-    if (cudaEventCreate(&e) != cudaSuccess) return bail(KF_ERR_CUDA);
+  for (auto& row : b->ev)
+    for (auto& e : row)
+      if (cudaEventCreate(&e) != cudaSuccess) return bail(KF_ERR_CUDA);
   // per member: seven argument records (< 2 KB) and two block maps of the co-resident grid
   b->table_cap = 64 * 1024 + (size_t)max_sessions * 2048;
   if (cudaMallocHost((void**)&b->h_table, b->table_cap) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
   if (cudaMalloc((void**)&b->d_table, b->table_cap) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
   const size_t hb = (size_t)max_sessions * KF_STATE_RESULT_BYTES;
-  if (cudaMallocHost((void**)&b->h_heads, hb) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
+  if (cudaMallocHost((void**)&b->h_heads, 2 * hb) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
   if (cudaMalloc((void**)&b->d_heads, hb) != cudaSuccess) return bail(KF_ERR_OUT_OF_MEMORY);
-  if (cudaMallocHost((void**)&b->h_inputs, max_sessions * sizeof(uint16_t*)) != cudaSuccess)
+  if (cudaMallocHost((void**)&b->h_inputs, 2 * max_sessions * sizeof(uint16_t*)) != cudaSuccess)
     return bail(KF_ERR_OUT_OF_MEMORY);
   if (cudaMalloc((void**)&b->d_inputs, max_sessions * sizeof(uint16_t*)) != cudaSuccess)
     return bail(KF_ERR_OUT_OF_MEMORY);
@@ -214,6 +255,7 @@ int kf_batch_create(int max_sessions, kf_batch** out) {
 
 int kf_batch_destroy(kf_batch* b) {
   if (!b) return KF_ERR_INVALID_ARGUMENT;
+  harvest(b);
   cudaStreamSynchronize(b->stream);
   free_batch(b);
   delete b;
@@ -238,11 +280,29 @@ int kf_batch_get_stage_times(kf_batch* b, float* ms) {
   return KF_OK;
 }
 
+int kf_batch_frame_step_u16_device_async(kf_batch* b, kf_session* const* sessions,
+                                         const uint16_t* const* device_depth_mm, int n) {
+  return enqueue_step(b, sessions, device_depth_mm, n, cudaMemcpyDeviceToDevice);
+}
+
+int kf_batch_sync(kf_batch* b) {
+  if (!b) return KF_ERR_INVALID_ARGUMENT;
+  return harvest(b);
+}
+
 int kf_batch_get_poses(kf_batch* b, int n, double* poses) {
   if (!b || !poses || n < 0) return KF_ERR_INVALID_ARGUMENT;
   if (n > b->last_n) return bfail(b, KF_ERR_INVALID_ARGUMENT, "more poses than the last step had sessions");
+  const char* heads = b->h_heads + (size_t)b->last_slot * b->cap * KF_STATE_RESULT_BYTES;
   for (int e = 0; e < n; ++e)
-    std::memcpy(poses + 16 * e, b->h_heads + (size_t)e * KF_STATE_RESULT_BYTES, 16 * sizeof(double));
+    std::memcpy(poses + 16 * e, heads + (size_t)e * KF_STATE_RESULT_BYTES, 16 * sizeof(double));
+  return KF_OK;
+}
+
+int kf_batch_get_tracked(kf_batch* b, int n, int32_t* tracked) {
+  if (!b || !tracked || n < 0) return KF_ERR_INVALID_ARGUMENT;
+  if (n > b->last_n) return bfail(b, KF_ERR_INVALID_ARGUMENT, "more flags than the last step had sessions");
+  for (int e = 0; e < n; ++e) tracked[e] = b->last_tracked[e];
   return KF_OK;
 }
 
@@ -255,6 +315,7 @@ int kf_batch_get_launch_count(kf_batch* b, uint64_t* n) {
 int kf_batch_set_launch_shape(kf_batch* b, const kf_launch_shape* shape) {
   if (!b || !shape || !kf_valid_int_zc(shape->integrate_z_chunk) || !kf_valid_ray_rows(shape->raycast_rows))
     return KF_ERR_INVALID_ARGUMENT;
+  if (int rc = harvest(b)) return rc;
   KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
   b->int_zc = shape->integrate_z_chunk;
   b->ray_rows = shape->raycast_rows;
@@ -280,6 +341,7 @@ int kf_batch_autotune(kf_batch* b, kf_session* const* ss, int n, int repeats, kf
   int cur = 0;
   KF_CUDA_TRY(b, cudaGetDevice(&cur));
   if (cur != b->device) KF_CUDA_TRY(b, cudaSetDevice(b->device));
+  if ((rc = harvest(b))) return rc;
   KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
   std::vector<kf_scratch_target> t(n);
   for (int e = 0; e < n && !rc; ++e) {

@@ -107,61 +107,65 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   const float fW1 = (float)(a.W - 1), fH1 = (float)(a.H - 1);
   const float ku = a.cx + 0.5f, kv = a.cy + 0.5f;
   const int zend = min(ZC, a.nz - zb);
-  // between anchors the position steps by delta along z, as integrate.cs:57-62 does
-  float px = 0.0f, py = 0.0f, pz = 0.0f;
-  for (int k = 0; k < zend; ++k, idx += slice, px += dz[0], py += dz[1], pz += dz[2]) {
-    if ((k & 7) == 0) {
-      const float czw = (zb + k + 0.5f) * a.dimz / a.nz;
-      px = fmaf(inv[2], czw, pxy[0]);
-      py = fmaf(inv[6], czw, pxy[1]);
-      pz = fmaf(inv[10], czw, pxy[2]);
-    }
-    if (pz < 0.0001f) continue;
-    const float iz = __fdividef(1.0f, pz);  // hardware reciprocal (2 ulp)
-    const float rx = px * iz;  // pos.x / pos.z
-    const float ry = py * iz;
-    // cameraX.x / cameraX.z + 0.5 = fx * x/z + cx + 0.5 (K has no skew, :67)
-    const float u = fmaf(a.fx, rx, ku);
-    const float v = fmaf(a.fy, ry, kv);
-    if (u < 0.0f || u > fW1 || v < 0.0f || v > fH1) continue;
-    const float d = __ldg(a.depth + (uint32_t)(int)v * (uint32_t)a.W + (uint32_t)(int)u) * 0.001f;
-    if (d == 0.0f) continue;
-    const float r2 = fmaf(rx, rx, fmaf(ry, ry, 1.0f));
-    const float diff = (d - pz) * (r2 * rsqrtf(r2));  // sqrt(r2), r2 >= 1
-    if (diff > -a.mu) {
-      const float sdf = fminf(1.0f, diff * a.inv_mu);
-      const V oldv = vf[idx];
-      const Wt oldw = vw[idx];
-      const float F = Vox<S>::raw_nc(&oldv, 0) * Vox<S>::kRawToF;
-      const float w = Vox<S>::weight(&oldw, 0);
-      const float wd = __fdividef(fmaf(w, F, sdf), w + 1.0f);
-      float nF, nw;
-      if (!a.band) {
-        // the reference's earlier update (integrate.cs:115-150)
-        nF = fminf(fmaxf(wd, -1.0f), 1.0f);
-        nw = fminf(w + 1.0f, a.maxw);
-      } else if (wd < 0.2f) {
-        nF = fminf(fmaxf(wd, -0.1f), 0.2f);
-        nw = fminf(w + 1.0f, a.maxw);
+  // one 8-voxel brick of the column at a time: the position is anchored at the brick's first
+  // voxel and steps by delta inside it, as integrate.cs:57-62 does (unrolled: no per-voxel
+  // loop or anchor test)
+  for (int k8 = 0; k8 < zend; k8 += 8) {
+    const float czw = (zb + k8 + 0.5f) * a.dimz / a.nz;
+    float px = fmaf(inv[2], czw, pxy[0]);
+    float py = fmaf(inv[6], czw, pxy[1]);
+    float pz = fmaf(inv[10], czw, pxy[2]);
+    const int n8 = min(8, zend - k8);
+    const int jb = (k8 >> 3) + 1;  // this brick's bit in flags
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj, idx += slice, px += dz[0], py += dz[1], pz += dz[2]) {
+      if (jj >= n8) break;
+      if (pz < 0.0001f) continue;
+      const float iz = __fdividef(1.0f, pz);  // hardware reciprocal (2 ulp)
+      const float rx = px * iz;  // pos.x / pos.z
+      const float ry = py * iz;
+      // cameraX.x / cameraX.z + 0.5 = fx * x/z + cx + 0.5 (K has no skew, :67)
+      const float u = fmaf(a.fx, rx, ku);
+      const float v = fmaf(a.fy, ry, kv);
+      if (u < 0.0f || u > fW1 || v < 0.0f || v > fH1) continue;
+      const float d = __ldg(a.depth + (uint32_t)(int)v * (uint32_t)a.W + (uint32_t)(int)u) * 0.001f;
+      if (d == 0.0f) continue;
+      const float r2 = fmaf(rx, rx, fmaf(ry, ry, 1.0f));
+      const float diff = (d - pz) * (r2 * rsqrtf(r2));  // sqrt(r2), r2 >= 1
+      if (diff > -a.mu) {
+        const float sdf = fminf(1.0f, diff * a.inv_mu);
+        const V oldv = vf[idx];
+        const Wt oldw = vw[idx];
+        const float F = Vox<S>::raw_nc(&oldv, 0) * Vox<S>::kRawToF;
+        const float w = Vox<S>::weight(&oldw, 0);
+        const float wd = __fdividef(fmaf(w, F, sdf), w + 1.0f);
+        float nF, nw;
+        if (!a.band) {
+          // the reference's earlier update (integrate.cs:115-150)
+          nF = fminf(fmaxf(wd, -1.0f), 1.0f);
+          nw = fminf(w + 1.0f, a.maxw);
+        } else if (wd < 0.2f) {
+          nF = fminf(fmaxf(wd, -0.1f), 0.2f);
+          nw = fminf(w + 1.0f, a.maxw);
+        } else {
+          nF = 0.0f;
+          nw = 0.0f;
+        }
+        const V ev = Vox<S>::encode_value(nF);
+        const Wt ew = Vox<S>::encode_weight(nw);
+        if (bits_of(ev) != bits_of(oldv)) vf[idx] = ev;
+        if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
+        // a non-negative nF never stores a negative value; a brick's first voxel is also
+        // the +1 layer of the brick below it (and, at z % 64 == 0, of the super-brick below)
+        if (nF < 0.0f) {
+          flags |= 1u << jb;
+          if (jj == 0) flags |= (1u << (jb - 1)) | (((zb + k8) & 63) == 0 ? 0xc0u : 0x40u);
+          else flags |= 0x40u;
+        }
       } else {
-        nF = 0.0f;
-        nw = 0.0f;
+        vf[idx] = Vox<S>::encode_value(0.0f);
+        vw[idx] = Vox<S>::encode_weight(0.0f);
       }
-      const V ev = Vox<S>::encode_value(nF);
-      const Wt ew = Vox<S>::encode_weight(nw);
-      if (bits_of(ev) != bits_of(oldv)) vf[idx] = ev;
-      if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
-      // a non-negative nF never stores a negative value
-      if (nF < 0.0f) {
-        const int z = zb + k;
-        const int j = (z >> 3) - (zb >> 3) + 1;
-        flags |= 1u << j;
-        if ((z & 7) == 0) flags |= 1u << (j - 1);
-        flags |= (z & 63) == 0 ? 0xc0u : 0x40u;
-      }
-    } else {
-      vf[idx] = Vox<S>::encode_value(0.0f);
-      vw[idx] = Vox<S>::encode_weight(0.0f);
     }
   }
   return flags;

@@ -586,14 +586,22 @@ struct kf_batch {
   // kf_batch_autotune); the integrate block prefix in the tables depends on int_zc
   int int_zc = 16;
   int ray_rows = 4;
-  // gathered frame results: [cap][KF_STATE_RESULT_BYTES]
+  // Steps use two slots in turn, so that an asynchronous step can be enqueued while the
+  // previous one is still running: each slot has its gathered frame results
+  // (h_heads + slot * cap * KF_STATE_RESULT_BYTES, pinned), its input pointer list and its
+  // stage events.  The device buffers are shared (the stream orders them).
   char* d_heads = nullptr;
-  char* h_heads = nullptr;
+  char* h_heads = nullptr;                // pinned, 2 * cap * KF_STATE_RESULT_BYTES
+  const uint16_t** h_inputs = nullptr;    // pinned, 2 * cap
+  const uint16_t** d_inputs = nullptr;    // device, cap
+  cudaEvent_t ev[2][7] = {};  // stage boundaries [0..5], results copied [6]
+  // the enqueued step whose results are not read yet (-1: none), and its members
+  int pend_slot = -1;
+  std::vector<kf_session*> pend_members;
+  // the last step whose results were read: its slot and member count
+  int last_slot = 0;
   int last_n = 0;
-  // per-step device input pointers (device-resident frames are read in place)
-  const uint16_t** h_inputs = nullptr;  // pinned, cap
-  const uint16_t** d_inputs = nullptr;  // device, cap
-  cudaEvent_t ev[6] = {};
+  std::vector<int32_t> last_tracked;
   float stage_ms[5] = {0, 0, 0, 0, 0};
   uint64_t steps = 0;
   uint64_t launches = 0;

@@ -344,60 +344,74 @@ __global__ void __launch_bounds__(128) mip_kernel(RayArgs a, float4* out) {
   out[(size_t)y * a.W + x] = make_float4(sum, 0.0f, 0.0f, 1.0f);
 }
 
-// Exact NEG flag of every brick from the volume itself, over the voxels [8B, 8B+8]
-// (clamped to the volume).
-template <int S>
-__global__ void __launch_bounds__(256) rebuild_bricks_kernel(const void* vol, int nx, int ny, int nz, int bx, int by,
-                                                            int bz, uint32_t* bricks) {
-  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= (uint32_t)bx * by * bz) return;
-  const int ix = b % bx, iy = (b / bx) % by, iz = b / (bx * by);
-  const typename Vox<S>::V* f = reinterpret_cast<const typename Vox<S>::V*>(vol);
-  uint32_t flag = 0;
-  for (int z = 8 * iz; z <= min(8 * iz + 8, nz - 1) && !flag; ++z)
-    for (int y = 8 * iy; y <= min(8 * iy + 8, ny - 1); ++y)
-      for (int x = 8 * ix; x <= min(8 * ix + 8, nx - 1); ++x)
-        if (Vox<S>::raw(f, (uint32_t)x + (uint32_t)nx * ((uint32_t)y + (uint32_t)ny * (uint32_t)z)) < 0.0f)
-          flag = KF_BRICK_NEG;
-  bricks[b] = flag;
-}
+// Exact NEG flags from the volume itself: a brick B is NEG when a value over the voxels
+// [8B, 8B+8] (clamped to the volume) is negative, a super-brick when one of its 8^3 bricks
+// is (super-bricks are cleared first and set here).  A block takes one row of 32 bricks
+// along x at brick (y, z): thread t scans voxel column x0 + t over the brick's 9 x 9 (y, z)
+// window (coalesced along x), the extra warp the first columns of the next row (the +1
+// layer of the last brick), and thread c merges brick c's 9 columns from shared memory.
+constexpr int kRebuildThreads = 256 + 32;
 
-// A super-brick is NEG when one of its 8^3 bricks is (they cover [64S, 64S+64]).
-__global__ void __launch_bounds__(256) rebuild_supers_kernel(const uint32_t* bricks, int bx, int by, int bz,
-                                                            uint32_t* supers, int sbx, int sby, int sbz) {
-  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (uint32_t)sbx * sby * sbz) return;
-  const int sx = q % sbx, sy = (q / sbx) % sby, sz = q / (sbx * sby);
-  uint32_t f = 0;
-  for (int z = 8 * sz; z < min(8 * sz + 8, bz) && !f; ++z)
-    for (int y = 8 * sy; y < min(8 * sy + 8, by) && !f; ++y)
-      for (int x = 8 * sx; x < min(8 * sx + 8, bx); ++x)
-        f |= bricks[(uint32_t)x + (uint32_t)bx * ((uint32_t)y + (uint32_t)by * (uint32_t)z)] & KF_BRICK_NEG;
-  supers[q] = f;
+template <int S>
+__global__ void __launch_bounds__(kRebuildThreads) rebuild_bricks_kernel(const void* vol, int nx, int ny, int nz,
+                                                                          int bx, int by, int bz, uint32_t* bricks,
+                                                                          uint32_t* supers, int sbx, int sby) {
+  __shared__ uint8_t s_neg[kRebuildThreads];
+  const typename Vox<S>::V* f = reinterpret_cast<const typename Vox<S>::V*>(vol);
+  const int x = blockIdx.x * 256 + threadIdx.x;
+  const int y0 = 8 * blockIdx.y, y1 = min(y0 + 8, ny - 1);
+  const int z0 = 8 * blockIdx.z, z1 = min(z0 + 8, nz - 1);
+  bool neg = false;
+  if (x < nx)
+    for (int z = z0; z <= z1 && !neg; ++z) {
+      // the plane's (up to) 9 rows are loaded together; the scan stops after a plane
+      const uint32_t base = (uint32_t)x + (uint32_t)nx * (uint32_t)ny * (uint32_t)z;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const int y = min(y0 + k, y1);  // rows past the volume repeat the last one
+        neg |= Vox<S>::raw(f, base + (uint32_t)nx * (uint32_t)y) < 0.0f;
+      }
+    }
+  s_neg[threadIdx.x] = neg ? 1 : 0;
+  __syncthreads();
+  const int c = threadIdx.x;
+  const int b = blockIdx.x * 32 + c;
+  if (c < 32 && b < bx) {
+    uint8_t m = 0;
+#pragma unroll
+    for (int k = 0; k <= 8; ++k) m |= s_neg[8 * c + k];  // columns past nx - 1 hold 0
+    const uint32_t flag = m ? KF_BRICK_NEG : 0u;
+    bricks[(uint32_t)b + (uint32_t)bx * ((uint32_t)blockIdx.y + (uint32_t)by * (uint32_t)blockIdx.z)] = flag;
+    if (flag) {
+      uint32_t* w = &supers[(uint32_t)(b >> 3) +
+                            (uint32_t)sbx * ((uint32_t)(blockIdx.y >> 3) + (uint32_t)sby * (uint32_t)(blockIdx.z >> 3))];
+      if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
+    }
+  }
 }
 
 }  // namespace
 
 int kf_rebuild_bricks(kf_session* s, cudaStream_t stream) {
-  const uint32_t nb = (uint32_t)s->bx * s->by * s->bz;
-  const int g = (int)((nb + 255) / 256);
+  const uint32_t ns = (uint32_t)s->sbx * s->sby * s->sbz;
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_supers, 0, ns * sizeof(uint32_t), stream));
+  const dim3 grid((s->bx + 31) / 32, s->by, s->bz);
   switch (s->cfg.storage) {
     case KF_STORAGE_F32F32:
-      rebuild_bricks_kernel<KF_STORAGE_F32F32><<<g, 256, 0, stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      rebuild_bricks_kernel<KF_STORAGE_F32F32><<<grid, kRebuildThreads, 0, stream>>>(
+          s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks, s->d_supers, s->sbx, s->sby);
       break;
     case KF_STORAGE_F16U16:
-      rebuild_bricks_kernel<KF_STORAGE_F16U16><<<g, 256, 0, stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      rebuild_bricks_kernel<KF_STORAGE_F16U16><<<grid, kRebuildThreads, 0, stream>>>(
+          s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks, s->d_supers, s->sbx, s->sby);
       break;
     default:
-      rebuild_bricks_kernel<KF_STORAGE_RG16I><<<g, 256, 0, stream>>>(s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks);
+      rebuild_bricks_kernel<KF_STORAGE_RG16I><<<grid, kRebuildThreads, 0, stream>>>(
+          s->d_vol, s->cfg.nx, s->cfg.ny, s->cfg.nz, s->bx, s->by, s->bz, s->d_bricks, s->d_supers, s->sbx, s->sby);
       break;
   }
   KF_CUDA_TRY(s, cudaGetLastError());
-  const uint32_t ns = (uint32_t)s->sbx * s->sby * s->sbz;
-  rebuild_supers_kernel<<<(ns + 255) / 256, 256, 0, stream>>>(s->d_bricks, s->bx, s->by, s->bz, s->d_supers, s->sbx,
-                                                              s->sby, s->sbz);
-  KF_CUDA_TRY(s, cudaGetLastError());
-  kf_note_launch(s, 2);
+  kf_note_launch(s, 1);
   s->frames_since_rebuild = 0;
   return KF_OK;
 }

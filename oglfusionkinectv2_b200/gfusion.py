@@ -431,6 +431,23 @@ class GFusionBatch:
                     "kf_batch_frame_step_u16_device")
         return np.array(list(t), dtype=bool)
 
+    def frameStepDeviceAsync(self, sessions, device_ptrs) -> None:
+        """Enqueue a step and read the previous one's results (poses(), tracked()); the
+        device runs this step while the caller prepares the next.  sync() finishes it."""
+        n = len(sessions)
+        hs = (C.c_void_p * n)(*[s.handle.value for s in sessions])
+        ps = (C.c_void_p * n)(*[int(p) for p in device_ptrs])
+        self._check(self.lib.kf_batch_frame_step_u16_device_async(self._h, hs, ps, n),
+                    "kf_batch_frame_step_u16_device_async")
+
+    def sync(self) -> None:
+        self._check(self.lib.kf_batch_sync(self._h), "kf_batch_sync")
+
+    def tracked(self, n: int) -> np.ndarray:
+        t = (C.c_int32 * n)()
+        self._check(self.lib.kf_batch_get_tracked(self._h, n, t), "kf_batch_get_tracked")
+        return np.array(list(t), dtype=bool)
+
     def poses(self, n: int) -> np.ndarray:
         """Camera-to-world poses (n x 4 x 4) of the last step's first n sessions."""
         a = np.empty((n, 16), np.float64)

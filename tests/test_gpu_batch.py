@@ -154,3 +154,30 @@ def test_batch_tables_follow_replaced_sessions():
     ref_b.frameStep(fr[1][0])
     assert_same(snapshot(c), snapshot(ref_c))
     assert_same(snapshot(b), snapshot(ref_b))
+
+
+def test_batch_async_steps_match_sync_steps():
+    """Asynchronous steps (device frames): each call returns the previous step's results;
+    the sessions end exactly where synchronous steps take them."""
+    import torch
+    F = 5
+    ws = workloads(F)
+    frames = [[w.frame(k) for k in range(F)] for w in ws]
+    dev = [torch.from_numpy(np.stack(fr).view(np.int16)).cuda() for fr in frames]
+    fbytes = 512 * 424 * 2
+    sync_s, async_s = fresh(ws), fresh(ws)
+    b1, b2 = GFusionBatch(4), GFusionBatch(4)
+    torch.cuda.synchronize()
+    sync_poses = []
+    for k in range(F):
+        b1.frameStepDevice(sync_s, [d.data_ptr() + k * fbytes for d in dev])
+        sync_poses.append(b1.poses(len(ws)))
+    for k in range(F):
+        b2.frameStepDeviceAsync(async_s, [d.data_ptr() + k * fbytes for d in dev])
+        if k > 0:
+            np.testing.assert_array_equal(b2.poses(len(ws)), sync_poses[k - 1])
+    b2.sync()
+    np.testing.assert_array_equal(b2.poses(len(ws)), sync_poses[-1])
+    assert b2.tracked(len(ws)).all()
+    for ga, gb in zip(sync_s, async_s):
+        assert_same(snapshot(ga), snapshot(gb))
