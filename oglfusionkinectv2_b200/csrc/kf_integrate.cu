@@ -87,10 +87,10 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   static_assert(ZC == 8 || ZC == 16 || ZC == 32, "z chunk: 8, 16 or 32 voxels");
   uint32_t flags = 0;
 
-  // getVolumePosition (integrate.cs:16-19) and delta = rotate(invTrack, (0,0,vz)): the
-  // camera-space position is computed directly at every z % 8 == 0 voxel and stepped by
-  // delta in between, so it does not depend on where a chunk starts (every z-chunk size
-  // gives the same volume)
+  // getVolumePosition (integrate.cs:16-19; along z as (i + 0.5) * voxel size) and
+  // delta = rotate(invTrack, (0,0,vz)): the camera-space position is computed directly at
+  // every z % 8 == 0 voxel and stepped by delta in between, so it does not depend on where
+  // a chunk starts (every z-chunk size gives the same volume)
   const float cxw = (x + 0.5f) * a.dimx / a.nx;
   const float cyw = (y + 0.5f) * a.dimy / a.ny;
   const float vz = a.dimz / a.nz;
@@ -98,7 +98,7 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     pxy[r] = fmaf(inv[r * 4 + 0], cxw, fmaf(inv[r * 4 + 1], cyw, inv[r * 4 + 3]));
-    dz[r] = inv[r * 4 + 2] * vz;
+    dz[r] = __fmul_rn(inv[r * 4 + 2], vz);  // kept rounded: the steps below are plain adds
   }
   V* vf = reinterpret_cast<V*>(a.vol);
   Wt* vw = reinterpret_cast<Wt*>(reinterpret_cast<char*>(a.vol) + a.count * sizeof(V));
@@ -107,65 +107,73 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   const float fW1 = (float)(a.W - 1), fH1 = (float)(a.H - 1);
   const float ku = a.cx + 0.5f, kv = a.cy + 0.5f;
   const int zend = min(ZC, a.nz - zb);
-  // one 8-voxel brick of the column at a time: the position is anchored at the brick's first
-  // voxel and steps by delta inside it, as integrate.cs:57-62 does (unrolled: no per-voxel
-  // loop or anchor test)
-  for (int k8 = 0; k8 < zend; k8 += 8) {
-    const float czw = (zb + k8 + 0.5f) * a.dimz / a.nz;
-    float px = fmaf(inv[2], czw, pxy[0]);
-    float py = fmaf(inv[6], czw, pxy[1]);
-    float pz = fmaf(inv[10], czw, pxy[2]);
-    const int n8 = min(8, zend - k8);
-    const int jb = (k8 >> 3) + 1;  // this brick's bit in flags
-#pragma unroll
-    for (int jj = 0; jj < 8; ++jj, idx += slice, px += dz[0], py += dz[1], pz += dz[2]) {
-      if (jj >= n8) break;
-      if (pz < 0.0001f) continue;
-      const float iz = __fdividef(1.0f, pz);  // hardware reciprocal (2 ulp)
-      const float rx = px * iz;  // pos.x / pos.z
-      const float ry = py * iz;
-      // cameraX.x / cameraX.z + 0.5 = fx * x/z + cx + 0.5 (K has no skew, :67)
-      const float u = fmaf(a.fx, rx, ku);
-      const float v = fmaf(a.fy, ry, kv);
-      if (u < 0.0f || u > fW1 || v < 0.0f || v > fH1) continue;
-      const float d = __ldg(a.depth + (uint32_t)(int)v * (uint32_t)a.W + (uint32_t)(int)u) * 0.001f;
-      if (d == 0.0f) continue;
-      const float r2 = fmaf(rx, rx, fmaf(ry, ry, 1.0f));
-      const float diff = (d - pz) * (r2 * rsqrtf(r2));  // sqrt(r2), r2 >= 1
-      if (diff > -a.mu) {
-        const float sdf = fminf(1.0f, diff * a.inv_mu);
-        const V oldv = vf[idx];
-        const Wt oldw = vw[idx];
-        const float F = Vox<S>::raw_nc(&oldv, 0) * Vox<S>::kRawToF;
-        const float w = Vox<S>::weight(&oldw, 0);
-        const float wd = __fdividef(fmaf(w, F, sdf), w + 1.0f);
-        float nF, nw;
-        if (!a.band) {
-          // the reference's earlier update (integrate.cs:115-150)
-          nF = fminf(fmaxf(wd, -1.0f), 1.0f);
-          nw = fminf(w + 1.0f, a.maxw);
-        } else if (wd < 0.2f) {
-          nF = fminf(fmaxf(wd, -0.1f), 0.2f);
-          nw = fminf(w + 1.0f, a.maxw);
-        } else {
-          nF = 0.0f;
-          nw = 0.0f;
-        }
-        const V ev = Vox<S>::encode_value(nF);
-        const Wt ew = Vox<S>::encode_weight(nw);
-        if (bits_of(ev) != bits_of(oldv)) vf[idx] = ev;
-        if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
-        // a non-negative nF never stores a negative value; a brick's first voxel is also
-        // the +1 layer of the brick below it (and, at z % 64 == 0, of the super-brick below)
-        if (nF < 0.0f) {
-          flags |= 1u << jb;
-          if (jj == 0) flags |= (1u << (jb - 1)) | (((zb + k8) & 63) == 0 ? 0xc0u : 0x40u);
-          else flags |= 0x40u;
-        }
+  float px, py, pz;
+  // one voxel of the march (integrate.cs:63-113); jj: its index in the current brick
+  auto voxel = [&](int jj, int jb, int k8) {
+    if (pz < 0.0001f) return;
+    const float iz = __fdividef(1.0f, pz);  // hardware reciprocal (2 ulp)
+    const float rx = px * iz;  // pos.x / pos.z
+    const float ry = py * iz;
+    // cameraX.x / cameraX.z + 0.5 = fx * x/z + cx + 0.5 (K has no skew, :67)
+    const float u = fmaf(a.fx, rx, ku);
+    const float v = fmaf(a.fy, ry, kv);
+    if (u < 0.0f || u > fW1 || v < 0.0f || v > fH1) return;
+    // explicitly rounded: no template instance may fuse the scaling into the subtraction,
+    // so every launch shape computes the same bits
+    const float d = __fmul_rn(__ldg(a.depth + (uint32_t)(int)v * (uint32_t)a.W + (uint32_t)(int)u), 0.001f);
+    if (d == 0.0f) return;
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, 1.0f));
+    const float diff = __fmul_rn(__fsub_rn(d, pz), __fmul_rn(r2, rsqrtf(r2)));  // sqrt(r2), r2 >= 1
+    if (diff > -a.mu) {
+      const float sdf = fminf(1.0f, __fmul_rn(diff, a.inv_mu));
+      const V oldv = vf[idx];
+      const Wt oldw = vw[idx];
+      const float F = __fmul_rn(Vox<S>::raw_nc(&oldv, 0), Vox<S>::kRawToF);
+      const float w = Vox<S>::weight(&oldw, 0);
+      const float wd = __fdividef(fmaf(w, F, sdf), w + 1.0f);
+      float nF, nw;
+      if (!a.band) {
+        // the reference's earlier update (integrate.cs:115-150)
+        nF = fminf(fmaxf(wd, -1.0f), 1.0f);
+        nw = fminf(w + 1.0f, a.maxw);
+      } else if (wd < 0.2f) {
+        nF = fminf(fmaxf(wd, -0.1f), 0.2f);
+        nw = fminf(w + 1.0f, a.maxw);
       } else {
-        vf[idx] = Vox<S>::encode_value(0.0f);
-        vw[idx] = Vox<S>::encode_weight(0.0f);
+        nF = 0.0f;
+        nw = 0.0f;
       }
+      const V ev = Vox<S>::encode_value(nF);
+      const Wt ew = Vox<S>::encode_weight(nw);
+      if (bits_of(ev) != bits_of(oldv)) vf[idx] = ev;
+      if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
+      // a non-negative nF never stores a negative value; a brick's first voxel is also
+      // the +1 layer of the brick below it (and, at z % 64 == 0, of the super-brick below)
+      if (nF < 0.0f) {
+        flags |= 1u << jb;
+        if (jj == 0) flags |= (1u << (jb - 1)) | (((zb + k8) & 63) == 0 ? 0xc0u : 0x40u);
+        else flags |= 0x40u;
+      }
+    } else {
+      vf[idx] = Vox<S>::encode_value(0.0f);
+      vw[idx] = Vox<S>::encode_weight(0.0f);
+    }
+  };
+  // One 8-voxel brick of the column at a time: the position is anchored at the brick's first
+  // voxel and steps by delta inside it, as integrate.cs:57-62 does, so it does not depend on
+  // where a chunk starts.  Whole bricks run unrolled; only a ragged last brick (nz not a
+  // multiple of 8) takes the counted loop.
+  for (int k8 = 0; k8 < zend; k8 += 8) {
+    const float czw = (zb + k8 + 0.5f) * vz;
+    px = fmaf(inv[2], czw, pxy[0]);
+    py = fmaf(inv[6], czw, pxy[1]);
+    pz = fmaf(inv[10], czw, pxy[2]);
+    const int jb = (k8 >> 3) + 1;  // this brick's bit in flags
+    if (k8 + 8 <= zend) {
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj, idx += slice, px += dz[0], py += dz[1], pz += dz[2]) voxel(jj, jb, k8);
+    } else {
+      for (int jj = 0; jj < zend - k8; ++jj, idx += slice, px += dz[0], py += dz[1], pz += dz[2]) voxel(jj, jb, k8);
     }
   }
   return flags;
