@@ -280,10 +280,12 @@ int ensure(kf_session* s, void** p, size_t* cap, size_t bytes) {
 }
 
 // Bytes for the vertex buffer: the vertices needed now, but at least room for one triangle
-// per 256 cubes (a fused scene's surface is about one triangle per 600 cubes), so a mesh
-// that grows as frames are fused rarely reallocates.
+// per 64 cubes (fused scenes reach one triangle per 200-600 cubes), so a mesh that grows as
+// frames are fused does not reallocate: a reallocation frees and allocates device memory,
+// which synchronises the device and takes the driver's locks, whose wait is unbounded on a
+// shared machine.
 size_t vertex_bytes(size_t ncube, size_t nverts) {
-  return std::max<size_t>(16, std::max(nverts, ncube / 256 * 3) * 16);
+  return std::max<size_t>(16, std::max(nverts, ncube / 64 * 3) * 16);
 }
 
 int histopyramid(kf_session* s, float iso, uint32_t* n_tri) {
