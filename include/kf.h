@@ -227,6 +227,17 @@ KF_API int kf_raycast(kf_session* s);   /* raycast(),   gFusion.cpp:1289-1366 */
  * tracked, raycast.  Replayed from a CUDA graph after the first call. */
 KF_API int kf_frame_step_u16(kf_session* s, const uint16_t* host_depth_mm, int* tracked);
 KF_API int kf_frame_step_u16_device(kf_session* s, const uint16_t* device_depth_mm, int* tracked);
+/* Pipelined frame steps: enqueues the upload of this frame (read from host_depth_mm until the
+ * step completes: keep the buffer unchanged until the next call), the frame and a copy of its
+ * result (pose and flags, 144 B), then reads the PREVIOUS asynchronous step's result, waiting
+ * for that step only; the device runs this frame while the caller prepares the next.  The
+ * previous step's error status is this call's return value.  kf_get_last_result returns the
+ * last result read (no wait); kf_frame_sync waits for and reads the step still in flight.
+ * Every synchronous call of the session reads it first.  A session stepped this way is not
+ * put in a batch until kf_frame_sync. */
+KF_API int kf_frame_step_u16_async(kf_session* s, const uint16_t* host_depth_mm);
+KF_API int kf_frame_sync(kf_session* s, int* tracked);
+KF_API int kf_get_last_result(kf_session* s, double pose[16], int* tracked);
 
 /* ---- accessors (getVerts/getNorms/getDepthImage/getVolume/getTrackImage) ------------- */
 KF_API int kf_get_raycast(kf_session* s, float* vertex4, float* normal4);            /* W*H*4 each */

@@ -134,6 +134,9 @@ SIGNATURES = {
     "kf_copy_volume_from_host": (_I, [_P, _P, C.c_uint64]),
     "kf_get_cum_twist": (_I, [_P, _PD]),
     "kf_intensity_projection": (_I, [_P, _P]),
+    "kf_frame_step_u16_async": (_I, [_P, _P]),
+    "kf_frame_sync": (_I, [_P, C.POINTER(_I)]),
+    "kf_get_last_result": (_I, [_P, _PD, C.POINTER(_I)]),
     "kf_set_depth_undistortion": (_I, [_P, C.POINTER(kf_ir_camera)]),
     "kf_get_undistortion_map": (_I, [_P, _P]),
     "kf_set_depth_filter": (_I, [_P, _I]),

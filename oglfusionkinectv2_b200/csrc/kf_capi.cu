@@ -112,6 +112,9 @@ void free_all(kf_session* s) {
   cudaFree(s->d_mip);
   cudaFree(s->d_undistort_map);
   cudaFree(s->d_depth_prep);
+  if (s->h_heads) cudaFreeHost(s->h_heads);
+  for (auto& e : s->head_ev)
+    if (e) cudaEventDestroy(e);
   if (s->h_state) cudaFreeHost(s->h_state);
   if (s->h_depth_pinned) cudaFreeHost(s->h_depth_pinned);
   if (s->h_u32_scalar) cudaFreeHost(s->h_u32_scalar);
@@ -135,7 +138,19 @@ int check_device_error(kf_session* s) {
   return KF_OK;
 }
 
+// Reads the result of the pending asynchronous frame step (waits for that step only) into
+// the host mirror, as a synchronous step would have.
+int finish_async(kf_session* s) {
+  const int p = s->async_pend;
+  if (p < 0) return KF_OK;
+  s->async_pend = -1;
+  KF_CUDA_TRY(s, cudaEventSynchronize(s->head_ev[p]));
+  std::memcpy(s->h_state, s->h_heads + (size_t)p * KF_STATE_RESULT_BYTES, KF_STATE_RESULT_BYTES);
+  return check_device_error(s);
+}
+
 int pull_state(kf_session* s) {
+  if (int rc = finish_async(s)) return rc;
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_state, s->d_state, sizeof(KfDevState), cudaMemcpyDeviceToHost, s->stream));
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return check_device_error(s);
@@ -143,6 +158,7 @@ int pull_state(kf_session* s) {
 
 // pose and result flags only (the per-frame result)
 int pull_state_head(kf_session* s) {
+  if (int rc = finish_async(s)) return rc;
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_state, s->d_state, KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream));
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return check_device_error(s);
@@ -742,6 +758,44 @@ int kf_frame_step_u16(kf_session* s, const uint16_t* host_depth_mm, int* tracked
   int rc = run_frame(s);
   if (rc) return rc;
   return finish_step(s, tracked);
+}
+
+int kf_frame_step_u16_async(kf_session* s, const uint16_t* host_depth_mm) {
+  if (!s || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
+  if (!s->h_heads) {
+    if (cudaMallocHost((void**)&s->h_heads, (size_t)kf_session::kRing * KF_STATE_RESULT_BYTES) != cudaSuccess) {
+      cudaGetLastError();
+      s->h_heads = nullptr;
+      return fail(s, KF_ERR_OUT_OF_MEMORY, "pinned result ring");
+    }
+    for (auto& e : s->head_ev) KF_CUDA_TRY(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->stream));
+  const int slot = (int)(s->frames_run % kf_session::kRing);  // the graph slot run_frame uses
+  int rc = run_frame(s);
+  if (rc) return rc;
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_heads + (size_t)slot * KF_STATE_RESULT_BYTES, s->d_state, KF_STATE_RESULT_BYTES,
+                                 cudaMemcpyDeviceToHost, s->stream));
+  KF_CUDA_TRY(s, cudaEventRecord(s->head_ev[slot], s->stream));
+  // the previous step's result is read now, while this one runs
+  rc = finish_async(s);
+  s->async_pend = slot;
+  return rc;
+}
+
+int kf_frame_sync(kf_session* s, int* tracked) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  int rc = finish_async(s);
+  if (!rc && tracked) *tracked = s->h_state->tracked;
+  return rc;
+}
+
+int kf_get_last_result(kf_session* s, double pose[16], int* tracked) {
+  if (!s) return KF_ERR_INVALID_ARGUMENT;
+  if (pose) std::memcpy(pose, s->h_state->pose, 16 * sizeof(double));
+  if (tracked) *tracked = s->h_state->tracked;
+  return KF_OK;
 }
 
 int kf_frame_step_u16_device(kf_session* s, const uint16_t* device_depth_mm, int* tracked) {

@@ -124,6 +124,11 @@ struct kf_session {
   cudaGraphExec_t frame_exec[kRing] = {};
   cudaEvent_t ring_ev[kRing][6] = {};
   int ring_pending[kRing] = {};  // slot holds an unread frame
+  // asynchronous frame steps (kf_frame_step_u16_async): each step's result head is copied into
+  // the pinned slot of its frame graph and read by the next call
+  char* h_heads = nullptr;            // pinned, kRing * KF_STATE_RESULT_BYTES (first use)
+  cudaEvent_t head_ev[kRing] = {};
+  int async_pend = -1;                // slot of the step whose result is not read yet
   int frame_kernels = 0;         // kernels in one frame graph
   uint64_t frames_run = 0;
   double stage_acc[6] = {0, 0, 0, 0, 0, 0};

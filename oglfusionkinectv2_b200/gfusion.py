@@ -221,6 +221,30 @@ class GFusion:
         self._check(self.lib.kf_frame_step_u16(self._h, d.ctypes.data, C.byref(t)), "kf_frame_step_u16")
         return bool(t.value)
 
+    def frameStepAsync(self, depth_u16) -> None:
+        """Pipelined frame step (kf_frame_step_u16_async): enqueue this frame and read the
+        previous one's result (lastResult()); frameSync() reads the one in flight.  The
+        frame array is kept alive until the next call."""
+        d = np.ascontiguousarray(depth_u16, dtype=np.uint16)
+        if d.shape != (self.intrinsics.height, self.intrinsics.width):
+            raise ValueError(f"depth must be {self.intrinsics.height}x{self.intrinsics.width}")
+        prev = getattr(self, "_async_frames", [])
+        self._check(self.lib.kf_frame_step_u16_async(self._h, d.ctypes.data), "kf_frame_step_u16_async")
+        self._async_frames = (prev + [d])[-2:]  # this frame and the one whose step may still run
+
+    def frameSync(self) -> bool:
+        t = C.c_int()
+        self._check(self.lib.kf_frame_sync(self._h, C.byref(t)), "kf_frame_sync")
+        self._async_frames = []
+        return bool(t.value)
+
+    def lastResult(self):
+        """(pose, tracked) of the last frame result read by the host (no wait)."""
+        a = (C.c_double * 16)()
+        t = C.c_int()
+        self._check(self.lib.kf_get_last_result(self._h, a, C.byref(t)), "kf_get_last_result")
+        return _pose_from_c(a), bool(t.value)
+
     def frameStepDevice(self, device_ptr: int, sync: bool = True):
         t = C.c_int()
         st = self.lib.kf_frame_step_u16_device(self._h, C.c_void_p(device_ptr),

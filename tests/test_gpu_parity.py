@@ -1,6 +1,6 @@
 """GPU (CUDA, through the C ABI) vs FP64 oracle parity on identical inputs.
 
-Tolerances (north star): TSDF max-abs <= 1e-3 of the truncation (normalised units) on
+Tolerances (the parity bar): TSDF max-abs <= 1e-3 of the truncation (normalised units) on
 every voxel whose evaluation is unambiguous; per-frame pose <= 0.1 mm / 0.01 deg with
 teacher forcing; raycast vertex <= 0.5 mm; free-running ATE within 1 mm of the oracle.
 """
@@ -221,6 +221,32 @@ def test_frame_step_graph_matches_step_by_step():
         np.testing.assert_array_equal(a.getPose(), b.getPose())
     np.testing.assert_array_equal(a.getVolumeRaw(), b.getVolumeRaw())
     np.testing.assert_array_equal(a.getVerts(), b.getVerts())
+
+
+def test_async_frame_steps_match_sync_steps():
+    """Pipelined frame steps: each call reads the previous frame's result; the session ends
+    exactly where synchronous steps take it."""
+    w = small_workload(6, size=64)
+    a, b = GFusion(w.config, w.intrinsics), GFusion(w.config, w.intrinsics)
+    for s in (a, b):
+        s.Reset(w.poses[0])
+    sync_res = []
+    for k in range(w.n_frames):
+        t = a.frameStep(w.frame(k))
+        sync_res.append((a.getPose(), t))
+    for k in range(w.n_frames):
+        b.frameStepAsync(w.frame(k))
+        if k > 0:
+            P, t = b.lastResult()
+            np.testing.assert_array_equal(P, sync_res[k - 1][0])
+            assert t == sync_res[k - 1][1]
+    assert b.frameSync() == sync_res[-1][1]
+    np.testing.assert_array_equal(b.lastResult()[0], sync_res[-1][0])
+    np.testing.assert_array_equal(a.getVolumeRaw(), b.getVolumeRaw())
+    np.testing.assert_array_equal(a.getVerts(), b.getVerts())
+    # a synchronous call after an asynchronous one reads the pending result first
+    b.frameStepAsync(w.frame(0))
+    np.testing.assert_array_equal(b.getPose(), b.lastResult()[0])
 
 
 def test_pose_library_and_recover():
