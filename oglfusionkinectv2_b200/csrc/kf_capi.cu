@@ -115,6 +115,11 @@ void free_all(kf_session* s) {
   if (s->h_heads) cudaFreeHost(s->h_heads);
   for (auto& e : s->head_ev)
     if (e) cudaEventDestroy(e);
+  if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+  cudaFree(s->d_frame_ring);
+  for (auto& e : s->upload_ev)
+    if (e) cudaEventDestroy(e);
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   if (s->h_state) cudaFreeHost(s->h_state);
   if (s->h_depth_pinned) cudaFreeHost(s->h_depth_pinned);
   if (s->h_u32_scalar) cudaFreeHost(s->h_u32_scalar);
@@ -222,13 +227,18 @@ int record(kf_session* s, int i) {
   return KF_OK;
 }
 
-// The device part of one frame of kinect.cpp:654-695 (input already in d_depth_u16),
+// The input frame of ring slot `slot` (the frame graph of that slot reads it).
+uint16_t* slot_frame(kf_session* s, int slot) {
+  return s->d_frame_ring + (size_t)slot * s->W[0] * s->H[0];
+}
+
+// The device part of one frame of kinect.cpp:654-695 (input already in the slot's frame),
 // with stage events ev[0..5]: start, pyramid, track, integrate, recover, raycast (event
 // record nodes in the captured graph, so they can be timed after every replay).
-int enqueue_frame(kf_session* s, cudaEvent_t* ev) {
+int enqueue_frame(kf_session* s, cudaEvent_t* ev, int slot) {
   int rc;
   KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[0], s->stream, cudaEventRecordExternal));
-  if ((rc = kf_launch_depth_ingest(s, s->d_depth_u16, nullptr))) return rc;
+  if ((rc = kf_launch_depth_ingest(s, slot_frame(s, slot), nullptr))) return rc;
   if ((rc = kf_launch_vertex_normal(s))) return rc;
   KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[1], s->stream, cudaEventRecordExternal));
   if (s->cfg.tracking == KF_TRACK_SDF) {
@@ -293,7 +303,7 @@ int run_frame(kf_session* s) {
     cudaGraph_t g = nullptr;
     KF_CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     s->capturing = true;
-    int rc = enqueue_frame(s, s->ring_ev[slot]);
+    int rc = enqueue_frame(s, s->ring_ev[slot], slot);
     s->capturing = false;
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
     if (rc) {
@@ -478,7 +488,7 @@ int kf_session_device_bytes(const kf_config* cfg, const kf_intrinsics* in, uint6
        ((cfg->nz + KF_BRICK - 1) / KF_BRICK) * 4 +
        (uint64_t)((cfg->nx + KF_SUPER - 1) / KF_SUPER) * ((cfg->ny + KF_SUPER - 1) / KF_SUPER) *
        ((cfg->nz + KF_SUPER - 1) / KF_SUPER) * 4;  // brick and super-brick flags
-  b += px * (2 + 4);                       // staging
+  b += px * (2 + 4) + px * 2 * kf_session::kRing;  // staging, and the frame graphs' inputs
   b += px * (4 + 16 + 16 + 4) * 2;         // three levels (sum < 4/3 of level 0)
   b += px * 32;                            // raycast maps
   b += px * 32;                            // sdf rows
@@ -523,6 +533,7 @@ int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out)
   const size_t px = (size_t)s->W[0] * s->H[0];
   if ((rc = alloc_volume(s))) return bail(rc);
   if ((rc = dalloc(s, &s->d_depth_u16, px))) return bail(rc);
+  if ((rc = dalloc(s, &s->d_frame_ring, px * kf_session::kRing))) return bail(rc);
   if ((rc = dalloc(s, &s->d_depth_f32_in, px))) return bail(rc);
   for (int l = 0; l < 3; ++l) {
     const size_t n = (size_t)s->W[l] * s->H[l];
@@ -754,7 +765,8 @@ int kf_raycast(kf_session* s) {
 int kf_frame_step_u16(kf_session* s, const uint16_t* host_depth_mm, int* tracked) {
   if (!s || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
   const size_t px = (size_t)s->W[0] * s->H[0];
-  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->stream));
+  const int slot = (int)(s->frames_run % kf_session::kRing);  // the graph slot run_frame uses
+  KF_CUDA_TRY(s, cudaMemcpyAsync(slot_frame(s, slot), host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->stream));
   int rc = run_frame(s);
   if (rc) return rc;
   return finish_step(s, tracked);
@@ -769,10 +781,18 @@ int kf_frame_step_u16_async(kf_session* s, const uint16_t* host_depth_mm) {
       return fail(s, KF_ERR_OUT_OF_MEMORY, "pinned result ring");
     }
     for (auto& e : s->head_ev) KF_CUDA_TRY(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : s->upload_ev) KF_CUDA_TRY(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    KF_CUDA_TRY(s, cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
   }
   const size_t px = (size_t)s->W[0] * s->H[0];
-  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->stream));
   const int slot = (int)(s->frames_run % kf_session::kRing);  // the graph slot run_frame uses
+  // the upload overlaps the frame still running: it goes on the copy stream once the last
+  // frame of this slot has read its input (the slot's pyramid-stage event), and the frame
+  // waits for it
+  if (s->ring_ev[slot][1]) KF_CUDA_TRY(s, cudaStreamWaitEvent(s->copy_stream, s->ring_ev[slot][1], 0));
+  KF_CUDA_TRY(s, cudaMemcpyAsync(slot_frame(s, slot), host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->copy_stream));
+  KF_CUDA_TRY(s, cudaEventRecord(s->upload_ev[slot], s->copy_stream));
+  KF_CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->upload_ev[slot], 0));
   int rc = run_frame(s);
   if (rc) return rc;
   KF_CUDA_TRY(s, cudaMemcpyAsync(s->h_heads + (size_t)slot * KF_STATE_RESULT_BYTES, s->d_state, KF_STATE_RESULT_BYTES,
@@ -801,7 +821,8 @@ int kf_get_last_result(kf_session* s, double pose[16], int* tracked) {
 int kf_frame_step_u16_device(kf_session* s, const uint16_t* device_depth_mm, int* tracked) {
   if (!s || !device_depth_mm) return KF_ERR_INVALID_ARGUMENT;
   const size_t px = (size_t)s->W[0] * s->H[0];
-  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_depth_u16, device_depth_mm, px * 2, cudaMemcpyDeviceToDevice, s->stream));
+  const int slot = (int)(s->frames_run % kf_session::kRing);  // the graph slot run_frame uses
+  KF_CUDA_TRY(s, cudaMemcpyAsync(slot_frame(s, slot), device_depth_mm, px * 2, cudaMemcpyDeviceToDevice, s->stream));
   int rc = run_frame(s);
   if (rc) return rc;
   return finish_step(s, tracked);

@@ -129,6 +129,11 @@ struct kf_session {
   char* h_heads = nullptr;            // pinned, kRing * KF_STATE_RESULT_BYTES (first use)
   cudaEvent_t head_ev[kRing] = {};
   int async_pend = -1;                // slot of the step whose result is not read yet
+  // the frame graphs' inputs: one staging frame per ring slot (slot k's graph reads frame
+  // k), so a pipelined step can upload the next frame on copy_stream while one runs
+  uint16_t* d_frame_ring = nullptr;   // kRing * W * H
+  cudaStream_t copy_stream = nullptr; // created by the first pipelined step
+  cudaEvent_t upload_ev[kRing] = {};
   int frame_kernels = 0;         // kernels in one frame graph
   uint64_t frames_run = 0;
   double stage_acc[6] = {0, 0, 0, 0, 0, 0};
