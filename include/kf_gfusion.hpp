@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "kf.h"
@@ -101,6 +102,29 @@ class GFusion {
     int t = 0;
     check(kf_frame_step_u16(s_, depthMm, &t), "kf_frame_step_u16");
     return t != 0;
+  }
+  // pipelined loop body: enqueues this frame (depthMm must stay unchanged until the next
+  // call) and reads the previous frame's result, returned by lastResult(); frameSync()
+  // reads the frame still in flight
+  void frameStepAsync(const uint16_t* depthMm) {
+    check(kf_frame_step_u16_async(s_, depthMm), "kf_frame_step_u16_async");
+  }
+  bool frameSync() {
+    int t = 0;
+    check(kf_frame_sync(s_, &t), "kf_frame_sync");
+    return t != 0;
+  }
+  std::pair<Pose, bool> lastResult() {
+    Pose p;
+    int t = 0;
+    check(kf_get_last_result(s_, p.data(), &t), "kf_get_last_result");
+    return {p, t != 0};
+  }
+  // launch shapes for this volume and GPU (results do not depend on them)
+  kf_launch_shape autotune(int repeats = 5) {
+    kf_launch_shape sh{};
+    check(kf_autotune(s_, repeats, &sh, nullptr), "kf_autotune");
+    return sh;
   }
 
   // ---- accessors (the reference returns GL names; these return data) ----
