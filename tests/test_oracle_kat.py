@@ -353,6 +353,25 @@ def test_intensity_projection_constant_volume(value):
         assert counts[cy, cx] == np.ceil(1.0 / (0.75 * c.mu))
 
 
+def test_intensity_projection_rg16i_scale():
+    """On the reference's RG16I volume a stored short s reads as s * 0.00003051944088
+    (mip.cs:39-49, 1/32766): a constant short of 16383 sums to 16383/32766 per sample."""
+    c = cfg(size=32, dim=1.0, mu=0.05, storage=L.KF_STORAGE_RG16I)
+    o = O.Oracle(c, INTR)
+    pose = np.eye(4)
+    pose[:3, 3] = [0.5, 0.5, -0.2]
+    o.Reset(pose)
+    n = 32 ** 3
+    raw = np.concatenate([np.full(n, 16383, np.int16), np.ones(n, np.int16)])
+    o.setVolumeRaw(raw.view(np.uint8))
+    m = o.intensityProjection()
+    counts, on_step = _mip_sample_counts(c, pose, 0.75 * c.mu)
+    want = counts * 16383 * 0.00003051944088
+    err = np.abs(m[..., 0] - want)
+    assert (counts > 0).mean() > 0.3
+    assert np.all(err[~on_step] <= 1e-6 * np.maximum(1.0, want[~on_step]))
+
+
 # ---- ICP (track.cs / reduce.cs / Track) ---------------------------------------------
 def test_icp_recovers_small_motion_on_same_frame():
     from oglfusionkinectv2_b200 import synth
