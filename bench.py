@@ -47,6 +47,10 @@ def parse():
     p.add_argument("--cpu-frames", type=int, default=4, help="oracle frames timed for cpu_baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-reference-quirks", action="store_true",
+                   help="skip the pass with the reference's own quirk set")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the batched and served sub-records of the default line")
     p.add_argument("--form", choices=["plain", "batched", "served", "large"], default="plain",
                    help="plain: the single-session frame step (default line); batched: config 3; "
                         "served: config 4; large: config 5")
@@ -108,7 +112,18 @@ class ClockSampler:
                 except Exception:
                     self._h = None
             if self._h is None:
-                self._h = N.nvmlDeviceGetHandleByIndex(0)
+                # by PCI address (NVML indices ignore CUDA_VISIBLE_DEVICES)
+                bus = getattr(props, "pci_bus_id", None)
+                dom = getattr(props, "pci_domain_id", 0) or 0
+                dv = getattr(props, "pci_device_id", 0) or 0
+                if bus is not None:
+                    try:
+                        self._h = N.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dv:02x}.0".encode())
+                    except Exception:
+                        self._h = None
+            if self._h is None:
+                self.error = "nvml device not matched (no UUID or PCI bus id match)"
+                return
             self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self._h, N.NVML_CLOCK_SM)
         except Exception as e:  # NVML unavailable: report what we could not sample
             self.error = str(e)
@@ -139,7 +154,8 @@ class ClockSampler:
 
     def summary(self):
         if self._h is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None,
+                    "reasons": [getattr(self, "error", None) or "nvml unavailable"]}
         s = sorted(self.samples)
         return {"sm_mhz": s[len(s) // 2] if s else None, "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(self.reasons), "samples": len(s)}
@@ -179,26 +195,73 @@ def algorithmic_bytes(cfg, stage):
     raise ValueError(stage)
 
 
+CPU_WARM_FRAMES = 2  # untimed oracle frames before the timed cpu_baseline sample
+
+
 def cpu_baseline(args, w, frames_by_idx):
-    """Time the FP64 oracle (CPU port of the reference algorithm) on a bounded sample."""
+    """Time the FP64 oracle (CPU port of the reference algorithm) on a bounded sample: frames
+    0 .. CPU_WARM_FRAMES + cpu_frames - 1 of the sequence from the first ground-truth pose.
+    Returns the baseline record, the oracle's pose after every frame, and the oracle's final
+    volume (raw bytes) for the accuracy comparison."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import kf_oracle as O
     O.Oracle.set_threads(0)
     o = O.Oracle(w.config, w.intrinsics)
     o.Reset(w.poses[0])
-    warm = 2
+    warm = CPU_WARM_FRAMES
     n = max(1, args.cpu_frames)
+    poses = []
     for i in range(warm):
         o.frameStep(frames_by_idx[i])
+        poses.append(o.getPose())
     t0 = time.perf_counter()
     for i in range(warm, warm + n):
         o.frameStep(frames_by_idx[i])
+        poses.append(o.getPose())
     dt = time.perf_counter() - t0
     cores = O.Oracle.threads()
+    vol = o.getVolumeRaw()
     o.close()
-    return {"value": n / dt, "unit": "frames/s", "cores": cores, "kind": "port",
-            "sample": f"frames {warm}-{warm + n - 1} of the same {w.config.volumeSize[0]}^3 sequence "
-                      f"after {warm} untimed frames (FP64 oracle, OpenMP, {cores} threads)"}
+    rec = {"value": n / dt, "unit": "frames/s", "cores": cores, "kind": "port",
+           "sample": f"frames {warm}-{warm + n - 1} of the same {w.config.volumeSize[0]}^3 sequence "
+                     f"after {warm} untimed frames (FP64 oracle, OpenMP, {cores} threads)"}
+    return rec, poses, vol
+
+
+def tsdf_error(raw_gpu, raw_oracle, cfg):
+    """TSDF value error (in units of the truncation mu: values are stored divided by mu)
+    between two raw volumes, over the voxels either side has touched."""
+    from oglfusionkinectv2_b200.gfusion import decode_volume
+    Fg, Wg = decode_volume(raw_gpu, cfg)
+    Fo, Wo = decode_volume(raw_oracle, cfg)
+    touched = (Wg > 0) | (Wo > 0)
+    d = np.abs(Fg - Fo)[touched]
+    n = int(touched.sum())
+    return {"voxels_touched": n,
+            "max_abs": float(d.max()) if n else 0.0,
+            "p99_99_abs": float(np.percentile(d, 99.99)) if n else 0.0,
+            "frac_above_1e-3": float(np.mean(d > 1e-3)) if n else 0.0,
+            "weight_mismatch_frac": float(np.mean((Wg != Wo)[touched])) if n else 0.0,
+            "unit": "TSDF value (fraction of mu)"}
+
+
+def accuracy_pass(w, base, fbytes, n_steps, prefix, final_pose_ref):
+    """A second session steps frames 0 .. n_steps-1 from the first ground-truth pose, one
+    synchronous frame at a time (every computation is deterministic, so it retraces the timed
+    session: its pose after the last frame is compared with the timed session's, bit for
+    bit).  Returns its per-frame poses and its raw volume after `prefix` frames."""
+    from oglfusionkinectv2_b200 import GFusion
+    ga = GFusion(w.config, w.intrinsics)
+    ga.Reset(w.poses[0])
+    poses, vol_prefix = [], None
+    for i in range(n_steps):
+        ga.frameStepDevice(base + i * fbytes)
+        poses.append(ga.getPose())
+        if i + 1 == prefix:
+            vol_prefix = ga.getVolumeRaw()
+    same = bool(np.array_equal(poses[-1], final_pose_ref)) if final_pose_ref is not None else None
+    ga.close()
+    return poses, vol_prefix, same
 
 
 def rmse_translation(est, gt) -> float:
@@ -206,12 +269,14 @@ def rmse_translation(est, gt) -> float:
     return float(np.sqrt(np.mean(d * d))) if len(d) else 0.0
 
 
-def run_batched(args):
+def run_batched(args, sub=False):
     """Config 3: sessions of uneven volume sizes stepped together (one launch per stage),
-    against the same sessions stepped one at a time through the single-session path."""
+    against the same sessions stepped one at a time through the single-session path.
+    sub: a bounded pass (20 steps after 5 warm-up steps) whose record is returned for the
+    default line instead of printed."""
     import torch
     from oglfusionkinectv2_b200 import GFusion, GFusionBatch, synth
-    K, W = args.steps, max(3, args.warmup)
+    K, W = (20, 5) if sub else (args.steps, max(3, args.warmup))
     K_plain = min(K, 20)
     n_frames = W + K + 2 + K_plain
     ws = synth.batched_c3(args.sessions, n_frames=n_frames)
@@ -320,6 +385,13 @@ def run_batched(args):
                                          "ratio_batched_over_plain": value / (len(ws) * K_plain / plain32_wall)},
             "ate_mm": {"mean": 1000 * float(np.mean(ate)), "max": 1000 * float(np.max(ate))},
             "gpu_launches": launches, "clocks": clk.summary()}
+    for g in gs:
+        g.close()
+    batch.close()
+    del frames
+    torch.cuda.empty_cache()
+    if sub:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 
@@ -436,18 +508,20 @@ def serve_pass(server, arrivals, seqs, gt, duration, fbytes, max_slots):
     return frames, admitted, max_wait, errs_all
 
 
-def run_served(args):
+def run_served(args, sub=False):
     """Config 4: Poisson session arrivals, 30 Hz frame streams, admission by slots and free
     device memory, continuous batching; against the same arrival process stepped one
-    session at a time."""
+    session at a time.  sub: a bounded pass (10 s of arrivals) whose record is returned for
+    the default line instead of printed."""
     import torch
     from oglfusionkinectv2_b200 import GFusionServer, synth
     torch.cuda.set_device(0)
+    duration = 10.0 if sub else args.duration
     n_scenes, L_seq = 16, 300
-    arrivals = synth.served_c4(args.duration, n_scenes=n_scenes)
+    arrivals = synth.served_c4(duration, n_scenes=n_scenes)
     scenes = [synth.session_scene(L_seq, splitmix(0xC0FFEE + 4000 + k), 128, phase_deg=22.5 * k,
                                   deg_per_frame=0.5 if k % 2 else -0.5) for k in range(n_scenes)]
-    log(f"rendering {n_scenes} x {L_seq} frames on the device; {len(arrivals)} arrivals in {args.duration} s")
+    log(f"rendering {n_scenes} x {L_seq} frames on the device; {len(arrivals)} arrivals in {duration} s")
     seqs = [w.frames_torch(range(L_seq), "cuda") for w in scenes]
     torch.cuda.synchronize()
     gt = [(w.poses, w.config, w.intrinsics) for w in scenes]
@@ -464,13 +538,13 @@ def run_served(args):
             cfg.volumeSize = (z, z, z)
             server.prewarm(cfg, gt[0][2], per)
         with ClockSampler(0) as clk:
-            frames, admitted, max_wait, errs = serve_pass(server, arrivals, seqs, gt, args.duration, fbytes, slots)
+            frames, admitted, max_wait, errs = serve_pass(server, arrivals, seqs, gt, duration, fbytes, slots)
         st = server.stats()
         server.close()
         flat = [e for es in errs for e in es]
-        results[name] = {"frames_per_s": frames / args.duration, "frames": frames, "p50_ms": st["p50_ms"],
+        results[name] = {"frames_per_s": frames / duration, "frames": frames, "p50_ms": st["p50_ms"],
                          "p99_ms": st["p99_ms"], "max_ms": st["max_ms"], "sessions_admitted": admitted,
-                         "max_admission_wait_s": max_wait, "busy_fraction": st["busy_s"] / args.duration,
+                         "max_admission_wait_s": max_wait, "busy_fraction": st["busy_s"] / duration,
                          "pose_err_mm": {"median": 1000 * float(np.median(flat)) if flat else None,
                                          "p99": 1000 * float(np.percentile(flat, 99)) if flat else None},
                          "clocks": clk.summary()}
@@ -481,13 +555,17 @@ def run_served(args):
             "ms_per_step": 1000.0 / sv["frames_per_s"] if sv["frames_per_s"] else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "c4_served", "duration_s": args.duration, "arrivals": len(arrivals),
+            "config": {"workload": "c4_served", "duration_s": duration, "arrivals": len(arrivals),
                        "slots": slots, "max_batch": batch_max, "storage": "f16u16", "jtj": "bf16",
                        "warm_pool": "sessions of every volume size created before the arrivals",
                        "scenes": f"{n_scenes} seeded sequences of {L_seq} frames, replayed back and forth"},
             "latency_ms": {"p50": sv["p50_ms"], "p99": sv["p99_ms"], "max": sv["max_ms"]},
             "served": sv, "plain_one_at_a_time": pl,
             "ratio_served_over_plain": sv["frames_per_s"] / pl["frames_per_s"] if pl["frames_per_s"] else None}
+    del seqs
+    torch.cuda.empty_cache()
+    if sub:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 
@@ -580,7 +658,8 @@ def main():
     # graphs, so at least five warm-up frames
     K, W = args.steps, max(3 if args.no_autotune else 5, args.warmup)
     n_e2e = 0 if args.no_e2e else K
-    n_frames = W + K + n_e2e + 1
+    n_lat = 0 if args.no_e2e else max(K, 50)
+    n_frames = W + K + n_e2e + 1 + n_lat
     w = workload(args, n_frames)
     ncpu = os.cpu_count() or 1
     log(f"rendering {n_frames} frames")
@@ -594,6 +673,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     from oglfusionkinectv2_b200 import GFusion, MCubes, _lib as L
+    import ctypes as C
 
     g = GFusion(w.config, w.intrinsics)
     g.Reset(w.poses[0])
@@ -622,8 +702,11 @@ def main():
             # untouched); the following warm-up frames capture the frame graphs with them
             shape, tms = g.autotune(repeats=5)
             tuned = {"integrate_z_chunk": shape[0], "raycast_rows": shape[1], "candidates_ms": tms}
+    mc_warm_ms = None
     if w.mc_every:
         mc.generateMarchingCubes(L.KF_MC_HISTOPYRAMID)  # first extraction allocates its buffers
+        mc.generateMarchingCubes(L.KF_MC_HISTOPYRAMID)  # a warm one, timed on the device
+        mc_warm_ms = float(g.getTimes()[5])
     torch.cuda.synchronize()
     log("warm-up done")
     if world > 1:
@@ -643,17 +726,19 @@ def main():
     log(f"timed pass {dev_ms:.1f} ms")
     launches = g.launchCount() - launches0
     stage_mean, stage_frames = g.stageStats()
+    pose_timed_last = g.getPose()                 # after frame W + K - 1
     tracked_ok = g.frameStepDevice(base + (W + K) * fbytes)  # a synchronised step: state readable
 
-    # end to end: pinned host frames through kf_frame_step_u16 (H2D frame + D2H pose/flags)
+    # end to end: pinned host frames through kf_frame_step_u16_async (H2D frame + D2H
+    # pose/flags); each call's result is the previous frame's pose
     e2e = None
+    e2e_poses = []
+    lib = L.load()
+    t = C.c_int()
     if n_e2e:
-        pinned = torch.empty((n_e2e, 424, 512), dtype=torch.int16).pin_memory()
-        pinned.copy_(torch.from_numpy(stack[W + K + 1:W + K + 1 + n_e2e]))
+        pinned = torch.empty((n_e2e + n_lat, 424, 512), dtype=torch.int16).pin_memory()
+        pinned.copy_(torch.from_numpy(stack[W + K + 1:W + K + 1 + n_e2e + n_lat]))
         hp = pinned.data_ptr()
-        lib = L.load()
-        import ctypes as C
-        t = C.c_int()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -669,6 +754,7 @@ def main():
                 raise L.KfError(st, "kf_frame_step_u16_async")
             if i:
                 lib.kf_get_last_result(g.handle, pose, C.byref(t))
+                e2e_poses.append(np.array(pose[:]))
             maybe_mc(i)
         st = lib.kf_frame_sync(g.handle, C.byref(t))
         if st:
@@ -676,9 +762,25 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+        lib.kf_get_last_result(g.handle, pose, C.byref(t))
+        e2e_poses.append(np.array(pose[:]))
         e2e_ms = e0.elapsed_time(e1)
         log(f"e2e pass {e2e_ms:.1f} ms")
         e2e = {"ms": e2e_ms, "wall_s": wall}
+
+        # frame latency: synchronous steps from pinned host frames, the host clock from the
+        # call to the frame's pose on the host (the session continues the same sequence)
+        lat_ms = []
+        for i in range(n_e2e, n_e2e + n_lat):
+            t1 = time.perf_counter()
+            st = lib.kf_frame_step_u16(g.handle, C.c_void_p(hp + i * fbytes), C.byref(t))
+            lib.kf_get_pose(g.handle, pose)
+            lat_ms.append(1000 * (time.perf_counter() - t1))
+            if st:
+                raise L.KfError(st, "kf_frame_step_u16")
+        e2e["latency_ms"] = {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
+                             "max": float(np.max(lat_ms)), "frames": n_lat,
+                             "from": "kf_frame_step_u16 call (pinned host frame) to the frame's pose on the host"}
 
     # max over ranks of the timed durations
     dev_ms_max, e2e_ms_max = max_over_ranks([dev_ms, e2e["ms"] if e2e else 0.0], world, "cuda")
@@ -710,22 +812,85 @@ def main():
             "clocks": clk.summary(),
             "tracked_last": bool(tracked_ok),
         }
+        if mc_warm_ms is not None:
+            # marching cubes every mc_every frames, amortised over the frames between extractions
+            out["mc_every"] = w.mc_every
+            out["mc_warm_ms"] = mc_warm_ms
+            out["ms_per_step_with_mc"] = dev_ms_max / K + mc_warm_ms / w.mc_every
         if e2e:
             out["e2e"] = {"value": world * n_e2e / (e2e_ms_max / 1000.0), "unit": "frames/s",
                           "h2d_bytes_per_step": fbytes, "d2h_bytes_per_step": 144,
                           "wall_frames_per_s": n_e2e / e2e["wall_s"],
                           "api": "kf_frame_step_u16_async from pinned host frames, each call reading "
-                                 "the previous frame's pose and flags"}
+                                 "the previous frame's pose and flags",
+                          "latency_ms": e2e["latency_ms"]}
     g.close()
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
-        log("cpu baseline")
-        out["cpu_baseline"] = cpu_baseline(args, w, frames)
+
+    if rank == 0 and world == 1 and not args.no_reference_quirks:
+        out["reference_quirks"] = reference_quirks_pass(w, base, fbytes, W, K)
+    if rank == 0 and world == 1:
+        # accuracy: ground truth over the timed frames (a deterministic re-run of the same
+        # frames) and over the end-to-end frames (that pass's own results); the FP64 oracle
+        # over the cpu_baseline prefix, poses and TSDF
+        prefix = CPU_WARM_FRAMES + max(1, args.cpu_frames)
+        log("accuracy pass")
+        acc_poses, vol_prefix, same = accuracy_pass(w, base, fbytes, W + K, prefix, pose_timed_last)
+        acc = {"ate_vs_ground_truth_mm": {
+                   "timed_frames": 1000 * rmse_translation(acc_poses[W:W + K], w.poses[W:W + K]),
+                   "all_frames_to_timed_end": 1000 * rmse_translation(acc_poses, w.poses[:W + K]),
+                   "rerun_matches_timed_session": same}}
+        if e2e_poses:
+            e2e_gt = w.poses[W + K + 1:W + K + 1 + len(e2e_poses)]
+            acc["ate_vs_ground_truth_mm"]["e2e_frames"] = 1000 * rmse_translation(e2e_poses, e2e_gt)
+        if not args.no_cpu_baseline:
+            log("cpu baseline")
+            out["cpu_baseline"], o_poses, o_vol = cpu_baseline(args, w, frames)
+            n = len(o_poses)
+            acc["vs_fp64_oracle"] = {
+                "frames": f"0-{n - 1} (the cpu_baseline frames, same start pose)",
+                "ate_mm": 1000 * rmse_translation(acc_poses[:n], o_poses),
+                "max_translation_diff_mm": 1000 * max(float(np.linalg.norm(a[:3, 3] - b[:3, 3]))
+                                                      for a, b in zip(acc_poses[:n], o_poses)),
+                "tsdf_after_prefix": tsdf_error(vol_prefix, o_vol, w.config)}
+        out["accuracy"] = acc
+    if rank == 0 and world == 1 and not args.no_forms:
+        log("batched form")
+        out["batched"] = run_batched(args, sub=True)
+        log("served form")
+        out["served"] = run_served(args, sub=True)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def reference_quirks_pass(w, base, fbytes, W, K):
+    """The same frames with the reference's own behaviour (every quirk bit set: same-pixel
+    ICP association and the narrow TSDF band among them), timed like the main pass."""
+    import torch
+    from oglfusionkinectv2_b200 import GFusion, _lib as L
+    c = w.config
+    cq = type(c)(**{**c.__dict__, "quirks": L.KF_QUIRKS_REFERENCE})
+    g = GFusion(cq, w.intrinsics)
+    g.Reset(w.poses[0])
+    for i in range(W):
+        g.frameStepDevice(base + i * fbytes, sync=False)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(W, W + K):
+        g.frameStepDevice(base + i * fbytes, sync=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    P = g.getPose()
+    g.close()
+    return {"value": K / (ms / 1000.0), "unit": "frames/s", "ms_per_step": ms / K,
+            "quirks": hex(L.KF_QUIRKS_REFERENCE), "steps": K,
+            "translation_error_last_frame_mm": 1000 * float(np.linalg.norm(P[:3, 3] - w.poses[W + K - 1][:3, 3]))}
 
 
 if __name__ == "__main__":

@@ -231,7 +231,10 @@ KF_API int kf_frame_step_u16_device(kf_session* s, const uint16_t* device_depth_
  * step completes: keep the buffer unchanged until the next call), the frame and a copy of its
  * result (pose and flags, 144 B), then reads the PREVIOUS asynchronous step's result, waiting
  * for that step only; the device runs this frame while the caller prepares the next.  The
- * previous step's error status is this call's return value.  kf_get_last_result returns the
+ * previous step's error status is this call's return value: when that is not KF_OK, THIS
+ * frame has still been enqueued and will be stepped, so a caller must not submit it again
+ * (a failure to enqueue, e.g. KF_ERR_INVALID_ARGUMENT, is returned before anything is
+ * enqueued and leaves the previous step unread).  kf_get_last_result returns the
  * last result read (no wait); kf_frame_sync waits for and reads the step still in flight.
  * Every synchronous call of the session reads it first.  A session stepped this way is not
  * put in a batch until kf_frame_sync. */
@@ -241,6 +244,12 @@ KF_API int kf_get_last_result(kf_session* s, double pose[16], int* tracked);
 
 /* ---- accessors (getVerts/getNorms/getDepthImage/getVolume/getTrackImage) ------------- */
 KF_API int kf_get_raycast(kf_session* s, float* vertex4, float* normal4);            /* W*H*4 each */
+/* Replace the maps Track() associates against (m_textureReferenceVertex/Normal, written by
+ * raycast(), gFusion.cpp:1289-1366) with the caller's W*H*4 world-frame vertex and normal
+ * maps (w = 1 where valid, 0 elsewhere), e.g. a model rendered elsewhere; the pose they were
+ * made from stays the last raycast's.  No counterpart in the reference, which tracks only
+ * against its own raycast. */
+KF_API int kf_set_reference_maps(kf_session* s, const float* vertex4, const float* normal4);
 KF_API int kf_get_vertex_map(kf_session* s, int level, float* vertex4);
 KF_API int kf_get_normal_map(kf_session* s, int level, float* normal4);
 KF_API int kf_get_depth_map(kf_session* s, int level, float* depth_mm);
@@ -430,9 +439,10 @@ KF_API int kf_prefix_sum_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, 
  * kf_prefix_sum_u32; the scratch is a 262,220-byte array compiled into the library,
  * which every GPU that loads the library keeps until the process exits.
  *   - n may be at most 2^28 (268,435,456) elements; larger n returns KF_ERR_CAPACITY.
- *   - The first call on a device looks up the array's device address (a host-side step,
- *     done once per device with that device current); make that first call before any
- *     stream capture on the device.
+ *   - The first call in a CUDA context looks up the array's device address (a host-side
+ *     step, done once per context with that context current, and again in every new
+ *     context: a primary context re-created after cudaDeviceReset, or one a framework
+ *     made with cuCtxCreate); make that first call before any stream capture.
  *   - All calls on a device share the one array: calls whose work overlaps on the GPU
  *     (different streams, or host threads) race and corrupt each other's results.
  *     Serialise them, e.g. on one stream.

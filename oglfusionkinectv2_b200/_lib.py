@@ -125,6 +125,7 @@ SIGNATURES = {
     "kf_frame_step_u16": (_I, [_P, _P, C.POINTER(_I)]),
     "kf_frame_step_u16_device": (_I, [_P, _P, C.POINTER(_I)]),
     "kf_get_raycast": (_I, [_P, _P, _P]),
+    "kf_set_reference_maps": (_I, [_P, _P, _P]),
     "kf_get_vertex_map": (_I, [_P, _I, _P]),
     "kf_get_normal_map": (_I, [_P, _I, _P]),
     "kf_get_depth_map": (_I, [_P, _I, _P]),

@@ -9,6 +9,12 @@ checkout at build time and writes them, in this project's own format, to
 csrc/generated/kf_mc_tables.inc (git-ignored; it ships beside the built libraries).
 
 Usage: python gen_mc_tables.py [path/to/tables.h] [out.inc]
+
+The reference's tables.h is looked for, in order, at: the first argument; $KF_MC_TABLES_H
+(a path to tables.h); $KF_REFERENCE_DIR/include/tables.h (a checkout of the reference);
+baseline/_ref/include/tables.h under the repository root; include/tables.h of a checkout
+named `reference` beside the repository.  When none exists, a previously generated
+header is kept; with neither, the script stops with an error naming these places.
 """
 from __future__ import annotations
 
@@ -17,8 +23,20 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/include/tables.h"
+REPO = os.path.dirname(os.path.dirname(HERE))
 DEFAULT_OUT = os.path.join(HERE, "generated", "kf_mc_tables.inc")
+
+
+def candidate_sources() -> list[str]:
+    """Where the reference's tables.h may be, in the order they are tried."""
+    c = []
+    if os.environ.get("KF_MC_TABLES_H"):
+        c.append(os.environ["KF_MC_TABLES_H"])
+    if os.environ.get("KF_REFERENCE_DIR"):
+        c.append(os.path.join(os.environ["KF_REFERENCE_DIR"], "include", "tables.h"))
+    c.append(os.path.join(REPO, "baseline", "_ref", "include", "tables.h"))
+    c.append(os.path.join(os.path.dirname(REPO), "reference", "include", "tables.h"))
+    return c
 
 
 def _array_body(text: str, name: str) -> str:
@@ -101,13 +119,16 @@ def emit(t: dict[str, list[int]], out: str) -> None:
 
 
 def main(argv: list[str]) -> int:
-    src = argv[1] if len(argv) > 1 else DEFAULT_SRC
+    tried = [argv[1]] if len(argv) > 1 else candidate_sources()
     out = argv[2] if len(argv) > 2 else DEFAULT_OUT
-    if not os.path.exists(src):
+    src = next((p for p in tried if os.path.exists(p)), None)
+    if src is None:
         if os.path.exists(out):
-            print(f"gen_mc_tables: {src} absent; keeping existing {out}")
+            print(f"gen_mc_tables: no tables.h found; keeping existing {out}")
             return 0
-        print(f"gen_mc_tables: neither {src} nor a previously generated {out} exists",
+        print("gen_mc_tables: the reference's include/tables.h was not found (tried: "
+              + ", ".join(tried) + ") and no previously generated " + out + " exists; "
+              "pass its path as the first argument or set KF_MC_TABLES_H or KF_REFERENCE_DIR",
               file=sys.stderr)
         return 1
     emit(parse(src), out)

@@ -843,6 +843,16 @@ int kf_get_raycast(kf_session* s, float* v, float* n) {
   return rc;
 }
 
+int kf_set_reference_maps(kf_session* s, const float* v, const float* n) {
+  if (!s || !v || !n) return KF_ERR_INVALID_ARGUMENT;
+  if (int rc = finish_async(s)) return rc;
+  const size_t px = (size_t)s->W[0] * s->H[0];
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_ref_vertex, v, px * 16, cudaMemcpyHostToDevice, s->stream));
+  KF_CUDA_TRY(s, cudaMemcpyAsync(s->d_ref_normal, n, px * 16, cudaMemcpyHostToDevice, s->stream));
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return KF_OK;
+}
+
 int kf_get_vertex_map(kf_session* s, int level, float* v) {
   if (!s || !v || level < 0 || level > 2) return KF_ERR_INVALID_ARGUMENT;
   return copy_out(s, v, s->d_vertex[level], (size_t)s->W[level] * s->H[level] * 16);

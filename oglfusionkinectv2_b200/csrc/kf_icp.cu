@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
   __shared__ long long s_fix[JTJ ? kWarps : 1][72];
   __shared__ double s_sums[32];
   __shared__ double s_csums[29], s_ccenter[3], s_ae;  // last centred row (for the tail)
+  __shared__ double s_gx[6];                            // the rank-guarded step (rare path)
   __shared__ int s_flag, s_conv;
   __shared__ __align__(16) __nv_bfloat16 s_hi[JTJ ? kWarps : 1][8][40];
   __shared__ __align__(16) __nv_bfloat16 s_mid[JTJ ? kWarps : 1][8][40];
@@ -431,15 +432,11 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
         // reduce.cs counts every pixel of the (group-7) rows in sums[28]
         const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
         const double nvalid = s_sums[28];
-        const double cx = s_cd[0], cy = s_cd[1], cz = s_cd[2];
-        double xp[6];
-        kf_cholesky6_warp(&s_sums[7], &s_sums[1], xp, lane);
-        // back to the reference's variables: w = w', t = t' - w x c
+        // the step in the reference's variables (JacobiSVD::solve, :696-697, with the rank
+        // guard of KF_ICP_RANK_TAU)
         double x[6];
-        x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
-        x[0] = xp[0] - (x[4] * cz - x[5] * cy);
-        x[1] = xp[1] - (x[5] * cx - x[3] * cz);
-        x[2] = xp[2] - (x[3] * cy - x[4] * cx);
+        int guarded;
+        kf_icp_solve_warp(&s_sums[7], &s_sums[1], s_cd, x, lane, s_gx, &guarded);
         // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2 (gFusion.cpp:700-703);
         // lanes 0..2 evaluate the three sincos at once
         double sn, cs;

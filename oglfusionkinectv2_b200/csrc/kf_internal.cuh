@@ -447,9 +447,12 @@ __device__ __forceinline__ void kf_sincos_step(double x, double* s, double* c) {
 // kf_cholesky6 for one warp: C given as the 21 upper-triangular values of reduce.cs rows
 // 7..27 (row-major), b as 6 values, both in shared or global memory read by every lane.
 // Lane i < 6 factors row i; every lane returns the whole solution in x (zero when C is
-// not numerically positive definite, as kf_cholesky6).  The pivots' reciprocals come from
-// kf_rsqrt_newton, so the dependent chain holds multiplies and shuffles, no divides.
-__device__ inline void kf_cholesky6_warp(const double* v21, const double* b, double* x, int lane) {
+// not numerically positive definite, as kf_cholesky6) and whether C was; lane i < 6 also
+// returns row i of the factor L in Lrow_out (entries 0..i) and 1 / L_ii in *inv_diag_out.
+// The pivots' reciprocals come from kf_rsqrt_newton, so the dependent chain holds
+// multiplies and shuffles, no divides.
+__device__ inline bool kf_cholesky6_warp(const double* v21, const double* b, double* x, int lane,
+                                         double* Lrow_out = nullptr, double* inv_diag_out = nullptr) {
   auto at = [&](int i, int j) {
     if (i > j) { const int t = i; i = j; j = t; }
     return v21[6 * i - (i * (i - 1)) / 2 + (j - i)];
@@ -484,10 +487,15 @@ __device__ inline void kf_cholesky6_warp(const double* v21, const double* b, dou
       if (lane == j) Lcol[k] = lkj;
     }
   }
+  if (Lrow_out) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) Lrow_out[k] = Lrow[k];
+    *inv_diag_out = inv_diag;
+  }
   if (!spd) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) x[k] = 0.0;
-    return;
+    return false;
   }
   // L y = b, then L^T x = y
   double y = b[i];
@@ -505,6 +513,195 @@ __device__ inline void kf_cholesky6_warp(const double* v21, const double* b, dou
   }
 #pragma unroll
   for (int k = 0; k < 6; ++k) x[k] = __shfl_sync(0xffffffffu, y, k);
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------
+// ICP rank guard (Q22).  The reference solves the 6x6 normal equations with JacobiSVD
+// (gFusion.cpp:696-697), which returns the minimum-norm least-squares step, dropping the
+// singular values below 6 * machine epsilon of the largest.  That cut sits far below the
+// rounding of FP32 sums, so a view of a single plane (rank 3: in-plane motion and rotation
+// about the normal are unobservable) yields steps made of rounding noise.  This build uses
+// the same rule with the cut at KF_ICP_RANK_TAU of the largest eigenvalue of the
+// world-frame C: x = sum_{l_i >= tau l_max} v_i (v_i . b) / l_i.  A full-rank system keeps
+// every direction, and x = C^-1 b; well-posed views have l_min / l_max near 1e-3.
+#define KF_ICP_RANK_TAU 1e-5
+
+// Cyclic Jacobi eigen-decomposition of a symmetric 6x6 matrix (row-major): A is
+// overwritten by its diagonalised form, V receives the eigenvectors in its columns.  At
+// most 32 sweeps; stops when the off-diagonal mass is below 1e-30 of the diagonal's.
+__host__ __device__ inline void kf_jacobi_eigen6(double* A, double* V) {
+  for (int i = 0; i < 36; ++i) V[i] = (i % 7 == 0) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 32; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int p = 0; p < 6; ++p) {
+      diag += A[p * 7] * A[p * 7];
+      for (int q = p + 1; q < 6; ++q) off += A[p * 6 + q] * A[p * 6 + q];
+    }
+    if (!(off > 1e-30 * diag)) break;
+    for (int p = 0; p < 6; ++p)
+      for (int q = p + 1; q < 6; ++q) {
+        const double apq = A[p * 6 + q];
+        if (apq == 0.0) continue;
+        const double theta = (A[q * 7] - A[p * 7]) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 6; ++k) {
+          const double akp = A[k * 6 + p], akq = A[k * 6 + q];
+          A[k * 6 + p] = c * akp - s * akq;
+          A[k * 6 + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 6; ++k) {
+          const double apk = A[p * 6 + k], aqk = A[q * 6 + k];
+          A[p * 6 + k] = c * apk - s * aqk;
+          A[q * 6 + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 6; ++k) {
+          const double vkp = V[k * 6 + p], vkq = V[k * 6 + q];
+          V[k * 6 + p] = c * vkp - s * vkq;
+          V[k * 6 + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+}
+
+// The rank-guarded step of a world-frame system C x = b (C row-major 6x6), as described
+// at KF_ICP_RANK_TAU.  Returns the number of eigen-directions kept.
+__host__ __device__ inline int kf_icp_guarded_solve(const double* C, const double* b, double* x) {
+  double A[36], V[36];
+  for (int i = 0; i < 36; ++i) A[i] = C[i];
+  kf_jacobi_eigen6(A, V);
+  double lmax = 0.0;
+  for (int k = 0; k < 6; ++k) lmax = fmax(lmax, A[k * 7]);
+  for (int i = 0; i < 6; ++i) x[i] = 0.0;
+  int kept = 0;
+  for (int k = 0; k < 6; ++k) {
+    const double l = A[k * 7];
+    if (!(l > 0.0 && l >= KF_ICP_RANK_TAU * lmax)) continue;
+    ++kept;
+    double vb = 0.0;
+    for (int i = 0; i < 6; ++i) vb += V[i * 6 + k] * b[i];
+    for (int i = 0; i < 6; ++i) x[i] += V[i * 6 + k] * vb / l;
+  }
+  return kept;
+}
+
+// The ICP step for one warp, from the centred sums (v21c: reduce.cs rows 7..27 of
+// J' = [n, (p - c) x n], bc: rows 1..6) about the centre c; every lane returns the
+// world-frame step x = (t, w) of gFusion.cpp:696-703.  The centred system C' = M^-T C M^-1
+// (M: t' = t - [c]x w) is solved by the lane-parallel Cholesky; that solution is kept when
+// the world-frame C provably keeps every direction under KF_ICP_RANK_TAU:
+// l_min >= 1 / trace(C^-1) and l_max <= trace(C), with trace(C) = sum_i m_i^T C' m_i
+// (m_i = M e_i) and (C^-1)_ii = |L'^-1 M^-T e_i|^2 for C' = L' L'^T.  Otherwise (rare: a
+// degenerate view) lane 0 forms the world-frame system and runs kf_icp_guarded_solve.
+// *guarded is set when that path ran.
+__device__ inline void kf_icp_solve_warp(const double* v21c, const double* bc, const double* c, double* x,
+                                         int lane, double* s_scratch, int* guarded) {
+  double xp[6], Lrow[6], inv_diag = 0.0;
+  const bool spd = kf_cholesky6_warp(v21c, bc, xp, lane, Lrow, &inv_diag);
+  const double cx = c[0], cy = c[1], cz = c[2];
+  auto at = [&](int i, int j) {
+    if (i > j) { const int t = i; i = j; j = t; }
+    return v21c[6 * i - (i * (i - 1)) / 2 + (j - i)];
+  };
+  bool fast = false;
+  if (spd) {
+    // lane i < 6: u = M^-T e_i, z = L'^-1 u (forward substitution, L' broadcast by shuffles),
+    // D_i = C_ii = m^T C' m with m = M e_i
+    const int i = lane < 6 ? lane : 0;
+    double u[6] = {0, 0, 0, 0, 0, 0}, m[6] = {0, 0, 0, 0, 0, 0};
+    if (i < 3) {
+      // M^-T e_i = (e_i; -(c x e_i)), M e_i = (e_i; 0)
+      u[i] = 1.0;
+      const double e0 = i == 0, e1 = i == 1, e2 = i == 2;
+      u[3] = -(cy * e2 - cz * e1);
+      u[4] = -(cz * e0 - cx * e2);
+      u[5] = -(cx * e1 - cy * e0);
+      m[i] = 1.0;
+    } else {
+      // M^-T e_i = (0; e_k), M e_i = (-(c x e_k); e_k), k = i - 3
+      const int k = i - 3;
+      u[i] = 1.0;
+      const double e0 = k == 0, e1 = k == 1, e2 = k == 2;
+      m[0] = -(cy * e2 - cz * e1);
+      m[1] = -(cz * e0 - cx * e2);
+      m[2] = -(cx * e1 - cy * e0);
+      m[i] = 1.0;
+    }
+    double z[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      double v = u[j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) v = fma(-__shfl_sync(0xffffffffu, Lrow[k], j), z[k], v);
+      z[j] = v * __shfl_sync(0xffffffffu, inv_diag, j);
+    }
+    double D = 0.0;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      double row = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) row = fma(at(r, q), m[q], row);
+      D = fma(m[r], row, D);
+    }
+    double zz = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) zz = fma(z[j], z[j], zz);
+    double tinv = lane < 6 ? zz : 0.0;  // (C^-1)_ii
+    double tr = lane < 6 ? D : 0.0;     // C_ii
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1) {
+      tinv += __shfl_xor_sync(0xffffffffu, tinv, o);
+      tr += __shfl_xor_sync(0xffffffffu, tr, o);
+    }
+    // lanes 0..7 hold the sums over lanes 0..7 (lanes 6, 7 add nothing)
+    tinv = __shfl_sync(0xffffffffu, tinv, 0);
+    tr = __shfl_sync(0xffffffffu, tr, 0);
+    fast = tinv * tr * KF_ICP_RANK_TAU <= 1.0;
+  }
+  if (fast) {
+    // back to the reference's variables: w = w', t = t' - w x c
+    x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
+    x[0] = xp[0] - (x[4] * cz - x[5] * cy);
+    x[1] = xp[1] - (x[5] * cx - x[3] * cz);
+    x[2] = xp[2] - (x[3] * cy - x[4] * cx);
+    *guarded = 0;
+    return;
+  }
+  if (lane == 0) {
+    // world form: b = M^T b', C = M^T C' M with M = [[I, -[c]x], [0, I]]
+    double Cp[36], Mx[36], T[36], Cw[36], bw[6], xw[6];
+    kf_make_jtj(v21c, Cp);
+    for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
+    // -[c]x in rows 0..2, columns 3..5
+    Mx[0 * 6 + 4] = cz;  Mx[0 * 6 + 5] = -cy;
+    Mx[1 * 6 + 3] = -cz; Mx[1 * 6 + 5] = cx;
+    Mx[2 * 6 + 3] = cy;  Mx[2 * 6 + 4] = -cx;
+    for (int r = 0; r < 6; ++r) {
+      double v = 0.0;
+      for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * bc[k];
+      bw[r] = v;
+    }
+    for (int r = 0; r < 6; ++r)
+      for (int cc = 0; cc < 6; ++cc) {
+        double v = 0.0;
+        for (int k = 0; k < 6; ++k) v += Cp[r * 6 + k] * Mx[k * 6 + cc];
+        T[r * 6 + cc] = v;
+      }
+    for (int r = 0; r < 6; ++r)
+      for (int cc = 0; cc < 6; ++cc) {
+        double v = 0.0;
+        for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * T[k * 6 + cc];
+        Cw[r * 6 + cc] = v;
+      }
+    kf_icp_guarded_solve(Cw, bw, xw);
+    for (int k = 0; k < 6; ++k) s_scratch[k] = xw[k];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 6; ++k) x[k] = s_scratch[k];
+  *guarded = 1;
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------------------------------

@@ -12,6 +12,8 @@
 // the 256 thread totals.  Tile totals go to a scratch array that is scanned by the same
 // code recursively (4096^2 = 16.7M elements per level), then added back.  There is no
 // inter-block waiting.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "kf_internal.cuh"
@@ -68,7 +70,10 @@ __global__ void __launch_bounds__(kThreads) tile_sum_kernel(const uint32_t* __re
 }
 
 // Exclusive scan of each tile plus its tile offset (offsets == nullptr: none).
-__global__ void __launch_bounds__(kThreads) tile_scan_kernel(const uint32_t* __restrict__ in, uint32_t* out,
+// `in` may equal `out` (the tile totals are scanned in place): each block reads its whole
+// tile into shared memory before the barrier and writes it after, and `in` is read with
+// ordinary loads (no restrict, no read-only cache path).
+__global__ void __launch_bounds__(kThreads) tile_scan_kernel(const uint32_t* in, uint32_t* out,
                                                              uint64_t n, const uint32_t* __restrict__ offsets,
                                                              uint32_t* total_out) {
   __shared__ uint32_t s_tile[kTile + kTile / 32];  // padded against bank conflicts
@@ -79,7 +84,7 @@ __global__ void __launch_bounds__(kThreads) tile_scan_kernel(const uint32_t* __r
   for (int k = 0; k < kItems; ++k) {
     const int j = k * kThreads + threadIdx.x;
     const uint64_t i = base + (uint64_t)j;
-    s_tile[pad(j)] = i < n ? __ldg(in + i) : 0u;
+    s_tile[pad(j)] = i < n ? in[i] : 0u;
   }
   __syncthreads();
   uint32_t x[kItems];
@@ -186,29 +191,66 @@ static __device__ __align__(256) uint32_t g_noalloc_scan_scratch[KF_NOALLOC_SCAN
 
 namespace {
 std::mutex g_noalloc_mu;
-constexpr int kNoallocMaxDevices = 256;
-uint32_t* g_noalloc_ptr[kNoallocMaxDevices] = {};  // device address of the array, per device
+// The array's device address per CUDA context, keyed by the context's process-unique id
+// (cuCtxGetId): a context created later (a new primary context after cudaDeviceReset, or a
+// context a host framework made with cuCtxCreate) never reuses an entry of an earlier one.
+struct NoallocEntry {
+  unsigned long long ctx_id;
+  uint32_t* ptr;
+};
+constexpr size_t kNoallocMaxEntries = 64;
+std::vector<NoallocEntry> g_noalloc_cache;
+typedef CUresult (*PFN_ctx_get_current)(CUcontext*);
+typedef CUresult (*PFN_ctx_get_id)(CUcontext, unsigned long long*);
+PFN_ctx_get_current g_ctx_get_current = nullptr;
+PFN_ctx_get_id g_ctx_get_id = nullptr;
+
+// The current context's id through the driver entry points (the library links only the
+// CUDA runtime); false when there is no current context.
+bool current_ctx_id(unsigned long long* id) {
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    void* f0 = nullptr;
+    void* f1 = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault) != cudaSuccess || !f0 || !f1) {
+      cudaGetLastError();
+      return false;
+    }
+    g_ctx_get_current = reinterpret_cast<PFN_ctx_get_current>(f0);
+    g_ctx_get_id = reinterpret_cast<PFN_ctx_get_id>(f1);
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  return g_ctx_get_id(ctx, id) == CUDA_SUCCESS;
+}
 }  // namespace
 
 // In host code g_noalloc_scan_scratch only names the symbol; its device address is looked
-// up once per device (with that device current) and cached.
+// up with cudaGetSymbolAddress once per CUDA context (the first call in a context, which
+// also makes the runtime's primary context current when none is) and cached by context id.
 static int noalloc_scratch(uint32_t** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
-    cudaGetLastError();
-    return KF_ERR_NO_DEVICE;
-  }
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return KF_ERR_CUDA;
-    }
-    g_noalloc_ptr[dev] = static_cast<uint32_t*>(p);
+  unsigned long long id = 0;
+  bool have_id = current_ctx_id(&id);
+  if (have_id) {
+    for (const NoallocEntry& e : g_noalloc_cache)
+      if (e.ctx_id == id) {
+        *out = e.ptr;
+        return KF_OK;
+      }
   }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return e == cudaErrorNoDevice ? KF_ERR_NO_DEVICE : KF_ERR_CUDA;
+  }
+  if (!have_id) have_id = current_ctx_id(&id);  // the lookup initialised the primary context
+  if (have_id) {
+    if (g_noalloc_cache.size() >= kNoallocMaxEntries) g_noalloc_cache.erase(g_noalloc_cache.begin());
+    g_noalloc_cache.push_back(NoallocEntry{id, static_cast<uint32_t*>(p)});
+  }
+  *out = static_cast<uint32_t*>(p);
   return KF_OK;
 }
 

@@ -270,6 +270,16 @@ class GFusion:
         self._check(self.lib.kf_get_raycast(self._h, None, n.ctypes.data), "kf_get_raycast")
         return n
 
+    def setReferenceMaps(self, vertex4, normal4) -> None:
+        """Replace the raycast maps Track() associates against (H x W x 4 each, world frame)."""
+        v = np.ascontiguousarray(vertex4, np.float32)
+        n = np.ascontiguousarray(normal4, np.float32)
+        shape = (self.intrinsics.height, self.intrinsics.width, 4)
+        if v.shape != shape or n.shape != shape:
+            raise ValueError(f"reference maps must be {shape}")
+        self._check(self.lib.kf_set_reference_maps(self._h, v.ctypes.data, n.ctypes.data),
+                    "kf_set_reference_maps")
+
     def getVertexMap(self, level: int = 0) -> np.ndarray:
         return self._map(self.lib.kf_get_vertex_map, level, 4)
 

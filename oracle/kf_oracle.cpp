@@ -306,6 +306,68 @@ void or_se3_exp(const double xi[6], double T[16]) {
   T[15] = 1;
 }
 
+/* Symmetric eigen-decomposition by cyclic Jacobi rotations: A (row-major, symmetric) is
+ * diagonalised in place, V receives the eigenvectors in its columns. */
+static void jacobi_eigen_sym6(double A[36], double V[36]) {
+  for (int i = 0; i < 36; ++i) V[i] = (i % 7 == 0) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0;
+    for (int p = 0; p < 6; ++p)
+      for (int q = p + 1; q < 6; ++q) off += A[p * 6 + q] * A[p * 6 + q];
+    if (off < 1e-300) break;
+    for (int p = 0; p < 6; ++p)
+      for (int q = p + 1; q < 6; ++q) {
+        double apq = A[p * 6 + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        double theta = (A[q * 6 + q] - A[p * 6 + p]) / (2 * apq);
+        double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+        double c = 1 / std::sqrt(t * t + 1), sn = t * c;
+        for (int k = 0; k < 6; ++k) {
+          double akp = A[k * 6 + p], akq = A[k * 6 + q];
+          A[k * 6 + p] = c * akp - sn * akq;
+          A[k * 6 + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < 6; ++k) {
+          double apk = A[p * 6 + k], aqk = A[q * 6 + k];
+          A[p * 6 + k] = c * apk - sn * aqk;
+          A[q * 6 + k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < 6; ++k) {
+          double vkp = V[k * 6 + p], vkq = V[k * 6 + q];
+          V[k * 6 + p] = c * vkp - sn * vkq;
+          V[k * 6 + q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+}
+
+/* The ICP step with the rank guard (Q22; the build's deliberate rule, applied identically
+ * by the CUDA path): the minimum-norm least-squares solution that JacobiSVD::solve returns
+ * (gFusion.cpp:696-697), x = sum v_i (v_i . b) / l_i over the eigen-directions of C, with
+ * the rank cut at tau = 1e-5 of the largest eigenvalue instead of JacobiSVD's 6 * epsilon
+ * (which rounding noise of the sums passes).  For a full-rank system this is C^-1 b; for a
+ * view of one plane the three unobservable directions get no motion.  Returns the number
+ * of directions kept. */
+int or_solve_icp_guarded6(const double C[36], const double b[6], double x[6]) {
+  const double tau = 1e-5;
+  double A[36], V[36];
+  std::memcpy(A, C, sizeof(A));
+  jacobi_eigen_sym6(A, V);
+  double lmax = 0;
+  for (int k = 0; k < 6; ++k) lmax = std::max(lmax, A[k * 7]);
+  for (int i = 0; i < 6; ++i) x[i] = 0;
+  int kept = 0;
+  for (int k = 0; k < 6; ++k) {
+    double l = A[k * 7];
+    if (!(l > 0 && l >= tau * lmax)) continue;
+    ++kept;
+    double vb = 0;
+    for (int i = 0; i < 6; ++i) vb += V[i * 6 + k] * b[i];
+    for (int i = 0; i < 6; ++i) x[i] += V[i * 6 + k] * vb / l;
+  }
+  return kept;
+}
+
 int or_solve_pinv6(const double Cin[36], const double b[6], double x[6]) {
   /* Symmetric Jacobi eigen-decomposition; x = sum_i (u_i.b / l_i) u_i over eigenvalues
    * above 6*eps*max|l| — the minimum-norm least-squares solution JacobiSVD::solve
@@ -711,7 +773,7 @@ bool track_icp(or_session* s) {
       make_jtj(&sums[7], C);
       ae = std::sqrt(sums[0] / sums[28]); /* getReduction :1167 */
       double x[6];
-      or_solve_pinv6(C, b, x);
+      or_solve_icp_guarded6(C, b, x); /* JacobiSVD::solve with the rank guard (Q22) */
       /* delta = eulerAngleXYZ(x3,x4,x5); delta[3].xyz = x0..2; m_pose = delta * m_pose */
       double R[9], delta[16];
       or_euler_xyz(&x[3], R);

@@ -91,6 +91,7 @@ int or_prefix_sum_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* t
 void or_euler_xyz(const double angles[3], double R[9]);        /* Rx*Ry*Rz, column-major */
 void or_se3_exp(const double xi[6], double T[16]);             /* xi = (w, v)            */
 int or_solve_pinv6(const double C[36], const double b[6], double x[6]);
+int or_solve_icp_guarded6(const double C[36], const double b[6], double x[6]);
 int or_solve_ldlt6(const double C[36], const double b[6], double x[6]);
 
 /* Marching-cubes tables as seen by the build (table self-consistency test). */

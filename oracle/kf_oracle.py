@@ -40,6 +40,7 @@ _SIG = {
     "or_mc_export_stl": [_P, C.c_char_p], "or_mc_export_ply": [_P, C.c_char_p],
     "or_prefix_sum_u32": [_P, _P, C.c_uint64, C.POINTER(C.c_uint32)],
     "or_euler_xyz": [_PD, _PD], "or_se3_exp": [_PD, _PD], "or_solve_pinv6": [_PD, _PD, _PD],
+    "or_solve_icp_guarded6": [_PD, _PD, _PD],
     "or_solve_ldlt6": [_PD, _PD, _PD], "or_mc_tables": [_P, _P, _P, _P, _P],
 }
 
@@ -324,6 +325,15 @@ def solve_pinv6(Cm, b):
     x = (C.c_double * 6)()
     rank = load().or_solve_pinv6(Cc, bb, x)
     return np.array(list(x)), rank
+
+
+def solve_icp_guarded6(Cm, b):
+    """The ICP step with the rank guard: (x, directions kept)."""
+    Cc = (C.c_double * 36)(*np.asarray(Cm, np.float64).flatten())
+    bb = (C.c_double * 6)(*b)
+    x = (C.c_double * 6)()
+    kept = load().or_solve_icp_guarded6(Cc, bb, x)
+    return np.array(list(x)), kept
 
 
 def solve_ldlt6(Cm, b):

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import kf_oracle as O
-from helpers import integrate_ambiguous, rot_deg, small_workload
+from helpers import integrate_ambiguous, raycast_ambiguous, rot_deg, small_workload
 from oglfusionkinectv2_b200 import GFusion, synth, _lib as L
 
 pytestmark = pytest.mark.gpu
@@ -88,10 +88,20 @@ def test_raycast_parity(storage):
     Vo, No = o.getVerts(), o.getNorms()
     hg, ho = Vg[..., 3] > 0, Vo[..., 3] > 0
     assert ho.mean() > 0.2
-    assert np.mean(hg == ho) > 0.999
     both = hg & ho
-    err = np.linalg.norm(Vg[..., :3] - Vo[..., :3], axis=-1)[both]
-    assert np.mean(err <= 0.5e-3) > 0.999, np.percentile(err, [50, 99, 99.9])
+    err = np.where(both, np.linalg.norm(Vg[..., :3] - Vo[..., :3], axis=-1), 0.0)
+    # every pixel whose hit/miss differs, or whose vertex is more than 0.5 mm off, must be an
+    # FP32/FP64 boundary case of the march (a sample within 1e-4 of 0 or of the 0.8 step
+    # switch, a sample on tfar, or a refinement with f(t0) - f(t1) < 0.02)
+    mism = (hg != ho) | (err > 0.5e-3)
+    ys, xs = np.nonzero(mism)
+    Fo, _ = o.getVolume()
+    amb = raycast_ambiguous(w.config, w.intrinsics, w.poses[2], Fo, (ys, xs))
+    assert amb.all(), f"{int((~amb).sum())} unexplained raycast mismatches of {len(xs)}"
+    assert mism.mean() < 1e-3, mism.mean()
+    # the largest vertex error among the explained pixels stays within two fine steps
+    step = min(w.config.volumeDimensions) / max(w.config.volumeSize)
+    assert err.max() <= 2 * step, (err.max(), step)
     nb = both & (No[..., 3] > 0) & (Ng[..., 3] > 0)
     cosang = np.clip(np.einsum("ijk,ijk->ij", Ng[..., :3], No[..., :3])[nb], -1, 1)
     assert np.mean(np.degrees(np.arccos(cosang)) < 1.0) > 0.99
@@ -178,8 +188,9 @@ def test_sdf_teacher_forced(quirks):
 
 @pytest.mark.parametrize("storage", [L.KF_STORAGE_F32F32, L.KF_STORAGE_F16U16])
 def test_frame_loop_ate_vs_oracle(storage):
-    """kinect.cpp:654-695 free-running on both sides: trajectories within 1 mm ATE."""
-    w = synth.plain_c1(30)
+    """kinect.cpp:654-695 free-running on both sides over the full 100 frames of the
+    128^3 plain workload: trajectories within 1 mm ATE."""
+    w = synth.plain_c1(100)
     w.config.storage = storage
     g, o = pair(w)
     for s in (g, o):
@@ -277,3 +288,66 @@ def test_errors_are_reported():
     with pytest.raises(L.KfError) as e:
         g.setVolumeRaw(np.zeros(7, np.uint8))
     assert e.value.status == L.KF_ERR_INVALID_ARGUMENT
+
+
+def _plane_maps(w, pose, plane_n, plane_h):
+    """Analytic world-frame vertex map of the plane n.X = h seen from `pose`, and the hit
+    mask; and float millimetre depth of the same view (0 where there is no hit in range)."""
+    dirs = w.pixel_rays() @ pose[:3, :3].T
+    o = pose[:3, 3]
+    n = np.asarray(plane_n, np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = (plane_h - n @ o) / (dirs @ n)
+    hit = np.isfinite(t) & (t >= 0.5) & (t <= 4.5)
+    X = o + dirs * np.where(hit, t, 0.0)[:, None]
+    H, W = w.intrinsics.height, w.intrinsics.width
+    depth = np.where(hit, t * 1000.0, 0.0).astype(np.float32).reshape(H, W)
+    return X.reshape(H, W, 3), hit.reshape(H, W), depth
+
+
+@pytest.mark.parametrize("jtj", [L.KF_JTJ_FP32, L.KF_JTJ_SPLIT_BF16])
+def test_icp_plane_only_rank_guard(jtj):
+    """Q22: a view of one plane leaves in-plane translation and rotation about the normal
+    unobservable (J^T J of rank 3).  Exact (float) plane depth tracked against exact plane
+    reference maps on both sides: the rank guard drops the same three directions on the
+    GPU and in the oracle, and both end on the same pose."""
+    w = small_workload(3, size=128, jtj=jtj)
+    ground = [p for p in w.scene.planes][0]
+    pn, ph = np.array(ground[0], np.float64), float(ground[1])
+    g, o = pair(w)
+    P0, P1 = w.poses[0], w.poses[1]
+    X0, hit0, _ = _plane_maps(w, P0, pn, ph)
+    _, _, d1 = _plane_maps(w, P1, pn, ph)
+    assert hit0.mean() > 0.2 and (d1 > 0).mean() > 0.2
+    # raycast normals point back towards the camera
+    nrm = -pn if pn @ P0[:3, 3] < ph else pn
+    V = np.zeros(hit0.shape + (4,), np.float32)
+    N = np.zeros(hit0.shape + (4,), np.float32)
+    V[hit0, :3] = X0[hit0]
+    V[hit0, 3] = 1.0
+    N[hit0, :3] = nrm
+    N[hit0, 3] = 1.0
+    for s in (g, o):
+        s.Reset(P0)
+        s.setPose(P0)
+        s.raycast()  # sets the association pose; the maps are replaced next
+    g.setReferenceMaps(V, N)
+    o.setRaycast(V.astype(np.float64), N.astype(np.float64))
+    for s in (g, o):
+        s.depthToVertex(d1)
+        s.vertexToNormal()
+    tg, to = g.Track(), o.Track()
+    assert tg == to
+    Pg, Po = g.getPose(), o.getPose()
+    assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 1e-4, np.linalg.norm(Pg[:3, 3] - Po[:3, 3])
+    assert rot_deg(Pg, Po) <= 0.01
+    # the last system was rank-deficient by the guard's measure on both sides
+    for red in (g.getReduction(), o.getReduction()):
+        Cm = np.zeros((6, 6))
+        k = 7
+        for i in range(6):
+            for j in range(i, 6):
+                Cm[i, j] = Cm[j, i] = red[k]
+                k += 1
+        lam = np.linalg.eigvalsh(Cm)
+        assert lam[2] < 1e-5 * lam[-1] and lam[3] > 1e-3 * lam[-1], lam

@@ -65,6 +65,35 @@ def test_solvers():
     assert r0 == 0 and np.all(x0 == 0)
 
 
+def test_icp_rank_guard_solve():
+    """The ICP step's rank guard: eigen-directions below 1e-5 of the largest eigenvalue
+    are dropped, the step is the minimum-norm solution over the rest (JacobiSVD::solve's
+    rule with a higher cut)."""
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((50, 6)) * np.array([1, 1, 1, 3, 3, 3])
+    C = A.T @ A
+    b = rng.standard_normal(6)
+    x, kept = O.solve_icp_guarded6(C, b)
+    assert kept == 6
+    np.testing.assert_allclose(x, np.linalg.solve(C, b), rtol=1e-9)
+    # rank 3 (a plane: J = [n, p x n] with one normal) plus rounding-size noise
+    n = np.array([0.0, -1.0, 0.0])
+    P = rng.uniform(-1, 1, (200, 3)) * [1, 0, 1] + [1.0, 1.3, 2.0]
+    J = np.hstack([np.tile(n, (200, 1)), np.cross(P, n)])
+    Cp = J.T @ J + 1e-13 * np.eye(6)
+    bp = J.T @ rng.standard_normal(200)
+    xp, kept = O.solve_icp_guarded6(Cp, bp)
+    assert kept == 3
+    lam, V = np.linalg.eigh(Cp)
+    keep = lam >= 1e-5 * lam[-1]
+    expect = V[:, keep] @ ((V[:, keep].T @ bp) / lam[keep])
+    np.testing.assert_allclose(xp, expect, rtol=1e-7, atol=1e-12)
+    # the unobservable directions get no motion: in-plane translation, rotation about n
+    assert abs(xp[0]) < 1e-9 and abs(xp[2]) < 1e-9 and abs(xp[4]) < 1e-9
+    x0, k0 = O.solve_icp_guarded6(np.zeros((6, 6)), b)
+    assert k0 == 0 and np.all(x0 == 0)
+
+
 def test_prefix_sum_matches_cumsum_and_wraps():
     rng = np.random.default_rng(2)
     for n in [0, 1, 2047, 2048, 2049, 100000]:
