@@ -488,7 +488,8 @@ def serve_pass(server, arrivals, seqs, gt, duration, fbytes, max_slots):
                 server.submit_device(sid, seqs[sc].data_ptr() + idx * fbytes)
                 sub += 1
             st[4] = sub
-        n_done = server.step()
+        # asynchronous steps: the device runs this step while the loop admits and queues
+        n_done = server.step_async()
         frames += n_done
         if n_done:
             ids, poses, _ = server.last_step(max_slots)
@@ -502,6 +503,7 @@ def serve_pass(server, arrivals, seqs, gt, duration, fbytes, max_slots):
                     errs_done.append(errs)
                     server.close_session(sid)
                     del active[sid]
+    server.sync()  # the step in flight (its frames are past the measured duration)
     errs_all = errs_done + [st[5] for st in active.values()]
     for sid in list(active):
         server.close_session(sid)

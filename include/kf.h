@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define KF_ABI_VERSION 1
+#define KF_ABI_VERSION 2
 
 #if defined(KF_BUILDING_LIBRARY) && defined(__GNUC__)
 #define KF_API __attribute__((visibility("default")))
@@ -296,16 +296,18 @@ KF_API int kf_get_stream(kf_session* s, void** cuda_stream);
  * Every shape computes bit-identical results; only the time differs. */
 typedef struct kf_launch_shape {
   int32_t integrate_z_chunk; /* voxels per thread along z: 8, 16 (default) or 32 */
-  int32_t raycast_rows;      /* raycast tile of 32 x rows pixels: 2, 4 (default) or 8 */
+  int32_t raycast_rows;      /* raycast tile of 32 x rows pixels: 2, 4 (default) or 8;  */
+                             /* 1 = persistent sweep, every warp taking the next 32-pixel */
+                             /* row segment from a queue (sessions only, not batches)     */
   int32_t reserved[6];
 } kf_launch_shape;
 KF_API int kf_set_launch_shape(kf_session* s, const kf_launch_shape* shape);
 KF_API int kf_get_launch_shape(kf_session* s, kf_launch_shape* shape);
-/* Times every integrate z-chunk and raycast tile shape on the session's current depth
- * frame, pose and volume (repeats launches each, twice over, into scratch copies: the
- * session's volume, maps and pose are untouched; needs one more volume's worth of device
- * memory meanwhile), then uses the fastest.  times_ms (optional, 6 floats) receives the
- * mean time of integrate with z-chunk 8, 16, 32 and raycast with rows 2, 4, 8.  Sessions
+/* Times every integrate z-chunk and raycast shape on the session's current depth frame,
+ * pose and volume (repeats launches each, twice over, into scratch copies: the session's
+ * volume, maps and pose are untouched; needs one more volume's worth of device memory
+ * meanwhile), then uses the fastest.  times_ms (optional, 7 floats) receives the mean time
+ * of integrate with z-chunk 8, 16, 32 and raycast with rows 1 (sweep), 2, 4, 8.  Sessions
  * created later with the same device, volume size, storage and image size start with the
  * shape chosen here. */
 KF_API int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* times_ms);
@@ -355,7 +357,8 @@ KF_API int kf_batch_get_launch_shape(kf_batch* b, kf_launch_shape* shape);
 /* kf_autotune for the batched launches over these sessions (the mix of one step): each
  * candidate shape times one batched integrate and raycast over all of them, into scratch
  * copies (one more copy of every member's volume meanwhile); the batch then uses the
- * fastest.  times_ms as for kf_autotune. */
+ * fastest.  times_ms (optional, 6 floats): integrate with z-chunk 8, 16, 32 and raycast
+ * with rows 2, 4, 8 (a batch has no sweep shape). */
 KF_API int kf_batch_autotune(kf_batch* b, kf_session* const* sessions, int n, int repeats,
                              kf_launch_shape* chosen, float* times_ms);
 
@@ -405,6 +408,16 @@ KF_API int kf_server_close(kf_server* v, int session_id);
 KF_API int kf_server_submit(kf_server* v, int session_id, const uint16_t* host_depth_mm);
 KF_API int kf_server_submit_device(kf_server* v, int session_id, const uint16_t* device_depth_mm);
 KF_API int kf_server_step(kf_server* v, int* frames_done);
+/* Asynchronous served step: enqueues a batched step over the sessions with a waiting frame
+ * and returns once the PREVIOUS step's results are on the host (waiting for that step
+ * only), so the host admits sessions and queues frames while the device runs.  After it,
+ * kf_server_last_step / kf_server_get_pose describe the previous step, whose frame count
+ * is *frames_done; when no frame is waiting, the step in flight is waited for instead.
+ * kf_server_sync completes the step in flight; kf_server_step does so first, and so does
+ * kf_server_close of a session in that step (its results are then the last step's).  A
+ * frame's latency runs from its arrival to the call that returns its pose. */
+KF_API int kf_server_step_async(kf_server* v, int* frames_done);
+KF_API int kf_server_sync(kf_server* v, int* frames_done);
 KF_API int kf_server_get_pose(kf_server* v, int session_id, double pose16[16], int* tracked,
                               uint64_t* frames_done);
 /* The sessions of the last kf_server_step (up to max_n): ids, poses (16 doubles each,

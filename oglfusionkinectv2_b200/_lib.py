@@ -185,6 +185,8 @@ SIGNATURES = {
     "kf_server_submit": (_I, [_P, _I, _P]),
     "kf_server_submit_device": (_I, [_P, _I, _P]),
     "kf_server_step": (_I, [_P, C.POINTER(_I)]),
+    "kf_server_step_async": (_I, [_P, C.POINTER(_I)]),
+    "kf_server_sync": (_I, [_P, C.POINTER(_I)]),
     "kf_server_get_pose": (_I, [_P, _I, _P, C.POINTER(_I), C.POINTER(C.c_uint64)]),
     "kf_server_pending": (_I, [_P, _I, C.POINTER(_I)]),
     "kf_server_last_step": (_I, [_P, _I, _P, _P, _P, C.POINTER(_I)]),

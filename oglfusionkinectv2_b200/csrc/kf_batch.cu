@@ -26,7 +26,7 @@ __global__ void batch_clear_kernel(KfDevState* const* states) {
     st->barrier_count = 0;
     st->sdf_barrier_count = 0;
   }
-  for (int k = threadIdx.x; k < 3 * 32; k += blockDim.x) (&st->icp_acc[0][0])[k] = 0;
+  for (int k = threadIdx.x; k < 3 * 32; k += blockDim.x) st->icp_acc[k / 32][k % 32][0] = 0;
 }
 
 // Gather each member's frame result (the first KF_STATE_RESULT_BYTES of its state).
@@ -67,7 +67,19 @@ bool same_members(const kf_batch* b, kf_session* const* ss, int n) {
   return true;
 }
 
+// The step graphs bake in the tables' launch configuration and shapes: dropped whenever
+// those change.
+void drop_graphs(kf_batch* b) {
+  for (int k = 0; k < 2; ++k) {
+    if (b->step_exec[k]) cudaGraphExecDestroy(b->step_exec[k]);
+    b->step_exec[k] = nullptr;
+    b->graph_n[k] = 0;
+    b->graph_kernels[k] = 0;
+  }
+}
+
 int rebuild_tables(kf_batch* b, kf_session* const* ss, int n) {
+  drop_graphs(b);
   b->members.assign(ss, ss + n);
   b->member_keys.resize(n);
   for (int e = 0; e < n; ++e) b->member_keys[e] = std::make_pair(ss[e]->uid, ss[e]->layout);
@@ -149,34 +161,73 @@ int enqueue_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* dept
     for (int e = 0; e < n; ++e)
       KF_CUDA_TRY(b, cudaMemcpyAsync(ss[e]->d_depth_u16, depth[e], px * 2, kind, b->stream));
   } else {
-    // device frames are read in place: one small upload of their addresses
+    // device frames are read in place: one small upload of their addresses (in the step)
     const uint16_t** hin = b->h_inputs + (size_t)slot * b->cap;
     for (int e = 0; e < n; ++e) hin[e] = depth[e];
-    KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_inputs, hin, n * sizeof(uint16_t*), cudaMemcpyHostToDevice, b->stream));
     inputs = b->d_inputs;
   }
-  KF_CUDA_TRY(b, cudaEventRecord(ev[0], b->stream));
-  batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
-  KF_CUDA_TRY(b, cudaGetLastError());
-  if ((rc = kf_batch_launch_pyramid(b, n, inputs))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(ev[1], b->stream));
-  if ((rc = kf_batch_launch_icp(b))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(ev[2], b->stream));
-  if ((rc = kf_batch_launch_integrate(b))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(ev[3], b->stream));
-  if ((rc = kf_batch_launch_sdf_recover(b))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(ev[4], b->stream));
-  if ((rc = kf_batch_launch_raycast(b, n))) return rc;
-  KF_CUDA_TRY(b, cudaEventRecord(ev[5], b->stream));
+  // the device part of the step: stages with their events, then every member's frame
+  // result gathered and copied to the slot's pinned heads
+  auto body = [&]() -> int {
+    int r;
+    if (inputs) KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_inputs, b->h_inputs + (size_t)slot * b->cap,
+                                               n * sizeof(uint16_t*), cudaMemcpyHostToDevice, b->stream));
+    KF_CUDA_TRY(b, cudaEventRecord(ev[0], b->stream));
+    batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
+    KF_CUDA_TRY(b, cudaGetLastError());
+    if ((r = kf_batch_launch_pyramid(b, n, inputs))) return r;
+    KF_CUDA_TRY(b, cudaEventRecord(ev[1], b->stream));
+    if ((r = kf_batch_launch_icp(b))) return r;
+    KF_CUDA_TRY(b, cudaEventRecord(ev[2], b->stream));
+    if ((r = kf_batch_launch_integrate(b))) return r;
+    KF_CUDA_TRY(b, cudaEventRecord(ev[3], b->stream));
+    if ((r = kf_batch_launch_sdf_recover(b))) return r;
+    KF_CUDA_TRY(b, cudaEventRecord(ev[4], b->stream));
+    if ((r = kf_batch_launch_raycast(b, n))) return r;
+    KF_CUDA_TRY(b, cudaEventRecord(ev[5], b->stream));
+    batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
+    KF_CUDA_TRY(b, cudaGetLastError());
+    b->launches += 2;
+    KF_CUDA_TRY(b, cudaMemcpyAsync(b->h_heads + (size_t)slot * b->cap * KF_STATE_RESULT_BYTES, b->d_heads,
+                                   (size_t)n * KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost, b->stream));
+    KF_CUDA_TRY(b, cudaEventRecord(ev[6], b->stream));
+    return KF_OK;
+  };
+  if (inputs) {
+    // device frames: the step is a CUDA graph per slot, captured on its first use with
+    // these tables and replayed (the input addresses are read from the slot's pinned list)
+    if (!b->step_exec[slot] || b->graph_n[slot] != n) {
+      if (b->step_exec[slot]) cudaGraphExecDestroy(b->step_exec[slot]);
+      b->step_exec[slot] = nullptr;
+      const uint64_t l0 = b->launches;
+      KF_CUDA_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      rc = body();
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+      if (rc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc ? rc : bfail(b, KF_ERR_CUDA, std::string("batch step capture: ") + cudaGetErrorString(ce));
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&b->step_exec[slot], g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        b->step_exec[slot] = nullptr;
+        return bfail(b, KF_ERR_CUDA, std::string("batch step graph: ") + cudaGetErrorString(ie));
+      }
+      b->graph_n[slot] = n;
+      b->graph_kernels[slot] = b->launches - l0;
+      b->launches = l0;
+    }
+    KF_CUDA_TRY(b, cudaGraphLaunch(b->step_exec[slot], b->stream));
+    b->launches += b->graph_kernels[slot];
+    b->graph_replays += 1;
+  } else if ((rc = body())) {
+    return rc;
+  }
   // every KF_BRICK_REBUILD_EVERY integrates a member's skip flags are rebuilt exactly
   for (int e = 0; e < n; ++e)
     if ((rc = kf_note_integrate(ss[e], b->stream))) return bfail(b, rc, "brick flag rebuild: " + ss[e]->last_error);
-  batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
-  KF_CUDA_TRY(b, cudaGetLastError());
-  b->launches += 2;
-  KF_CUDA_TRY(b, cudaMemcpyAsync(b->h_heads + (size_t)slot * b->cap * KF_STATE_RESULT_BYTES, b->d_heads,
-                                 (size_t)n * KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost, b->stream));
-  KF_CUDA_TRY(b, cudaEventRecord(ev[6], b->stream));
   b->steps += 1;
   // the previous step's results are read now, while this one runs
   const int prev = harvest(b);
@@ -199,6 +250,7 @@ int batch_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* depth,
 }
 
 void free_batch(kf_batch* b) {
+  drop_graphs(b);
   cudaFree(b->d_table);
   cudaFreeHost(b->h_table);
   cudaFree(b->d_heads);
@@ -313,7 +365,7 @@ int kf_batch_get_launch_count(kf_batch* b, uint64_t* n) {
 }
 
 int kf_batch_set_launch_shape(kf_batch* b, const kf_launch_shape* shape) {
-  if (!b || !shape || !kf_valid_int_zc(shape->integrate_z_chunk) || !kf_valid_ray_rows(shape->raycast_rows))
+  if (!b || !shape || !kf_valid_int_zc(shape->integrate_z_chunk) || !kf_valid_batch_ray_rows(shape->raycast_rows))
     return KF_ERR_INVALID_ARGUMENT;
   if (int rc = harvest(b)) return rc;
   KF_CUDA_TRY(b, cudaStreamSynchronize(b->stream));
@@ -369,7 +421,7 @@ int kf_batch_autotune(kf_batch* b, kf_session* const* ss, int n, int repeats, kf
       if (cudaStreamSynchronize(b->stream) != cudaSuccess) { rc = bfail(b, KF_ERR_CUDA, "autotune"); break; }
       b->table_used = 0;
       if (ray) {
-        b->ray_rows = kf_tune_ray_rows[c - 3];
+        b->ray_rows = kf_tune_batch_ray_rows[c - 3];
         rc = kf_batch_prepare_raycast(b, t.data());
       } else {
         b->int_zc = kf_tune_int_zc[c];
@@ -409,7 +461,7 @@ int kf_batch_autotune(kf_batch* b, kf_session* const* ss, int n, int repeats, kf
   for (int c = 3; c < 6; ++c)
     if (best[c] < best[ri]) ri = c;
   b->int_zc = kf_tune_int_zc[zi];
-  b->ray_rows = kf_tune_ray_rows[ri - 3];
+  b->ray_rows = kf_tune_batch_ray_rows[ri - 3];
   if (chosen) kf_batch_get_launch_shape(b, chosen);
   if (times_ms) std::memcpy(times_ms, best, sizeof(best));
   return KF_OK;

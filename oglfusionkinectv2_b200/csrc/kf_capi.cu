@@ -414,7 +414,7 @@ int kf_launch_sdf_policy(kf_session* s) {
   return KF_OK;
 }
 
-int kf_occupancy_blocks(kf_session* s, const void* kernel, int threads, size_t smem) {
+int kf_occupancy_blocks(kf_session* s, const void* kernel, int threads, size_t smem, int max_per_sm) {
   std::lock_guard<std::mutex> lk(g_occ_mu);
   auto key = std::make_pair(kernel, s->device);
   auto it = g_occ.find(key);
@@ -429,10 +429,10 @@ int kf_occupancy_blocks(kf_session* s, const void* kernel, int threads, size_t s
     }
     g_occ[key] = per_sm;
   }
-  // two co-resident blocks per SM: enough warps to hide the gather latency, few enough
-  // partial rows for the single-block FP64 reduction
-  const int blocks = std::min(per_sm, 2) * s->num_sms;
-  return std::min(blocks, KF_MAX_TRACK_BLOCKS);
+  // the tracking kernels: two co-resident blocks per SM, enough warps to hide the gather
+  // latency, few enough partial rows for the single-block FP64 reduction
+  const int blocks = std::min(per_sm, max_per_sm) * s->num_sms;
+  return max_per_sm == 2 ? std::min(blocks, KF_MAX_TRACK_BLOCKS) : blocks;
 }
 
 // =========================================================================================
@@ -1248,9 +1248,9 @@ int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* time
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(s, KF_ERR_CUDA, "autotune events");
   // each candidate: one untimed launch, then `repeats` launches between two events; two
   // rounds over all candidates, the better mean kept (clock and cache drift even out)
-  float best[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+  float best[7] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
   for (int round = 0; round < 2 && !rc; ++round)
-    for (int c = 0; c < 6 && !rc; ++c) {
+    for (int c = 0; c < 7 && !rc; ++c) {
       const bool ray = c >= 3;
       const int v = ray ? kf_tune_ray_rows[c - 3] : kf_tune_int_zc[c];
       auto launch = [&]() {
@@ -1273,10 +1273,10 @@ int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* time
   if (e1) cudaEventDestroy(e1);
   kf_scratch_free(&t);
   if (rc) return rc;
-  int zi = 1, ri = 4;  // the defaults win ties
+  int zi = 1, ri = 5;  // the defaults (z-chunk 16, 32 x 4 tiles) win ties
   for (int c = 0; c < 3; ++c)
     if (best[c] < best[zi]) zi = c;
-  for (int c = 3; c < 6; ++c)
+  for (int c = 3; c < 7; ++c)
     if (best[c] < best[ri]) ri = c;
   kf_launch_shape sh{};
   sh.integrate_z_chunk = kf_tune_int_zc[zi];

@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       c[0] = s_c[0]; c[1] = s_c[1]; c[2] = s_c[2];
 
       // ---------------- track + accumulate ----------------
-      long long* accbuf = &a.st->icp_acc[gi % 3u][0];
+      long long* accbuf = &a.st->icp_acc[gi % 3u][0][0];  // sum k at accbuf[k * KF_ACC_STRIDE]
       float acc[JTJ ? 1 : 28];
 #pragma unroll
       for (int k = 0; k < (JTJ ? 1 : 28); ++k) acc[k] = 0.0f;
@@ -365,7 +365,9 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
           float v = 0.0f;
 #pragma unroll
           for (int w = 0; w < kWarps; ++w) v += tid < 28 ? s_warp[w][tid] : s_pw[w][tid - 28];
-          atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid), (unsigned long long)__float2ll_rn(v * kFix));
+          // adding zero changes nothing: blocks without pixels at a coarse level skip it
+          const long long q = __float2ll_rn(v * kFix);
+          if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid * KF_ACC_STRIDE), (unsigned long long)q);
         }
       } else {
         // lane (g, t) holds M[g][2t], M[g][2t+1]; lanes t == 3 also sum q_g
@@ -397,11 +399,12 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) v += s_fix[w][64 + tid - 29] + s_fix[w][64 + tid - 26];
           }
-          atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid), (unsigned long long)v);
+          // adding zero changes nothing: blocks without pixels at a coarse level skip it
+          if (v != 0) atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid * KF_ACC_STRIDE), (unsigned long long)v);
         }
       }
       // the buffer of the next iteration was last read before the previous barrier
-      if (local == 0 && tid >= 32 && tid < 64) a.st->icp_acc[(gi + 1u) % 3u][tid - 32] = 0;
+      if (local == 0 && tid >= 32 && tid < 64) a.st->icp_acc[(gi + 1u) % 3u][tid - 32][0] = 0;
 
       // ---------------- grid barrier; then every block solves ----------------
       // Every block reads the same exact sums and solves the same system in FP64, so all
@@ -425,7 +428,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
           }
         }
       }
-      if (tid < 32) s_sums[tid] = (double)__ldcg(accbuf + tid) * kInvFix;
+      if (tid < 32) s_sums[tid] = (double)__ldcg(accbuf + tid * KF_ACC_STRIDE) * kInvFix;
       __syncthreads();
       if (warp == 0) {
         // ---- solve, lane-parallel in warp 0 ----

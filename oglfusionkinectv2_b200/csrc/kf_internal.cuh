@@ -18,6 +18,9 @@
 #define KF_TRACK_THREADS 256      // threads per block of the persistent tracking kernels
 #define KF_MAX_TRACK_BLOCKS 1024  // upper bound of the persistent grid
 
+// Words of 8 bytes between two ICP reduction sums (one 128-byte line each).
+#define KF_ACC_STRIDE 16
+
 // Device-side error word values (KfDevState::error).
 #define KF_DEV_ERR_TIMEOUT 1
 
@@ -48,11 +51,18 @@ struct KfDevState {
   int do_integrate;     // frame policy: integrate this frame
   int reset_window;     // kinect.cpp `reset` flag
   int iterations_run;   // ICP/SDF iterations executed by the last tracking call
-  unsigned barrier_count;      // grid barrier of the ICP launch
-  unsigned sdf_barrier_count;  // grid barrier of the SDF launch
+  // grid barrier counters, each on its own 128-byte line (polled by every block while the
+  // reduction atomics land elsewhere)
+  alignas(128) unsigned barrier_count;      // grid barrier of the ICP launch
+  alignas(128) unsigned sdf_barrier_count;  // grid barrier of the SDF launch
   // ICP reduction rows as fixed-point sums (value * 2^32, exact and order-independent),
-  // three buffers used in turn by successive iterations of a launch
-  alignas(8) long long icp_acc[3][32];
+  // three buffers used in turn by successive iterations of a launch; every sum on its own
+  // 128-byte line (KF_ACC_STRIDE words apart), so the blocks' 64-bit atomics on the 32
+  // sums of a row spread over the L2 slices instead of queueing on two lines
+  alignas(128) long long icp_acc[3][32][KF_ACC_STRIDE];
+  // the persistent raycast sweep's row-segment queue: next segment, warps done (both zero
+  // between launches: the sweep's last warp resets them)
+  alignas(128) unsigned ray_queue[2];
   double icp_center_cam[3];  // ICP centre at the end of the last frame (camera frame)
   double lib_pose[KF_MAX_LIBRARY][16];  // pose library
 };
@@ -163,7 +173,7 @@ struct kf_session {
 
   // launch shapes (kf_set_launch_shape / kf_autotune); every choice computes the same result
   int int_zc = 16;   // integrate: voxels per thread along z (8, 16, 32)
-  int ray_rows = 4;  // raycast: tile rows of 32 pixels (2, 4, 8)
+  int ray_rows = 4;  // raycast: tile rows of 32 pixels (2, 4, 8), or 1: persistent sweep
 
   // depth ingest before the pyramid (off by default): Kinect-v2 undistortion through a
   // source-index map, and the filter3D.cs validity filter; their output is d_depth_prep
@@ -201,6 +211,14 @@ struct Vox<KF_STORAGE_F32F32> {
   __device__ static __forceinline__ Wt encode_weight(float w) { return w; }
 };
 
+// A 16-bit integer as float and back without conversion instructions (exact): the integer
+// in the low mantissa bits of 2^23, and a non-negative float below 2^16 truncated by an add
+// of 2^23 rounded toward zero.
+__device__ __forceinline__ float kf_u16_to_float(uint32_t w) { return __int_as_float(0x4B000000 | w) - 8388608.0f; }
+__device__ __forceinline__ uint32_t kf_float_to_u16_trunc(float w) {
+  return (uint32_t)__float_as_int(__fadd_rz(w, 8388608.0f)) & 0xFFFFu;  // 0 <= w <= 65535
+}
+
 template <>
 struct Vox<KF_STORAGE_F16U16> {
   typedef __half V;
@@ -208,10 +226,10 @@ struct Vox<KF_STORAGE_F16U16> {
   static constexpr float kRawToF = 1.0f;
   __device__ static __forceinline__ float raw(const V* f, size_t i) { return __half2float(__ldg(f + i)); }
   __device__ static __forceinline__ float raw_nc(const V* f, size_t i) { return __half2float(f[i]); }
-  __device__ static __forceinline__ float weight(const Wt* w, size_t i) { return (float)w[i]; }
+  __device__ static __forceinline__ float weight(const Wt* w, size_t i) { return kf_u16_to_float(w[i]); }
   __device__ static __forceinline__ V encode_value(float F) { return __float2half_rn(F); }
   __device__ static __forceinline__ Wt encode_weight(float w) {
-    return (uint16_t)fminf(fmaxf(w, 0.0f), 65535.0f);
+    return (uint16_t)kf_float_to_u16_trunc(fminf(fmaxf(w, 0.0f), 65535.0f));
   }
 };
 
@@ -586,6 +604,40 @@ __host__ __device__ inline int kf_icp_guarded_solve(const double* C, const doubl
   return kept;
 }
 
+// The rank-guarded step from the centred sums about c, in the world frame: b = M^T b',
+// C = M^T C' M with M = [[I, -[c]x], [0, I]], then kf_icp_guarded_solve.  Kept out of line:
+// it runs only for degenerate views, and its arrays would crowd the caller's registers.
+static __device__ __noinline__ void kf_icp_world_guarded_step(const double* v21c, const double* bc, const double* c,
+                                                       double* out) {
+  const double cx = c[0], cy = c[1], cz = c[2];
+  double Cp[36], Mx[36], T[36], Cw[36], bw[6], xw[6];
+  kf_make_jtj(v21c, Cp);
+  for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
+  // -[c]x in rows 0..2, columns 3..5
+  Mx[0 * 6 + 4] = cz;  Mx[0 * 6 + 5] = -cy;
+  Mx[1 * 6 + 3] = -cz; Mx[1 * 6 + 5] = cx;
+  Mx[2 * 6 + 3] = cy;  Mx[2 * 6 + 4] = -cx;
+  for (int r = 0; r < 6; ++r) {
+    double v = 0.0;
+    for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * bc[k];
+    bw[r] = v;
+  }
+  for (int r = 0; r < 6; ++r)
+    for (int cc = 0; cc < 6; ++cc) {
+      double v = 0.0;
+      for (int k = 0; k < 6; ++k) v += Cp[r * 6 + k] * Mx[k * 6 + cc];
+      T[r * 6 + cc] = v;
+    }
+  for (int r = 0; r < 6; ++r)
+    for (int cc = 0; cc < 6; ++cc) {
+      double v = 0.0;
+      for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * T[k * 6 + cc];
+      Cw[r * 6 + cc] = v;
+    }
+  kf_icp_guarded_solve(Cw, bw, xw);
+  for (int k = 0; k < 6; ++k) out[k] = xw[k];
+}
+
 // The ICP step for one warp, from the centred sums (v21c: reduce.cs rows 7..27 of
 // J' = [n, (p - c) x n], bc: rows 1..6) about the centre c; every lane returns the
 // world-frame step x = (t, w) of gFusion.cpp:696-703.  The centred system C' = M^-T C M^-1
@@ -606,47 +658,37 @@ __device__ inline void kf_icp_solve_warp(const double* v21c, const double* bc, c
   };
   bool fast = false;
   if (spd) {
-    // lane i < 6: u = M^-T e_i, z = L'^-1 u (forward substitution, L' broadcast by shuffles),
-    // D_i = C_ii = m^T C' m with m = M e_i
+    // lane i < 6: u = M^-T e_i, z = L'^-1 u (forward substitution, L' broadcast by
+    // shuffles), and C_ii = m^T C' m with m = M e_i.  For i < 3: u = (e_i; -(c x e_i)),
+    // m = e_i; for i = 3 + k: u = e_i, m = (-(c x e_k); e_k).
     const int i = lane < 6 ? lane : 0;
-    double u[6] = {0, 0, 0, 0, 0, 0}, m[6] = {0, 0, 0, 0, 0, 0};
-    if (i < 3) {
-      // M^-T e_i = (e_i; -(c x e_i)), M e_i = (e_i; 0)
-      u[i] = 1.0;
-      const double e0 = i == 0, e1 = i == 1, e2 = i == 2;
-      u[3] = -(cy * e2 - cz * e1);
-      u[4] = -(cz * e0 - cx * e2);
-      u[5] = -(cx * e1 - cy * e0);
-      m[i] = 1.0;
-    } else {
-      // M^-T e_i = (0; e_k), M e_i = (-(c x e_k); e_k), k = i - 3
-      const int k = i - 3;
-      u[i] = 1.0;
-      const double e0 = k == 0, e1 = k == 1, e2 = k == 2;
-      m[0] = -(cy * e2 - cz * e1);
-      m[1] = -(cz * e0 - cx * e2);
-      m[2] = -(cx * e1 - cy * e0);
-      m[i] = 1.0;
-    }
+    const int k3 = i < 3 ? i : i - 3;
+    // c x e_k
+    const double ck0 = k3 == 0 ? 0.0 : (k3 == 1 ? -cz : cy);
+    const double ck1 = k3 == 0 ? cz : (k3 == 1 ? 0.0 : -cx);
+    const double ck2 = k3 == 0 ? -cy : (k3 == 1 ? cx : 0.0);
     double z[6];
+    double zz = 0.0;
 #pragma unroll
     for (int j = 0; j < 6; ++j) {
-      double v = u[j];
+      double v = j == i ? 1.0 : 0.0;
+      if (i < 3 && j >= 3) v = -(j == 3 ? ck0 : (j == 4 ? ck1 : ck2));
 #pragma unroll
       for (int k = 0; k < j; ++k) v = fma(-__shfl_sync(0xffffffffu, Lrow[k], j), z[k], v);
       z[j] = v * __shfl_sync(0xffffffffu, inv_diag, j);
+      zz = fma(z[j], z[j], zz);
     }
-    double D = 0.0;
-#pragma unroll
-    for (int r = 0; r < 6; ++r) {
-      double row = 0.0;
-#pragma unroll
-      for (int q = 0; q < 6; ++q) row = fma(at(r, q), m[q], row);
-      D = fma(m[r], row, D);
+    double D;
+    if (i < 3) {
+      D = at(i, i);
+    } else {
+      // m = (-ck; e_k): m^T C' m = ck^T C'_tt ck - 2 ck^T C'_t,(3+k) + C'_(3+k),(3+k)
+      const double m0 = -ck0, m1 = -ck1, m2 = -ck2;
+      const double r0 = at(0, 0) * m0 + at(0, 1) * m1 + at(0, 2) * m2;
+      const double r1 = at(1, 0) * m0 + at(1, 1) * m1 + at(1, 2) * m2;
+      const double r2 = at(2, 0) * m0 + at(2, 1) * m1 + at(2, 2) * m2;
+      D = m0 * r0 + m1 * r1 + m2 * r2 + 2.0 * (m0 * at(0, i) + m1 * at(1, i) + m2 * at(2, i)) + at(i, i);
     }
-    double zz = 0.0;
-#pragma unroll
-    for (int j = 0; j < 6; ++j) zz = fma(z[j], z[j], zz);
     double tinv = lane < 6 ? zz : 0.0;  // (C^-1)_ii
     double tr = lane < 6 ? D : 0.0;     // C_ii
 #pragma unroll
@@ -668,35 +710,7 @@ __device__ inline void kf_icp_solve_warp(const double* v21c, const double* bc, c
     *guarded = 0;
     return;
   }
-  if (lane == 0) {
-    // world form: b = M^T b', C = M^T C' M with M = [[I, -[c]x], [0, I]]
-    double Cp[36], Mx[36], T[36], Cw[36], bw[6], xw[6];
-    kf_make_jtj(v21c, Cp);
-    for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
-    // -[c]x in rows 0..2, columns 3..5
-    Mx[0 * 6 + 4] = cz;  Mx[0 * 6 + 5] = -cy;
-    Mx[1 * 6 + 3] = -cz; Mx[1 * 6 + 5] = cx;
-    Mx[2 * 6 + 3] = cy;  Mx[2 * 6 + 4] = -cx;
-    for (int r = 0; r < 6; ++r) {
-      double v = 0.0;
-      for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * bc[k];
-      bw[r] = v;
-    }
-    for (int r = 0; r < 6; ++r)
-      for (int cc = 0; cc < 6; ++cc) {
-        double v = 0.0;
-        for (int k = 0; k < 6; ++k) v += Cp[r * 6 + k] * Mx[k * 6 + cc];
-        T[r * 6 + cc] = v;
-      }
-    for (int r = 0; r < 6; ++r)
-      for (int cc = 0; cc < 6; ++cc) {
-        double v = 0.0;
-        for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * T[k * 6 + cc];
-        Cw[r * 6 + cc] = v;
-      }
-    kf_icp_guarded_solve(Cw, bw, xw);
-    for (int k = 0; k < 6; ++k) s_scratch[k] = xw[k];
-  }
+  if (lane == 0) kf_icp_world_guarded_step(v21c, bc, c, s_scratch);
   __syncwarp();
 #pragma unroll
   for (int k = 0; k < 6; ++k) x[k] = s_scratch[k];
@@ -812,6 +826,13 @@ struct kf_batch {
   float stage_ms[5] = {0, 0, 0, 0, 0};
   uint64_t steps = 0;
   uint64_t launches = 0;
+  // per-slot CUDA graphs of a device-frame step (input addresses read from the slot's
+  // pinned list at replay), valid while the tables and launch shapes they were captured
+  // with are (graph_n members); kernels per replay
+  cudaGraphExec_t step_exec[2] = {nullptr, nullptr};
+  int graph_n[2] = {0, 0};
+  uint64_t graph_kernels[2] = {0, 0};
+  uint64_t graph_replays = 0;
 };
 
 // Reserves `bytes` in the host table (256-byte aligned); returns the matching device
@@ -880,9 +901,12 @@ int kf_launch_raycast(kf_session* s);
 int kf_launch_integrate_shape(kf_session* s, int gated, int zc, const kf_scratch_target* t);
 int kf_launch_raycast_shape(kf_session* s, int rows, const kf_scratch_target* t);
 inline bool kf_valid_int_zc(int zc) { return zc == 8 || zc == 16 || zc == 32; }
-inline bool kf_valid_ray_rows(int r) { return r == 2 || r == 4 || r == 8; }
+// raycast shapes: 32 x rows tiles (2, 4, 8), or 1 = the persistent sweep (sessions only)
+inline bool kf_valid_ray_rows(int r) { return r == 1 || r == 2 || r == 4 || r == 8; }
+inline bool kf_valid_batch_ray_rows(int r) { return r == 2 || r == 4 || r == 8; }
 constexpr int kf_tune_int_zc[3] = {8, 16, 32};
-constexpr int kf_tune_ray_rows[3] = {2, 4, 8};
+constexpr int kf_tune_ray_rows[4] = {1, 2, 4, 8};        // session autotuner
+constexpr int kf_tune_batch_ray_rows[3] = {2, 4, 8};     // batch autotuner
 // Scratch copies of a session's volume, brick flags and control block plus scratch maps,
 // for timing launches without touching the session (kf_capi.cu).
 int kf_scratch_alloc(kf_session* s, kf_scratch_target* t);
@@ -906,4 +930,6 @@ int kf_mc_run(kf_session* s, float iso, int method, uint32_t* n_tri);
 int kf_scan_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* d_total,
                 cudaStream_t stream, uint32_t* d_scratch, size_t scratch_words);
 size_t kf_scan_scratch_words(uint64_t n);
-int kf_occupancy_blocks(kf_session* s, const void* kernel, int threads, size_t smem);
+// Co-resident blocks of `kernel` on the session's device: min(per SM, max_per_sm) x SMs
+// (with the default 2, capped at KF_MAX_TRACK_BLOCKS for the tracking kernels).
+int kf_occupancy_blocks(kf_session* s, const void* kernel, int threads, size_t smem, int max_per_sm = 2);

@@ -75,37 +75,10 @@ struct Sampler {
   }
 };
 
-// BATCH: blockIdx.z selects the session's arguments in `many`.
-template <int S, bool BATCH, int ROWS>
-__global__ void __launch_bounds__(32 * ROWS) raycast_kernel(RayArgs one, const RayArgs* many) {
-  static_assert(ROWS == 2 || ROWS == 4 || ROWS == 8, "raycast tile rows: 2, 4 or 8");
-  __shared__ RayArgs s_args;
-  __shared__ float s_view[12];  // rows of m_pose * invK: (R K^-1 | t)
-  if constexpr (BATCH) {
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    const int* src = reinterpret_cast<const int*>(many + blockIdx.z);
-    for (int k = tid; k < (int)(sizeof(RayArgs) / 4); k += 32 * ROWS) reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
-    __syncthreads();
-  }
-  const RayArgs& a = BATCH ? s_args : one;
-  if (threadIdx.y == 0 && threadIdx.x < 12) {
-    // view = m_pose * invK (gFusion.cpp:1296) from the FP32 pose rows and float invK
-    const int r = threadIdx.x >> 2, c = threadIdx.x & 3;
-    const float* P = a.st->pose_rows;
-    float v;
-    if (c == 0) v = P[r * 4 + 0] * a.ikx;
-    else if (c == 1) v = P[r * 4 + 1] * a.iky;
-    else if (c == 2) v = fmaf(P[r * 4 + 0], a.ikcx, fmaf(P[r * 4 + 1], a.ikcy, P[r * 4 + 2]));
-    else v = P[r * 4 + 3];
-    s_view[r * 4 + c] = v;
-  }
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.y == 1 && threadIdx.x < 16)
-    a.st_out->raycast_pose[threadIdx.x] = a.st->pose[threadIdx.x];
-  __syncthreads();
-  const int x = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= a.W || y >= a.H) return;
-
+// One pixel of raycast.cs:133-321 for view rows s_view (m_pose * invK): march, refine,
+// gradient normal; writes the pixel's vertex and normal.
+template <int S>
+__device__ __forceinline__ void raycast_pixel(const RayArgs& a, const float* s_view, int x, int y) {
   Sampler<S> smp;
   smp.f = reinterpret_cast<const typename Vox<S>::V*>(a.vol);
   smp.nx = a.nx; smp.ny = a.ny; smp.nz = a.nz;
@@ -281,6 +254,76 @@ __global__ void __launch_bounds__(32 * ROWS) raycast_kernel(RayArgs one, const R
   } else {
     a.out_v[o] = make_float4(0.f, 0.f, 0.f, 0.f);
     a.out_n[o] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// view = m_pose * invK (gFusion.cpp:1296) from the FP32 pose rows and float invK; thread
+// t < 12 writes element t of the 3x4 rows.
+__device__ __forceinline__ void raycast_view(const RayArgs& a, float* s_view, int t) {
+  const int r = t >> 2, c = t & 3;
+  const float* P = a.st->pose_rows;
+  float v;
+  if (c == 0) v = P[r * 4 + 0] * a.ikx;
+  else if (c == 1) v = P[r * 4 + 1] * a.iky;
+  else if (c == 2) v = fmaf(P[r * 4 + 0], a.ikcx, fmaf(P[r * 4 + 1], a.ikcy, P[r * 4 + 2]));
+  else v = P[r * 4 + 3];
+  s_view[r * 4 + c] = v;
+}
+
+// BATCH: blockIdx.z selects the session's arguments in `many`.
+template <int S, bool BATCH, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS) raycast_kernel(RayArgs one, const RayArgs* many) {
+  static_assert(ROWS == 2 || ROWS == 4 || ROWS == 8, "raycast tile rows: 2, 4 or 8");
+  __shared__ RayArgs s_args;
+  __shared__ float s_view[12];  // rows of m_pose * invK: (R K^-1 | t)
+  if constexpr (BATCH) {
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int* src = reinterpret_cast<const int*>(many + blockIdx.z);
+    for (int k = tid; k < (int)(sizeof(RayArgs) / 4); k += 32 * ROWS) reinterpret_cast<int*>(&s_args)[k] = __ldg(src + k);
+    __syncthreads();
+  }
+  const RayArgs& a = BATCH ? s_args : one;
+  if (threadIdx.y == 0 && threadIdx.x < 12) raycast_view(a, s_view, threadIdx.x);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.y == 1 && threadIdx.x < 16)
+    a.st_out->raycast_pose[threadIdx.x] = a.st->pose[threadIdx.x];
+  __syncthreads();
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= a.W || y >= a.H) return;
+  raycast_pixel<S>(a, s_view, x, y);
+}
+
+// The same rays as a persistent sweep: one block per resident slot, and every warp takes
+// the next row segment of 32 pixels from a device counter until the image is done, so no
+// warp waits for another and long rays do not leave SMs idle at the end of the launch.
+// The last warp to find the queue empty resets the counter (and its own completion count)
+// for the next launch.  Every pixel runs raycast_pixel: the maps are the tiled kernel's.
+template <int S>
+__global__ void __launch_bounds__(256) raycast_sweep_kernel(RayArgs a, unsigned* queue) {
+  __shared__ float s_view[12];
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 12) raycast_view(a, s_view, threadIdx.x);
+  if (blockIdx.x == 0 && threadIdx.x >= 32 && threadIdx.x < 48)
+    a.st_out->raycast_pose[threadIdx.x - 32] = a.st->pose[threadIdx.x - 32];
+  __syncthreads();
+  const int segs_x = (a.W + 31) / 32;
+  const unsigned nseg = (unsigned)segs_x * (unsigned)a.H;
+  for (;;) {
+    unsigned seg = 0;
+    if (lane == 0) seg = atomicAdd(queue, 1u);
+    seg = __shfl_sync(0xffffffffu, seg, 0);
+    if (seg >= nseg) break;
+    const int y = (int)(seg / (unsigned)segs_x);
+    const int x = (int)(seg % (unsigned)segs_x) * 32 + lane;
+    if (x < a.W) raycast_pixel<S>(a, s_view, x, y);
+  }
+  // every warp drew one ticket past the end; the last of them resets the queue
+  if (lane == 0) {
+    const unsigned warps = gridDim.x * (blockDim.x / 32);
+    if (atomicAdd(queue + 1, 1u) == warps - 1) {
+      queue[0] = 0u;
+      queue[1] = 0u;
+    }
   }
 }
 
@@ -496,6 +539,23 @@ RayArgs retarget(RayArgs a, const kf_scratch_target* t) {
 
 int kf_launch_raycast_shape(kf_session* s, int rows, const kf_scratch_target* t) {
   const RayArgs a = retarget(make_ray_args(s), t);
+  if (rows == 1) {
+    // persistent sweep: every resident slot of 256 threads, the queue in the session state
+    const void* fn = s->cfg.storage == KF_STORAGE_F32F32   ? (const void*)raycast_sweep_kernel<KF_STORAGE_F32F32>
+                     : s->cfg.storage == KF_STORAGE_F16U16 ? (const void*)raycast_sweep_kernel<KF_STORAGE_F16U16>
+                                                           : (const void*)raycast_sweep_kernel<KF_STORAGE_RG16I>;
+    const int blocks = kf_occupancy_blocks(s, fn, 256, 0, 64);
+    if (blocks <= 0) return KF_ERR_CUDA;
+    unsigned* q = s->d_state->ray_queue;
+    switch (s->cfg.storage) {
+      case KF_STORAGE_F32F32: raycast_sweep_kernel<KF_STORAGE_F32F32><<<blocks, 256, 0, s->stream>>>(a, q); break;
+      case KF_STORAGE_F16U16: raycast_sweep_kernel<KF_STORAGE_F16U16><<<blocks, 256, 0, s->stream>>>(a, q); break;
+      default: raycast_sweep_kernel<KF_STORAGE_RG16I><<<blocks, 256, 0, s->stream>>>(a, q); break;
+    }
+    KF_CUDA_TRY(s, cudaGetLastError());
+    kf_note_launch(s);
+    return KF_OK;
+  }
   dim3 grid((a.W + 31) / 32, (a.H + rows - 1) / rows);
   launch_ray<false>(s->cfg.storage, rows, grid, s->stream, a, nullptr);
   KF_CUDA_TRY(s, cudaGetLastError());

@@ -40,6 +40,7 @@ struct Slot {
   uint64_t done = 0;
   int tracked = 0;
   double pose[16];
+  int ring_in_flight = 0;  // host-submitted frames of this session in the step in flight
 };
 
 }  // namespace
@@ -61,6 +62,12 @@ struct kf_server {
   std::vector<int32_t> step_tracked;
   std::vector<double> step_poses;
   int last_n = 0;
+  // the asynchronous step in flight (kf_server_step_async): its sessions' ids, their frames'
+  // arrival times and whether each frame came from the session's staging ring
+  std::vector<int> fl_ids;
+  std::vector<double> fl_arrival;
+  std::vector<char> fl_ring;
+  bool in_flight = false;
 };
 
 namespace {
@@ -127,6 +134,7 @@ int kf_server_create(const kf_server_config* cfg, kf_server** out) {
 
 int kf_server_destroy(kf_server* v) {
   if (!v) return KF_ERR_INVALID_ARGUMENT;
+  if (v->in_flight && v->batch) kf_batch_sync(v->batch);
   for (auto& sl : v->slots) {
     if (sl.s) kf_destroy(sl.s);
     cudaFree(sl.d_ring);
@@ -258,6 +266,12 @@ int kf_server_prewarm(kf_server* v, const kf_config* cfg, const kf_intrinsics* i
 int kf_server_close(kf_server* v, int id) {
   Slot* sl = slot_of(v, id);
   if (!sl) return KF_ERR_INVALID_ARGUMENT;
+  if (v->in_flight && std::find(v->fl_ids.begin(), v->fl_ids.end(), id) != v->fl_ids.end()) {
+    // the session is in the step in flight: finish that step first (its results are then
+    // what kf_server_last_step describes)
+    int n = 0;
+    if (int rc = kf_server_sync(v, &n)) return rc;
+  }
   sl->queue.clear();
   v->idle.push_back(*sl);  // kept for reuse; its bytes stay counted
   *sl = Slot();
@@ -267,7 +281,7 @@ int kf_server_close(kf_server* v, int id) {
 int kf_server_submit(kf_server* v, int id, const uint16_t* host_depth_mm) {
   Slot* sl = slot_of(v, id);
   if (!sl || !host_depth_mm) return KF_ERR_INVALID_ARGUMENT;
-  int host_queued = 0;
+  int host_queued = sl->ring_in_flight;  // a frame in flight still occupies its ring slot
   for (const Frame& f : sl->queue)
     if (f.d_depth >= sl->d_ring && f.d_depth < sl->d_ring + (size_t)kRing * sl->s->W[0] * sl->s->H[0]) ++host_queued;
   if (host_queued >= kRing) return sfail(v, KF_ERR_CAPACITY, "session frame queue full");
@@ -289,46 +303,27 @@ int kf_server_submit_device(kf_server* v, int id, const uint16_t* device_depth_m
   return KF_OK;
 }
 
-int kf_server_step(kf_server* v, int* n_done) {
-  if (!v) return KF_ERR_INVALID_ARGUMENT;
-  if (n_done) *n_done = 0;
-  // sessions with a waiting frame, oldest waiting frame first
-  v->step_ids.clear();
-  for (int k = 0; k < (int)v->slots.size(); ++k)
-    if (v->slots[k].s && !v->slots[k].queue.empty()) v->step_ids.push_back(k);
-  if (v->step_ids.empty()) {
-    v->last_n = 0;
-    return KF_OK;
-  }
-  std::stable_sort(v->step_ids.begin(), v->step_ids.end(), [&](int a, int b) {
-    return v->slots[a].queue.front().t_arrival < v->slots[b].queue.front().t_arrival;
-  });
-  if ((int)v->step_ids.size() > v->cfg.max_batch) v->step_ids.resize(v->cfg.max_batch);
-  // a stable member order keeps the batch's argument tables from being rebuilt when the
-  // same sessions step again
-  std::sort(v->step_ids.begin(), v->step_ids.end());
-  const int n = (int)v->step_ids.size();
-  v->step_sessions.resize(n);
-  v->step_frames.resize(n);
+}  // extern "C"
+
+namespace {
+
+// Records the results of the step in flight (its poses and flags are the batch's last
+// read step): per-frame latency, the sessions' poses and counts.
+void complete_in_flight(kf_server* v, int* n_done) {
+  const int n = (int)v->fl_ids.size();
+  const double t = now_s();
+  v->step_ids = v->fl_ids;
   v->step_tracked.resize(n);
-  for (int e = 0; e < n; ++e) {
-    Slot& sl = v->slots[v->step_ids[e]];
-    v->step_sessions[e] = sl.s;
-    v->step_frames[e] = sl.queue.front().d_depth;
-  }
-  if (cudaStreamSynchronize(v->copy_stream) != cudaSuccess) return sfail(v, KF_ERR_CUDA, "frame upload failed");
-  const double t0 = now_s();
-  int rc = kf_batch_frame_step_u16_device(v->batch, v->step_sessions.data(), v->step_frames.data(), n,
-                                          v->step_tracked.data());
-  if (rc) return sfail(v, rc, std::string("batch step: ") + kf_batch_last_error(v->batch));
-  const double t1 = now_s();
-  v->busy_s += t1 - t0;
   v->step_poses.resize((size_t)16 * n);
   kf_batch_get_poses(v->batch, n, v->step_poses.data());
+  kf_batch_get_tracked(v->batch, n, v->step_tracked.data());
+  float ms[5] = {0, 0, 0, 0, 0};
+  kf_batch_get_stage_times(v->batch, ms);
+  v->busy_s += (ms[0] + ms[1] + ms[2] + ms[3] + ms[4]) / 1000.0;
   for (int e = 0; e < n; ++e) {
-    Slot& sl = v->slots[v->step_ids[e]];
-    v->latency_ms.push_back((float)(1000.0 * (t1 - sl.queue.front().t_arrival)));
-    sl.queue.pop_front();
+    Slot& sl = v->slots[v->fl_ids[e]];
+    v->latency_ms.push_back((float)(1000.0 * (t - v->fl_arrival[e])));
+    if (v->fl_ring[e]) sl.ring_in_flight -= 1;
     sl.done += 1;
     sl.tracked = v->step_tracked[e];
     std::memcpy(sl.pose, &v->step_poses[(size_t)16 * e], sizeof(sl.pose));
@@ -336,7 +331,99 @@ int kf_server_step(kf_server* v, int* n_done) {
   v->last_n = n;
   v->frames += (uint64_t)n;
   v->steps += 1;
+  v->in_flight = false;
+  v->fl_ids.clear();
   if (n_done) *n_done = n;
+}
+
+// One batched step over the sessions with a waiting frame (oldest waiting frame first, up
+// to max_batch).  async: the step is enqueued and the previous one completed (when no frame
+// waits, the step in flight is waited for); otherwise the step is run to completion.
+int server_step(kf_server* v, bool async, int* n_done) {
+  if (!v) return KF_ERR_INVALID_ARGUMENT;
+  if (n_done) *n_done = 0;
+  // sessions with a waiting frame, oldest waiting frame first
+  std::vector<int> ids;
+  for (int k = 0; k < (int)v->slots.size(); ++k)
+    if (v->slots[k].s && !v->slots[k].queue.empty()) ids.push_back(k);
+  if (ids.empty()) {
+    if (v->in_flight) {
+      if (int rc = kf_batch_sync(v->batch)) {
+        v->in_flight = false;
+        return sfail(v, rc, std::string("batch step: ") + kf_batch_last_error(v->batch));
+      }
+      complete_in_flight(v, n_done);
+    } else {
+      v->last_n = 0;
+    }
+    return KF_OK;
+  }
+  std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
+    return v->slots[a].queue.front().t_arrival < v->slots[b].queue.front().t_arrival;
+  });
+  if ((int)ids.size() > v->cfg.max_batch) ids.resize(v->cfg.max_batch);
+  // a stable member order keeps the batch's argument tables (and its step graphs) from being
+  // rebuilt when the same sessions step again
+  std::sort(ids.begin(), ids.end());
+  const int n = (int)ids.size();
+  v->step_sessions.resize(n);
+  v->step_frames.resize(n);
+  std::vector<double> arrival(n);
+  std::vector<char> ring(n);
+  for (int e = 0; e < n; ++e) {
+    Slot& sl = v->slots[ids[e]];
+    const Frame f = sl.queue.front();
+    sl.queue.pop_front();
+    v->step_sessions[e] = sl.s;
+    v->step_frames[e] = f.d_depth;
+    arrival[e] = f.t_arrival;
+    ring[e] = f.d_depth >= sl.d_ring && f.d_depth < sl.d_ring + (size_t)kRing * sl.s->W[0] * sl.s->H[0];
+    if (ring[e]) sl.ring_in_flight += 1;
+  }
+  if (cudaStreamSynchronize(v->copy_stream) != cudaSuccess) return sfail(v, KF_ERR_CUDA, "frame upload failed");
+  // enqueue this step; the batch completes the previous one (its results are then readable)
+  const int rc = kf_batch_frame_step_u16_device_async(v->batch, v->step_sessions.data(), v->step_frames.data(), n);
+  const bool had = v->in_flight;
+  if (had && !rc) complete_in_flight(v, n_done);
+  v->fl_ids = ids;
+  v->fl_arrival = arrival;
+  v->fl_ring = ring;
+  v->in_flight = true;
+  if (rc) {
+    v->in_flight = false;
+    v->fl_ids.clear();
+    return sfail(v, rc, std::string("batch step: ") + kf_batch_last_error(v->batch));
+  }
+  if (!async) {
+    // synchronous: wait for this step and return its results
+    if (int r = kf_batch_sync(v->batch)) {
+      v->in_flight = false;
+      return sfail(v, r, std::string("batch step: ") + kf_batch_last_error(v->batch));
+    }
+    int done_now = 0;
+    complete_in_flight(v, &done_now);
+    if (n_done) *n_done += done_now;
+  }
+  return KF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kf_server_step(kf_server* v, int* n_done) { return server_step(v, false, n_done); }
+
+int kf_server_step_async(kf_server* v, int* n_done) { return server_step(v, true, n_done); }
+
+int kf_server_sync(kf_server* v, int* n_done) {
+  if (!v) return KF_ERR_INVALID_ARGUMENT;
+  if (n_done) *n_done = 0;
+  if (!v->in_flight) return KF_OK;
+  if (int rc = kf_batch_sync(v->batch)) {
+    v->in_flight = false;
+    return sfail(v, rc, std::string("batch step: ") + kf_batch_last_error(v->batch));
+  }
+  complete_in_flight(v, n_done);
   return KF_OK;
 }
 

@@ -17,8 +17,9 @@ import numpy as np
 from . import _lib as L
 
 
-def _tune_times(t) -> dict:
-    names = ["integrate_z8", "integrate_z16", "integrate_z32", "raycast_rows2", "raycast_rows4", "raycast_rows8"]
+def _tune_times(t, sweep: bool = True) -> dict:
+    names = ["integrate_z8", "integrate_z16", "integrate_z32"] + (["raycast_sweep"] if sweep else []) + \
+            ["raycast_rows2", "raycast_rows4", "raycast_rows8"]
     return {n: float(v) for n, v in zip(names, t)}
 
 
@@ -337,7 +338,7 @@ class GFusion:
         """Time every integrate z-chunk and raycast tile shape on the current frame and use
         the fastest.  Returns ((z_chunk, rows), {shape name: mean ms})."""
         sh = L.kf_launch_shape()
-        t = (C.c_float * 6)()
+        t = (C.c_float * 7)()
         self._check(self.lib.kf_autotune(self._h, int(repeats), C.byref(sh), t), "kf_autotune")
         return (sh.integrate_z_chunk, sh.raycast_rows), _tune_times(t)
 
@@ -515,7 +516,7 @@ class GFusionBatch:
         sh = L.kf_launch_shape()
         t = (C.c_float * 6)()
         self._check(self.lib.kf_batch_autotune(self._h, hs, n, int(repeats), C.byref(sh), t), "kf_batch_autotune")
-        return (sh.integrate_z_chunk, sh.raycast_rows), _tune_times(t)
+        return (sh.integrate_z_chunk, sh.raycast_rows), _tune_times(t, sweep=False)
 
 
 class GFusionServer:
@@ -585,6 +586,18 @@ class GFusionServer:
     def step(self) -> int:
         n = C.c_int()
         self._check(self.lib.kf_server_step(self._h, C.byref(n)), "kf_server_step")
+        return n.value
+
+    def step_async(self) -> int:
+        """Enqueue a step; returns the frame count of the previous step, whose results are
+        now readable (last_step, pose)."""
+        n = C.c_int()
+        self._check(self.lib.kf_server_step_async(self._h, C.byref(n)), "kf_server_step_async")
+        return n.value
+
+    def sync(self) -> int:
+        n = C.c_int()
+        self._check(self.lib.kf_server_sync(self._h, C.byref(n)), "kf_server_sync")
         return n.value
 
     def pose(self, sid: int):

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_host_only_entry_points():
     lib = L.load()
-    assert lib.kf_abi_version() == 1
+    assert lib.kf_abi_version() == 2
     c = L.kf_config()
     assert lib.kf_config_default(C.byref(c)) == L.KF_OK
     # gFusionConfig() defaults (gFusion.h:56-69)

@@ -12,7 +12,7 @@ from oglfusionkinectv2_b200 import GFusion, GFusionBatch, _lib as L
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = list(itertools.product((8, 16, 32), (2, 4, 8)))
+SHAPES = list(itertools.product((8, 16, 32), (1, 2, 4, 8)))  # rows 1: the persistent sweep
 
 
 def _state(g):
@@ -54,9 +54,9 @@ def test_autotune_leaves_state_untouched_and_is_remembered():
         b.frameStep(w.frame(k))
     before = _state(a)
     shape, times = a.autotune(repeats=3)
-    assert shape[0] in (8, 16, 32) and shape[1] in (2, 4, 8)
+    assert shape[0] in (8, 16, 32) and shape[1] in (1, 2, 4, 8)
     assert a.launchShape() == shape
-    assert len(times) == 6 and all(0 < t < 100 for t in times.values())
+    assert len(times) == 7 and all(0 < t < 100 for t in times.values())
     _assert_same(_state(a), before)
     for k in range(4, 8):
         assert a.frameStep(w.frame(k)) == b.frameStep(w.frame(k))
@@ -75,6 +75,11 @@ def test_invalid_shapes_are_rejected():
         assert e.value.status == L.KF_ERR_INVALID_ARGUMENT
     with pytest.raises(L.KfError):
         g.autotune(repeats=0)
+    # the persistent raycast sweep is a session shape only
+    batch = GFusionBatch(2)
+    with pytest.raises(L.KfError) as e:
+        batch.setLaunchShape(16, 1)
+    assert e.value.status == L.KF_ERR_INVALID_ARGUMENT
 
 
 def test_batch_autotune_keeps_results_exact():

@@ -181,3 +181,27 @@ def test_batch_async_steps_match_sync_steps():
     assert b2.tracked(len(ws)).all()
     for ga, gb in zip(sync_s, async_s):
         assert_same(snapshot(ga), snapshot(gb))
+
+
+def test_batch_step_graphs_match_direct_launches():
+    """Device-frame steps run as per-slot CUDA graphs (captured on first use, replayed,
+    recaptured when the membership changes); host-frame steps launch directly.  Both take
+    the sessions to the same bits, across a membership change."""
+    import torch
+    F = 6
+    ws = workloads(F)
+    frames = [[w.frame(k) for k in range(F)] for w in ws]
+    dev = [torch.from_numpy(np.stack(fr).view(np.int16)).cuda() for fr in frames]
+    fbytes = 512 * 424 * 2
+    direct, graphed = fresh(ws), fresh(ws)
+    b1, b2 = GFusionBatch(4), GFusionBatch(4)
+    torch.cuda.synchronize()
+    for k in range(F):
+        members = range(len(ws)) if k < 3 or k >= 5 else range(1, len(ws))  # session 0 sits out
+        b1.frameStep([direct[i] for i in members], [frames[i][k] for i in members])
+        b2.frameStepDevice([graphed[i] for i in members], [dev[i].data_ptr() + k * fbytes for i in members])
+        np.testing.assert_array_equal(b1.poses(len(members)), b2.poses(len(members)))
+    for ga, gb in zip(direct, graphed):
+        assert_same(snapshot(ga), snapshot(gb))
+    # a replayed graph counts its kernels like direct launches do
+    assert b2.launchCount() == b1.launchCount()

@@ -119,3 +119,46 @@ def test_server_prewarm_and_eviction():
     assert v.step() == 2
     np.testing.assert_array_equal(v.pose(a)[0], alone_poses(ws[0], f[:1])[-1])
     np.testing.assert_array_equal(v.pose(b)[0], alone_poses(ws[1], f[1:])[-1])
+
+
+def test_server_async_steps_match_alone():
+    """Asynchronous served steps: each call enqueues a step and returns the previous one's
+    frame count; submissions and an admission happen while a step is on the device, and
+    every session's poses equal running it alone."""
+    F = 5
+    ws = workloads(F)
+    frames = [[w.frame(k) for k in range(F)] for w in ws]
+    ref = [alone_poses(w, fr) for w, fr in zip(ws, frames)]
+    v = GFusionServer(max_sessions=3, max_batch=3)
+    a = v.open(ws[0].config, ws[0].intrinsics, ws[0].poses[0])
+    b = v.open(ws[1].config, ws[1].intrinsics, ws[1].poses[0])
+    seen = {a: [], b: []}
+
+    def collect(n):
+        if n:
+            ids, poses, _ = v.last_step(3)
+            assert len(ids) == n
+            for sid, P in zip(ids.tolist(), poses):
+                seen[sid].append(P)
+
+    c = None
+    for k in range(F):
+        v.submit(a, frames[0][k])
+        v.submit(b, frames[1][k])
+        if k == 2:
+            c = v.open(ws[2].config, ws[2].intrinsics, ws[2].poses[0])  # joins mid-stream
+            seen[c] = []
+        if c is not None:
+            v.submit(c, frames[2][k - 2])
+        collect(v.step_async())
+    for k in range(F - 2, F):  # c's remaining frames, one step each
+        v.submit(c, frames[2][k])
+        collect(v.step_async())
+    collect(v.sync())
+    assert v.sync() == 0
+    assert v.stats()["frames"] == 3 * F
+    for sid, r in ((a, ref[0]), (b, ref[1]), (c, ref[2])):
+        assert len(seen[sid]) == F
+        for P, Q in zip(seen[sid], r):
+            np.testing.assert_array_equal(P, Q)
+    v.close_session(c)
