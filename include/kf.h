@@ -90,6 +90,12 @@ extern "C" {
                                             gFusion.cpp:747-755                          */
 #define KF_Q19_EIG_TRANSLATION (1u << 8) /* resetPose seeds the SDF pose chain with the     \
                                             translation only, gFusion.cpp:275-287         */
+#define KF_Q24_MC_SHADER_UNITS (1u << 11) /* the scan (classic) marching-cubes path writes  \
+                                            marchingCubes.cs's units: corners at           \
+                                            -1 + gridPos * voxelSize, vertex / 128 *       \
+                                            voxelSize.x with z negated, w = 1, voxelSize = \
+                                            1000 * dim / size (mcubes.h:30-39); clear:     \
+                                            voxel-index units (marchingCubes.cs:205-299)   */
 /* Exactly the reference's behaviour. */
 #define KF_QUIRKS_REFERENCE                                                                  \
   (KF_Q1_LAST_GROUP_ONLY | KF_Q3_DOWN_FROM_LEFT | KF_Q4_SAME_PIXEL | KF_Q6_SDF_D2_TWICE |      \
@@ -434,10 +440,34 @@ KF_API int kf_server_reset_stats(kf_server* v);
  * w = 0 (traverseHistoPyramids.cs:218-241). */
 KF_API int kf_mc_extract(kf_session* s, float iso, int method, uint32_t* n_triangles);
 KF_API int kf_mc_copy_vertices(kf_session* s, float* vertex4, uint64_t max_vertices);
+/* Per vertex of the last extraction, its triangle's face normal cross(v1 - v0, v2 - v0),
+ * unnormalised, w = 0: calcNormal of marchingCubes.cs:87-93, written to norm[] at :290-299
+ * (in the units the positions were computed in, before the Q24 output scaling); the
+ * histoPyramid path, which writes no normals in the reference, gets the same. */
+KF_API int kf_mc_copy_normals(kf_session* s, float* normal4, uint64_t max_vertices);
 /* Base level: numTri | cubeIndex << 16 per cube (RG16UI, histoPyramids.cs:170). */
 KF_API int kf_mc_copy_base_level(kf_session* s, uint32_t* base, uint64_t count);
 KF_API int kf_mc_export_stl(kf_session* s, const char* path);  /* exportMesh, :429-509 */
 KF_API int kf_mc_export_ply(kf_session* s, const char* path);  /* exportPointCloud, :391-427 */
+
+/* Welded mesh for export (no counterpart in the reference: exportMesh writes the triangle
+ * soup with the normal (1,1,1), mcubes.cpp:451-500).  Extracted on the device from the
+ * current volume with the classic path's corner order and case table (marchingCubes.cs)
+ * over the interior cubes: one vertex per cut voxel edge that a triangle uses, numbered in
+ * voxel order then axis (x, y, z), so the numbering does not depend on the launch;
+ * positions in world metres ((voxel index + 0.5) * dim / size, integrate.cs:16-19);
+ * normals the unit TSDF gradient (central differences at the edge's two voxels,
+ * interpolated); triangles as three vertex indices, counter-clockwise seen from the
+ * positive (free-space) side, so facet normals follow the gradient. */
+KF_API int kf_mc_extract_mesh(kf_session* s, float iso, uint32_t* n_vertices, uint32_t* n_triangles);
+/* Copies of the last welded mesh (any pointer may be NULL): 3 floats per vertex position
+ * and normal, 3 indices per triangle. */
+KF_API int kf_mc_copy_mesh(kf_session* s, float* positions3, float* normals3, uint32_t* indices3,
+                           uint64_t max_vertices, uint64_t max_triangles);
+/* Binary little-endian PLY (vertex x y z nx ny nz, face lists) and binary STL (zeroed
+ * header, true triangle count, unit facet normals) of the last welded mesh. */
+KF_API int kf_mc_export_mesh_ply(kf_session* s, const char* path);
+KF_API int kf_mc_export_mesh_stl(kf_session* s, const char* path);
 
 /* ---- prefix sum (prefixSum.cs, MCubes::prefixSum mcubes.cpp:136-204) --------------------
  * Exclusive scan of n uint32 device values on `stream` (0 = legacy default); *total, if

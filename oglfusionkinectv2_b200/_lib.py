@@ -42,6 +42,7 @@ KF_Q15_MC_BORDER_SKIP = 1 << 5
 KF_Q18_STL_COUNT_X4 = 1 << 6
 KF_Q23_SDF_XY_OFFSET = 1 << 7
 KF_Q19_EIG_TRANSLATION = 1 << 8
+KF_Q24_MC_SHADER_UNITS = 1 << 11
 KF_Q8_NARROW_BAND = 1 << 9
 KF_Q4_SAME_PIXEL = 1 << 10
 KF_QUIRKS_REFERENCE = (KF_Q1_LAST_GROUP_ONLY | KF_Q3_DOWN_FROM_LEFT | KF_Q4_SAME_PIXEL
@@ -164,6 +165,11 @@ SIGNATURES = {
     "kf_mc_copy_base_level": (_I, [_P, _P, C.c_uint64]),
     "kf_mc_export_stl": (_I, [_P, C.c_char_p]),
     "kf_mc_export_ply": (_I, [_P, C.c_char_p]),
+    "kf_mc_copy_normals": (_I, [_P, _P, C.c_uint64]),
+    "kf_mc_extract_mesh": (_I, [_P, C.c_float, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "kf_mc_copy_mesh": (_I, [_P, _P, _P, _P, C.c_uint64, C.c_uint64]),
+    "kf_mc_export_mesh_ply": (_I, [_P, C.c_char_p]),
+    "kf_mc_export_mesh_stl": (_I, [_P, C.c_char_p]),
     "kf_prefix_sum_u32": (_I, [_P, _P, C.c_uint64, C.POINTER(C.c_uint32), _P]),
     "kf_prefix_sum_u32_noalloc": (_I, [_P, _P, C.c_uint64, C.POINTER(C.c_uint32), _P]),
     "kf_batch_create": (_I, [_I, C.POINTER(_P)]),

@@ -77,8 +77,21 @@ void free_mc(kf_session* s) {
   cudaFree(s->d_mc_scratch);
   s->d_mc_scratch = nullptr;
   s->mc_scratch_words = 0;
+  cudaFree(s->d_mc_normals);
+  s->d_mc_normals = nullptr;
+  s->mc_normal_cap = 0;
   s->mc_valid = 0;
   s->mc_triangles = 0;
+  cudaFree(s->d_mesh_mask);
+  cudaFree(s->d_mesh_scratch);
+  cudaFree(s->d_mesh_pos);
+  cudaFree(s->d_mesh_nrm);
+  cudaFree(s->d_mesh_idx);
+  s->d_mesh_mask = s->d_mesh_scratch = s->d_mesh_idx = nullptr;
+  s->d_mesh_pos = s->d_mesh_nrm = nullptr;
+  s->mesh_mask_cap = s->mesh_scratch_cap = s->mesh_pos_cap = s->mesh_nrm_cap = s->mesh_idx_cap = 0;
+  s->mesh_vertices = s->mesh_triangles = 0;
+  s->mesh_valid = 0;
 }
 
 void drop_graph(kf_session* s) {

@@ -162,6 +162,19 @@ struct kf_session {
   int mc_P = 0, mc_top = 0;
   float4* d_mc_vertices = nullptr;
   size_t mc_vertex_cap = 0;
+  float4* d_mc_normals = nullptr;  // face normal of each soup vertex's triangle (w = 0)
+  size_t mc_normal_cap = 0;
+  // welded mesh (kf_mc_extract_mesh): one vertex per cut voxel edge, indexed triangles
+  uint32_t* d_mesh_mask = nullptr;  // edge bits, 10 voxels x 3 axes per word
+  size_t mesh_mask_cap = 0;
+  uint32_t* d_mesh_scratch = nullptr;  // triangle counts/offsets, word offsets, scan scratch
+  size_t mesh_scratch_cap = 0;
+  float* d_mesh_pos = nullptr;  // 3 floats per vertex (metres)
+  float* d_mesh_nrm = nullptr;  // 3 floats per vertex (unit)
+  uint32_t* d_mesh_idx = nullptr;  // 3 per triangle
+  size_t mesh_pos_cap = 0, mesh_nrm_cap = 0, mesh_idx_cap = 0;
+  uint32_t mesh_vertices = 0, mesh_triangles = 0;
+  int mesh_valid = 0;
   uint32_t mc_triangles = 0;
   int mc_valid = 0;
   uint32_t* d_mc_scratch = nullptr;  // level table / scan path verts, offsets, scan scratch

@@ -665,6 +665,34 @@ class MCubes:
         f._check(f.lib.kf_mc_copy_vertices(f._h, out.ctypes.data, out.shape[0]), "kf_mc_copy_vertices")
         return out
 
+    def getNormals(self) -> np.ndarray:
+        """Face normal of each vertex's triangle (calcNormal, unnormalised, w = 0)."""
+        f = self.fusion
+        out = np.empty((3 * self.nTriangles, 4), np.float32)
+        f._check(f.lib.kf_mc_copy_normals(f._h, out.ctypes.data, out.shape[0]), "kf_mc_copy_normals")
+        return out
+
+    def extractMesh(self):
+        """Welded mesh of the current volume at the iso level: (positions n x 3 metres,
+        unit normals n x 3, triangle indices t x 3)."""
+        f = self.fusion
+        nv, nt = C.c_uint32(), C.c_uint32()
+        f._check(f.lib.kf_mc_extract_mesh(f._h, self.isoLevel, C.byref(nv), C.byref(nt)), "kf_mc_extract_mesh")
+        P = np.empty((nv.value, 3), np.float32)
+        N = np.empty((nv.value, 3), np.float32)
+        I = np.empty((nt.value, 3), np.uint32)
+        f._check(f.lib.kf_mc_copy_mesh(f._h, P.ctypes.data, N.ctypes.data, I.ctypes.data, nv.value, nt.value),
+                 "kf_mc_copy_mesh")
+        return P, N, I
+
+    def exportWeldedMeshPly(self, path: str) -> None:
+        f = self.fusion
+        f._check(f.lib.kf_mc_export_mesh_ply(f._h, path.encode()), "kf_mc_export_mesh_ply")
+
+    def exportWeldedMeshStl(self, path: str) -> None:
+        f = self.fusion
+        f._check(f.lib.kf_mc_export_mesh_stl(f._h, path.encode()), "kf_mc_export_mesh_stl")
+
     def getBaseLevel(self) -> np.ndarray:
         f = self.fusion
         nx, ny, nz = f.configuration.volumeSize

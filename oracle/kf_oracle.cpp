@@ -515,6 +515,10 @@ struct or_session {
   std::vector<uint32_t> mc_base;                /* nx*ny*nz, numTri | ci << 16 */
   std::vector<std::vector<uint32_t>> mc_levels; /* level k>=1, (P>>k)^3 */
   std::vector<float> mc_vertices;               /* 4 per vertex */
+  std::vector<float> mc_normals;                /* 4 per vertex: the face normal, w = 0 */
+  std::vector<float> mesh_pos, mesh_nrm;        /* welded mesh: 3 per vertex */
+  std::vector<uint32_t> mesh_idx;               /* 3 per triangle */
+  int mesh_valid = 0;
   uint32_t mc_triangles = 0;
   int mc_valid = 0;
 };
@@ -1230,6 +1234,18 @@ void intensity_projection(or_session* s, double* rgba) {
 const int kHpOff[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 0, 1}, {1, 0, 1},
                           {0, 1, 0}, {1, 1, 0}, {0, 1, 1}, {1, 1, 1}}; /* cubeOffsets */
 
+/* calcNormal (marchingCubes.cs:87-93): cross(v1 - v0, v2 - v0), unnormalised, for the
+ * three vertices of a triangle starting at vertex v0i; w = 0. */
+void store_face_normal(or_session* s, size_t v0i, const double P[3][3]) {
+  double e0[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
+  double e1[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
+  double n[3] = {e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2], e0[0] * e1[1] - e0[1] * e1[0]};
+  for (int k = 0; k < 3; ++k) {
+    float* o = &s->mc_normals[(v0i + k) * 4];
+    o[0] = (float)n[0]; o[1] = (float)n[1]; o[2] = (float)n[2]; o[3] = 0.0f;
+  }
+}
+
 int mc_histopyramid(or_session* s, double iso) {
   const Volume& V = s->vol;
   const int nx = V.nx, ny = V.ny, nz = V.nz;
@@ -1286,6 +1302,7 @@ int mc_histopyramid(or_session* s, double iso) {
   uint32_t total = top > 0 ? s->mc_levels[top][0] : (s->mc_base[0] & 0xffff);
   s->mc_triangles = total;
   s->mc_vertices.assign((size_t)total * 3 * 4, 0.0f);
+  s->mc_normals.assign((size_t)total * 3 * 4, 0.0f);
   auto level_val = [&](int k, int x, int y, int z) -> uint32_t {
     if (k == 0) {
       if (x >= nx || y >= ny || z >= nz) return 0;
@@ -1320,6 +1337,7 @@ int mc_histopyramid(or_session* s, double iso) {
     cx /= 2; cy /= 2; cz /= 2;
     unsigned ci = s->mc_base[V.idx(cx, cy, cz)] >> 16;
     int j = (int)(target - w);
+    double P[3][3];
     for (int k = 0; k < 3; ++k) {
       int edge = kf_mc_tri_table[ci * 16 + 3 * j + k];
       const uint8_t* o = &kf_mc_offsets3[edge * 6];
@@ -1330,9 +1348,13 @@ int mc_histopyramid(or_session* s, double iso) {
       double a = (iso - v0) / (v1 - v0);
       if (a > 1 || a < 0) a = 0.5;
       float* out = &s->mc_vertices[((size_t)t * 3 + k) * 4];
-      for (int q = 0; q < 3; ++q) out[q] = (float)(p0[q] * (1.0 - a) + p1[q] * a);
+      for (int q = 0; q < 3; ++q) {
+        P[k][q] = p0[q] * (1.0 - a) + p1[q] * a;
+        out[q] = (float)P[k][q];
+      }
       out[3] = 0.0f;
     }
+    store_face_normal(s, (size_t)t * 3, P);
   }
   return KF_OK;
 }
@@ -1376,6 +1398,11 @@ int mc_scan(or_session* s, double iso) {
   s->mc_levels.clear();
   s->mc_triangles = total_verts / 3;
   s->mc_vertices.assign((size_t)total_verts * 4, 0.0f);
+  s->mc_normals.assign((size_t)total_verts * 4, 0.0f);
+  /* Q24: the shader's units, corners at -1 + gridPos * voxelSize (launchGenerateTriangles,
+   * marchingCubes.cs:205-220), voxelSize = mCubeConfig's 1000 * dim / size */
+  const bool q24 = s->cfg.quirks & KF_Q24_MC_SHADER_UNITS;
+  const double vs[3] = {1000.0 * s->cfg.dim_x / nx, 1000.0 * s->cfg.dim_y / ny, 1000.0 * s->cfg.dim_z / nz};
 #pragma omp parallel for collapse(2) schedule(static)
   for (int z = 0; z < nz; ++z)
     for (int y = 0; y < ny; ++y)
@@ -1385,17 +1412,129 @@ int mc_scan(or_session* s, double iso) {
         double f[8];
         for (int k = 0; k < 8; ++k) f[k] = sample(x + kBourke[k][0], y + kBourke[k][1], z + kBourke[k][2]);
         unsigned ci = cis[i];
-        for (unsigned v = 0; v < verts[i]; ++v) {
-          int e = kf_mc_tri_table[ci * 16 + v];
-          int a = kBourkeEdge[e][0], b = kBourkeEdge[e][1];
-          double t = (iso - f[a]) / (f[b] - f[a]); /* vertexInterp, :81-85 */
-          float* out = &s->mc_vertices[((size_t)scan[i] + v) * 4];
-          out[0] = (float)((x + kBourke[a][0]) * (1.0 - t) + (x + kBourke[b][0]) * t);
-          out[1] = (float)((y + kBourke[a][1]) * (1.0 - t) + (y + kBourke[b][1]) * t);
-          out[2] = (float)((z + kBourke[a][2]) * (1.0 - t) + (z + kBourke[b][2]) * t);
-          out[3] = 1.0f;
+        const int g[3] = {x, y, z};
+        for (unsigned v = 0; v < verts[i]; v += 3) {
+          double P[3][3];
+          for (int k = 0; k < 3; ++k) {
+            int e = kf_mc_tri_table[ci * 16 + v + k];
+            int a = kBourkeEdge[e][0], b = kBourkeEdge[e][1];
+            double t = (iso - f[a]) / (f[b] - f[a]); /* vertexInterp, :81-85 */
+            for (int q = 0; q < 3; ++q) {
+              double pa = g[q] + kBourke[a][q], pb = g[q] + kBourke[b][q];
+              if (q24) {
+                pa = -1.0 + g[q] * vs[q] + kBourke[a][q] * vs[q];
+                pb = -1.0 + g[q] * vs[q] + kBourke[b][q] * vs[q];
+              }
+              P[k][q] = pa * (1.0 - t) + pb * t;
+            }
+          }
+          store_face_normal(s, (size_t)scan[i] + v, P);
+          for (int k = 0; k < 3; ++k) {
+            float* out = &s->mc_vertices[((size_t)scan[i] + v + k) * 4];
+            if (q24) { /* pos[index] of :290-299: / 128 * voxelSize.x, z negated */
+              out[0] = (float)(P[k][0] / 128.0 * vs[0]);
+              out[1] = (float)(P[k][1] / 128.0 * vs[0]);
+              out[2] = (float)(-(P[k][2] / 128.0) * vs[0]);
+            } else {
+              out[0] = (float)P[k][0]; out[1] = (float)P[k][1]; out[2] = (float)P[k][2];
+            }
+            out[3] = 1.0f;
+          }
         }
       }
+  return KF_OK;
+}
+
+/* ---- welded mesh: the export form of the CUDA path, restated --------------------------
+ * Interior cubes [0, n-2]^3 in the classic path's Bourke order and case table; a triangle
+ * vertex on cube edge e belongs to the edge's lower voxel and axis; used edges are numbered
+ * in voxel order, then axis; position = voxel-index point + 0.5, times dim / size (metres);
+ * normal = the unit interpolation of the central-difference gradients at the two voxels. */
+int mc_mesh(or_session* s, double iso) {
+  const Volume& V = s->vol;
+  const int nx = V.nx, ny = V.ny, nz = V.nz;
+  const bool q13 = s->cfg.quirks & KF_Q13_MC_FIRST_SEVEN;
+  const size_t n = V.count();
+  static const int owner[12][4] = {{0, 0, 0, 0}, {1, 0, 0, 1}, {0, 1, 0, 0}, {0, 0, 0, 1},
+                                   {0, 0, 1, 0}, {1, 0, 1, 1}, {0, 1, 1, 0}, {0, 0, 1, 1},
+                                   {0, 0, 0, 2}, {1, 0, 0, 2}, {1, 1, 0, 2}, {0, 1, 0, 2}};
+  std::vector<uint8_t> mark(n, 0);
+  std::vector<std::pair<size_t, unsigned>> cubes; /* (voxel, case) of cubes with triangles */
+  for (int z = 0; z + 1 < nz; ++z)
+    for (int y = 0; y + 1 < ny; ++y)
+      for (int x = 0; x + 1 < nx; ++x) {
+        double f[8];
+        for (int k = 0; k < 8; ++k) f[k] = V.raw(V.idx(x + kBourke[k][0], y + kBourke[k][1], z + kBourke[k][2]));
+        bool pos = false;
+        for (int k = 0; k < (q13 ? 7 : 8); ++k) pos |= f[k] > 0;
+        if (!pos) continue;
+        unsigned ci = 0;
+        for (int k = 0; k < 8; ++k) ci |= (unsigned)(f[k] < iso) << k;
+        if (!kf_mc_num_verts[ci]) continue;
+        cubes.emplace_back(V.idx(x, y, z), ci);
+        for (int k = 0; k < kf_mc_num_verts[ci]; ++k) {
+          const int* o = owner[kf_mc_tri_table[ci * 16 + k]];
+          mark[V.idx(x + o[0], y + o[1], z + o[2])] |= (uint8_t)(1u << o[3]);
+        }
+      }
+  std::vector<uint32_t> id(3 * n, 0xffffffffu);
+  uint32_t nv = 0;
+  for (size_t v = 0; v < n; ++v)
+    for (int a = 0; a < 3; ++a)
+      if (mark[v] >> a & 1) id[3 * v + a] = nv++;
+  s->mesh_pos.assign((size_t)nv * 3, 0.0f);
+  s->mesh_nrm.assign((size_t)nv * 3, 0.0f);
+  const int dims[3] = {nx, ny, nz};
+  const double dimm[3] = {s->cfg.dim_x, s->cfg.dim_y, s->cfg.dim_z};
+  auto val = [&](int x, int y, int z) {
+    x = std::min(std::max(x, 0), nx - 1);
+    y = std::min(std::max(y, 0), ny - 1);
+    z = std::min(std::max(z, 0), nz - 1);
+    return V.raw(V.idx(x, y, z));
+  };
+  auto grad = [&](int x, int y, int z, double* g) {
+    g[0] = (val(x + 1, y, z) - val(x - 1, y, z)) * 0.5 * nx / dimm[0];
+    g[1] = (val(x, y + 1, z) - val(x, y - 1, z)) * 0.5 * ny / dimm[1];
+    g[2] = (val(x, y, z + 1) - val(x, y, z - 1)) * 0.5 * nz / dimm[2];
+  };
+  for (size_t v = 0; v < n; ++v)
+    for (int a = 0; a < 3; ++a) {
+      if (!(mark[v] >> a & 1)) continue;
+      const uint32_t i = id[3 * v + a];
+      int p0[3] = {(int)(v % nx), (int)((v / nx) % ny), (int)(v / ((size_t)nx * ny))};
+      int p1[3] = {p0[0], p0[1], p0[2]};
+      p1[a] += 1;
+      const double f0 = V.raw(V.idx(p0[0], p0[1], p0[2])), f1 = V.raw(V.idx(p1[0], p1[1], p1[2]));
+      const double t = (iso - f0) / (f1 - f0);
+      double g0[3], g1[3], g[3];
+      grad(p0[0], p0[1], p0[2], g0);
+      grad(p1[0], p1[1], p1[2], g1);
+      for (int k = 0; k < 3; ++k) {
+        const double p = p0[k] + t * (p1[k] - p0[k]);
+        s->mesh_pos[3 * i + k] = (float)((p + 0.5) * dimm[k] / dims[k]);
+        g[k] = g0[k] + t * (g1[k] - g0[k]);
+      }
+      const double len = std::sqrt(dot3(g, g));
+      for (int k = 0; k < 3; ++k) s->mesh_nrm[3 * i + k] = (float)(len > 0 ? g[k] / len : 0.0);
+    }
+  /* each triangle (a, b, c) of the table is stored as (a, c, b): counter-clockwise seen
+   * from the positive side, its facet normal along the gradient */
+  s->mesh_idx.clear();
+  for (const auto& c : cubes) {
+    const size_t v = c.first;
+    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)(v / ((size_t)nx * ny));
+    for (int k = 0; k < kf_mc_num_verts[c.second]; k += 3) {
+      uint32_t t[3];
+      for (int q = 0; q < 3; ++q) {
+        const int* o = owner[kf_mc_tri_table[c.second * 16 + k + q]];
+        t[q] = id[3 * V.idx(x + o[0], y + o[1], z + o[2]) + o[3]];
+      }
+      s->mesh_idx.push_back(t[0]);
+      s->mesh_idx.push_back(t[2]);
+      s->mesh_idx.push_back(t[1]);
+    }
+  }
+  s->mesh_valid = 1;
   return KF_OK;
 }
 
@@ -1628,6 +1767,28 @@ int or_mc_copy_vertices(or_session* s, float* v, uint64_t max_vertices) {
   uint64_t n = (uint64_t)s->mc_triangles * 3;
   if (max_vertices < n) return KF_ERR_CAPACITY;
   std::memcpy(v, s->mc_vertices.data(), n * 16);
+  return KF_OK;
+}
+
+int or_mc_extract_mesh(or_session* s, float iso, uint32_t* nv, uint32_t* nt) {
+  int rc = mc_mesh(s, iso);
+  *nv = (uint32_t)(s->mesh_pos.size() / 3);
+  *nt = (uint32_t)(s->mesh_idx.size() / 3);
+  return rc;
+}
+
+int or_mc_copy_mesh(or_session* s, float* pos, float* nrm, uint32_t* idx) {
+  if (!s->mesh_valid) return KF_ERR_STATE;
+  std::memcpy(pos, s->mesh_pos.data(), s->mesh_pos.size() * 4);
+  std::memcpy(nrm, s->mesh_nrm.data(), s->mesh_nrm.size() * 4);
+  std::memcpy(idx, s->mesh_idx.data(), s->mesh_idx.size() * 4);
+  return KF_OK;
+}
+
+int or_mc_copy_normals(or_session* s, float* n, uint64_t max_vertices) {
+  uint64_t cnt = (uint64_t)s->mc_triangles * 3;
+  if (max_vertices < cnt) return KF_ERR_CAPACITY;
+  std::memcpy(n, s->mc_normals.data(), cnt * 16);
   return KF_OK;
 }
 

@@ -80,6 +80,9 @@ int or_get_cum_twist(or_session* s, double twist[6]);
 
 int or_mc_extract(or_session* s, float iso, int method, uint32_t* n_triangles);
 int or_mc_copy_vertices(or_session* s, float* vertex4, uint64_t max_vertices);
+int or_mc_copy_normals(or_session* s, float* n, uint64_t max_vertices);
+int or_mc_extract_mesh(or_session* s, float iso, uint32_t* nv, uint32_t* nt);
+int or_mc_copy_mesh(or_session* s, float* pos, float* nrm, uint32_t* idx);
 int or_mc_copy_base_level(or_session* s, uint32_t* base, uint64_t count);
 int or_mc_export_stl(or_session* s, const char* path);
 int or_mc_export_ply(or_session* s, const char* path);

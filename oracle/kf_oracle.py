@@ -37,6 +37,9 @@ _SIG = {
     "or_copy_volume_from_host": [_P, _P, C.c_uint64], "or_get_pose_library_size": [_P, C.POINTER(_I)],
     "or_get_cum_twist": [_P, _PD], "or_mc_extract": [_P, C.c_float, _I, C.POINTER(C.c_uint32)],
     "or_mc_copy_vertices": [_P, _P, C.c_uint64], "or_mc_copy_base_level": [_P, _P, C.c_uint64],
+    "or_mc_copy_normals": [_P, _P, C.c_uint64],
+    "or_mc_extract_mesh": [_P, C.c_float, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+    "or_mc_copy_mesh": [_P, _P, _P, _P],
     "or_mc_export_stl": [_P, C.c_char_p], "or_mc_export_ply": [_P, C.c_char_p],
     "or_prefix_sum_u32": [_P, _P, C.c_uint64, C.POINTER(C.c_uint32)],
     "or_euler_xyz": [_PD, _PD], "or_se3_exp": [_PD, _PD], "or_solve_pinv6": [_PD, _PD, _PD],
@@ -283,6 +286,21 @@ class Oracle:
         out = np.empty((3 * self._ntri, 4), np.float32)
         _ok(self.lib.or_mc_copy_vertices(self._h, out.ctypes.data, out.shape[0]), "mc_verts")
         return out
+
+    def mcNormals(self):
+        out = np.empty((3 * self._ntri, 4), np.float32)
+        _ok(self.lib.or_mc_copy_normals(self._h, out.ctypes.data, out.shape[0]), "mc_normals")
+        return out
+
+    def mcMesh(self, iso=0.0):
+        """Welded mesh: (positions n x 3, unit normals n x 3, indices t x 3)."""
+        nv, nt = C.c_uint32(), C.c_uint32()
+        _ok(self.lib.or_mc_extract_mesh(self._h, iso, C.byref(nv), C.byref(nt)), "mc_mesh")
+        P = np.empty((nv.value, 3), np.float32)
+        N = np.empty((nv.value, 3), np.float32)
+        I = np.empty((nt.value, 3), np.uint32)
+        _ok(self.lib.or_mc_copy_mesh(self._h, P.ctypes.data, N.ctypes.data, I.ctypes.data), "mc_mesh_copy")
+        return P, N, I
 
     def mcBaseLevel(self):
         nx, ny, nz = self.configuration.volumeSize

@@ -52,7 +52,7 @@ def test_quirk_presets_match_header():
     for name in ["KF_Q1_LAST_GROUP_ONLY", "KF_Q3_DOWN_FROM_LEFT", "KF_Q4_SAME_PIXEL", "KF_Q6_SDF_D2_TWICE",
                  "KF_Q7_SDF_LAST_COLUMN", "KF_Q8_NARROW_BAND", "KF_Q13_MC_FIRST_SEVEN",
                  "KF_Q15_MC_BORDER_SKIP", "KF_Q18_STL_COUNT_X4", "KF_Q19_EIG_TRANSLATION",
-                 "KF_Q23_SDF_XY_OFFSET"]:
+                 "KF_Q23_SDF_XY_OFFSET", "KF_Q24_MC_SHADER_UNITS"]:
         m = re.search(r"#define " + name + r" \(1u << (\d+)\)", text)
         assert m and getattr(L, name) == 1 << int(m.group(1)), name
 

@@ -130,3 +130,84 @@ def test_prefix_sum_device():
     ref, rtot = O.prefix_sum(a)
     np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint32), ref)
     assert tot.value == rtot
+
+
+@pytest.mark.parametrize("storage", [L.KF_STORAGE_F32F32, L.KF_STORAGE_F16U16, L.KF_STORAGE_RG16I])
+@pytest.mark.parametrize("method", [L.KF_MC_HISTOPYRAMID, L.KF_MC_SCAN])
+def test_face_normals_match_oracle(storage, method):
+    """calcNormal (marchingCubes.cs:87-93) per vertex: cross(v1 - v0, v2 - v0) of its
+    triangle, w = 0, for both extraction paths."""
+    cfg = GFusionConfig(volumeSize=(64,) * 3, volumeDimensions=(1.0,) * 3, storage=storage,
+                        quirks=L.KF_QUIRKS_TRACKING & ~(L.KF_Q13_MC_FIRST_SEVEN | L.KF_Q15_MC_BORDER_SKIP))
+    g, o = both(cfg, sphere_raw(64, storage))
+    m, ng = compare(g, o, method)
+    assert ng > 1000
+    Ng, No = m.getNormals(), o.mcNormals()
+    assert (Ng[:, 3] == 0).all()
+    scale = np.linalg.norm(No[:, :3], axis=1).max()
+    assert np.max(np.abs(Ng - No)) <= 1e-4 * scale + 1e-6
+
+
+@pytest.mark.parametrize("storage", [L.KF_STORAGE_F32F32, L.KF_STORAGE_RG16I])
+def test_scan_path_shader_units(storage):
+    """Q24: the scan path writes marchingCubes.cs's output convention: corners at
+    -1 + gridPos * voxelSize, vertex / 128 * voxelSize.x with z negated, w = 1, normals in
+    the unscaled shader units (voxelSize = 1000 * dim / size)."""
+    q = (L.KF_QUIRKS_TRACKING & ~(L.KF_Q13_MC_FIRST_SEVEN | L.KF_Q15_MC_BORDER_SKIP)) | L.KF_Q24_MC_SHADER_UNITS
+    cfg = GFusionConfig(volumeSize=(64,) * 3, volumeDimensions=(1.0,) * 3, storage=storage, quirks=q)
+    g, o = both(cfg, sphere_raw(64, storage))
+    m = MCubes(g)
+    ng = m.generateMarchingCubes(L.KF_MC_SCAN)
+    assert ng == o.mcExtract(0.0, L.KF_MC_SCAN) > 1000
+    Vg, Vo = m.getVertices(), o.mcVertices()
+    assert (Vg[:, 3] == 1).all()
+    assert np.max(np.abs(Vg - Vo)) <= 1e-5 * np.abs(Vo).max()
+    vs = 1000.0 / 64
+    # the same triangles as voxel-index output, mapped by the shader's formula
+    cfg2 = GFusionConfig(volumeSize=(64,) * 3, volumeDimensions=(1.0,) * 3, storage=storage,
+                         quirks=q & ~L.KF_Q24_MC_SHADER_UNITS)
+    g2 = GFusion(cfg2, INTR)
+    g2.setVolumeRaw(sphere_raw(64, storage))
+    m2 = MCubes(g2)
+    assert m2.generateMarchingCubes(L.KF_MC_SCAN) == ng
+    Vi = m2.getVertices()[:, :3].astype(np.float64)
+    expect = (-1.0 + Vi * vs) / 128.0 * vs * np.array([1.0, 1.0, -1.0])
+    assert np.max(np.abs(Vg[:, :3] - expect)) <= 1e-4 * np.abs(expect).max()
+    Ng, No = m.getNormals(), o.mcNormals()
+    assert np.max(np.abs(Ng - No)) <= 1e-4 * np.linalg.norm(No[:, :3], axis=1).max()
+
+
+@pytest.mark.parametrize("storage", [L.KF_STORAGE_F32F32, L.KF_STORAGE_F16U16, L.KF_STORAGE_RG16I])
+def test_welded_mesh_matches_oracle(storage, tmp_path):
+    """The welded mesh: vertex and triangle counts and every index bit-exact with the
+    oracle, positions within 1e-6 m, unit normals within 1e-3; the exports carry it."""
+    cfg = GFusionConfig(volumeSize=(64,) * 3, volumeDimensions=(1.0,) * 3, storage=storage,
+                        quirks=L.KF_QUIRKS_TRACKING & ~(L.KF_Q13_MC_FIRST_SEVEN | L.KF_Q15_MC_BORDER_SKIP))
+    g, o = both(cfg, sphere_raw(64, storage))
+    m = MCubes(g)
+    Pg, Ng, Ig = m.extractMesh()
+    Po, No, Io = o.mcMesh(0.0)
+    assert len(Pg) == len(Po) > 1000 and len(Ig) == len(Io)
+    np.testing.assert_array_equal(Ig, Io)
+    assert np.max(np.abs(Pg - Po)) <= 1e-6
+    assert np.max(np.abs(Ng - No)) <= 1e-3
+    # a closed surface: V - E + F = 2; as many triangles as the scan path's soup
+    E = np.unique(np.sort(np.concatenate([Ig[:, [0, 1]], Ig[:, [1, 2]], Ig[:, [2, 0]]]), axis=1), axis=0)
+    assert len(Pg) - len(E) + len(Ig) == 2
+    assert m.generateMarchingCubes(L.KF_MC_SCAN) == len(Ig)
+    # exports
+    ply, stl = str(tmp_path / "m.ply"), str(tmp_path / "m.stl")
+    m.exportWeldedMeshPly(ply)
+    m.exportWeldedMeshStl(stl)
+    raw = open(ply, "rb").read()
+    head, body = raw.split(b"end_header\n", 1)
+    assert f"element vertex {len(Pg)}".encode() in head and f"element face {len(Ig)}".encode() in head
+    assert len(body) == len(Pg) * 24 + len(Ig) * 13
+    V = np.frombuffer(body[:len(Pg) * 24], np.float32).reshape(-1, 6)
+    np.testing.assert_array_equal(V[:, :3], Pg)
+    s = open(stl, "rb").read()
+    assert int.from_bytes(s[80:84], "little") == len(Ig) and len(s) == 84 + 50 * len(Ig)
+    fn = np.frombuffer(s[84:], np.uint8).reshape(-1, 50)[:, :12].copy().view(np.float32)
+    c = np.array([0.5, 0.5, 0.5])
+    cen = Pg[Ig].mean(axis=1)
+    assert np.mean(np.sum(fn * (cen - c), axis=1) > 0) > 0.999  # outward facets

@@ -516,3 +516,31 @@ def test_stl_and_ply_export(tmp_path):
     lines = ply.read_text().splitlines()
     assert lines[0] == "ply" and lines[2] == f"element vertex {3 * n}"
     assert len(lines) == 7 + 3 * n
+
+
+def test_welded_mesh_of_a_sphere():
+    """The oracle's welded mesh of an analytic sphere TSDF: a closed surface (V - E + F = 2)
+    with the classic path's triangle count, vertices on the sphere, unit normals pointing
+    out, facets wound counter-clockwise from outside."""
+    from oglfusionkinectv2_b200 import GFusionConfig, Intrinsics, _lib as L
+    n = 40
+    g = (np.arange(n) + 0.5) / n
+    Z, Y, X = np.meshgrid(g, g, g, indexing="ij")
+    sd = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2) - 0.3
+    F = np.clip(sd / 0.05, -1, 1).astype(np.float32).ravel()
+    raw = np.concatenate([F, np.ones(n ** 3, np.float32)]).view(np.uint8)
+    cfg = GFusionConfig(volumeSize=(n,) * 3, volumeDimensions=(1.0,) * 3, storage=L.KF_STORAGE_F32F32,
+                        quirks=L.KF_QUIRKS_TRACKING & ~(L.KF_Q13_MC_FIRST_SEVEN | L.KF_Q15_MC_BORDER_SKIP))
+    o = O.Oracle(cfg, Intrinsics())
+    o.setVolumeRaw(raw)
+    P, N, I = o.mcMesh(0.0)
+    E = np.unique(np.sort(np.concatenate([I[:, [0, 1]], I[:, [1, 2]], I[:, [2, 0]]]), axis=1), axis=0)
+    assert len(P) - len(E) + len(I) == 2
+    assert o.mcExtract(0.0, L.KF_MC_SCAN) == len(I)
+    c = np.array([0.5, 0.5, 0.5])
+    r = np.linalg.norm(P - c, axis=1)
+    assert np.abs(r - 0.3).max() < 2e-3
+    np.testing.assert_allclose(np.linalg.norm(N, axis=1), 1.0, rtol=1e-5)
+    assert np.mean(np.sum(N * (P - c), axis=1) > 0) == 1.0
+    fn = np.cross(P[I[:, 1]] - P[I[:, 0]], P[I[:, 2]] - P[I[:, 0]])
+    assert np.mean(np.sum(fn * (P[I].mean(axis=1) - c), axis=1) > 0) == 1.0
