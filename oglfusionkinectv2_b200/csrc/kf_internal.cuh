@@ -55,6 +55,14 @@ struct KfDevState {
   // reduction atomics land elsewhere)
   alignas(128) unsigned barrier_count;      // grid barrier of the ICP launch
   alignas(128) unsigned sdf_barrier_count;  // grid barrier of the SDF launch
+  // the ICP launch's per-level grid barriers (levels 2, 1 may run on fewer blocks than
+  // level 0), the count of finished levels, and the hand-over to the blocks that join a
+  // finer level: pose, accumulation centre and iteration count at its start
+  alignas(128) unsigned icp_lvl_barrier[3][32];
+  alignas(128) unsigned icp_stage;
+  alignas(128) double icp_hand_pose[16];
+  double icp_hand_cd[3];
+  unsigned icp_hand_gi;
   // ICP reduction rows as fixed-point sums (value * 2^32, exact and order-independent),
   // three buffers used in turn by successive iterations of a launch; every sum on its own
   // 128-byte line (KF_ACC_STRIDE words apart), so the blocks' 64-bit atomics on the 32
@@ -186,6 +194,7 @@ struct kf_session {
 
   // launch shapes (kf_set_launch_shape / kf_autotune); every choice computes the same result
   int int_zc = 16;   // integrate: voxels per thread along z (8, 16, 32)
+  int icp_coarse_px = 512;  // ICP levels 2, 1: pixels per block (0: every block)
   int ray_rows = 4;  // raycast: tile rows of 32 pixels (2, 4, 8), or 1: persistent sweep
 
   // depth ingest before the pyramid (off by default): Kinect-v2 undistortion through a
@@ -598,8 +607,9 @@ __host__ __device__ inline void kf_jacobi_eigen6(double* A, double* V) {
 
 // The rank-guarded step of a world-frame system C x = b (C row-major 6x6), as described
 // at KF_ICP_RANK_TAU.  Returns the number of eigen-directions kept.
-__host__ __device__ inline int kf_icp_guarded_solve(const double* C, const double* b, double* x) {
-  double A[36], V[36];
+__host__ __device__ inline int kf_icp_guarded_solve(const double* C, const double* b, double* x, double* A,
+                                                    double* V) {
+  // A, V: 36 doubles of scratch each
   for (int i = 0; i < 36; ++i) A[i] = C[i];
   kf_jacobi_eigen6(A, V);
   double lmax = 0.0;
@@ -618,12 +628,18 @@ __host__ __device__ inline int kf_icp_guarded_solve(const double* C, const doubl
 }
 
 // The rank-guarded step from the centred sums about c, in the world frame: b = M^T b',
-// C = M^T C' M with M = [[I, -[c]x], [0, I]], then kf_icp_guarded_solve.  Kept out of line:
-// it runs only for degenerate views, and its arrays would crowd the caller's registers.
-static __device__ __noinline__ void kf_icp_world_guarded_step(const double* v21c, const double* bc, const double* c,
-                                                       double* out) {
+// C = M^T C' M with M = [[I, -[c]x], [0, I]], then kf_icp_guarded_solve.  It runs only for
+// degenerate views; its matrices live in the caller's scratch sm (6 * 36 + 12 doubles,
+// shared memory), so they take no registers from the caller.
+__device__ inline void kf_icp_world_guarded_step(const double* v21c, const double* bc, const double* c, double* out,
+                                                 double* sm) {
   const double cx = c[0], cy = c[1], cz = c[2];
-  double Cp[36], Mx[36], T[36], Cw[36], bw[6], xw[6];
+  double* Cp = sm;
+  double* Mx = sm + 36;
+  double* T = sm + 72;
+  double* Cw = sm + 108;
+  double* bw = sm + 216;
+  double* xw = sm + 222;
   kf_make_jtj(v21c, Cp);
   for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
   // -[c]x in rows 0..2, columns 3..5
@@ -647,7 +663,7 @@ static __device__ __noinline__ void kf_icp_world_guarded_step(const double* v21c
       for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * T[k * 6 + cc];
       Cw[r * 6 + cc] = v;
     }
-  kf_icp_guarded_solve(Cw, bw, xw);
+  kf_icp_guarded_solve(Cw, bw, xw, sm + 144, sm + 180);
   for (int k = 0; k < 6; ++k) out[k] = xw[k];
 }
 
@@ -659,7 +675,8 @@ static __device__ __noinline__ void kf_icp_world_guarded_step(const double* v21c
 // l_min >= 1 / trace(C^-1) and l_max <= trace(C), with trace(C) = sum_i m_i^T C' m_i
 // (m_i = M e_i) and (C^-1)_ii = |L'^-1 M^-T e_i|^2 for C' = L' L'^T.  Otherwise (rare: a
 // degenerate view) lane 0 forms the world-frame system and runs kf_icp_guarded_solve.
-// *guarded is set when that path ran.
+// s_scratch: 8 + 228 doubles of shared memory (the step in the first 6).  *guarded is set
+// when that path ran.
 __device__ inline void kf_icp_solve_warp(const double* v21c, const double* bc, const double* c, double* x,
                                          int lane, double* s_scratch, int* guarded) {
   double xp[6], Lrow[6], inv_diag = 0.0;
@@ -723,7 +740,7 @@ __device__ inline void kf_icp_solve_warp(const double* v21c, const double* bc, c
     *guarded = 0;
     return;
   }
-  if (lane == 0) kf_icp_world_guarded_step(v21c, bc, c, s_scratch);
+  if (lane == 0) kf_icp_world_guarded_step(v21c, bc, c, s_scratch, s_scratch + 8);
   __syncwarp();
 #pragma unroll
   for (int k = 0; k < 6; ++k) x[k] = s_scratch[k];
