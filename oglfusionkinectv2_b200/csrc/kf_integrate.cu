@@ -34,6 +34,8 @@ struct IntArgs {
   // eta is surely <= -mu when d - z < behind_cut, and surely >= mu when d - z > free_cut:
   // the ray-length factor sqrt(1 + (x/z)^2 + (y/z)^2) is >= 1 (rounding margin 2^-16)
   float behind_cut, free_cut;
+  const uint8_t* tiles;  // per 8x8 depth tile: some pixel has depth (null: not used)
+  int tw, th;
   int band;  // Q8
   const int* gate;
   const KfDevState* st;
@@ -79,10 +81,47 @@ __device__ __forceinline__ bool box_outside_frustum(const IntArgs& a, const floa
          (o3 & 0xffu) == 0xffu || (o4 & 0xffu) == 0xffu;
 }
 
+// True when no voxel of the warp's 32 x 1 x 8 brick (x in [xb, xb + 32), row y, z in
+// [z0, z0 + 8)) can change: the brick (with a voxel of margin) lies outside one frustum
+// half-space, or every depth pixel it can project to is 0 (integrate.cs:70-75 skips those
+// voxels).  The brick lies in front of the camera, so its projection is inside the box of
+// its corners' projections; the pixel range gets a pixel of margin.  Called by the whole
+// warp; lane & 7 projects one corner.
+__device__ __forceinline__ bool warp_brick_idle(const IntArgs& a, const float* inv, int xb, int y, int z0) {
+  const int b0[3] = {xb - 1, y - 1, z0 - 1};
+  const int b1[3] = {xb + 32, y + 1, z0 + 8};
+  if (box_outside_frustum(a, inv, b0, b1)) return true;
+  if (!a.tiles) return false;
+  const float vx = a.dimx / a.nx, vy = a.dimy / a.ny, vz = a.dimz / a.nz;
+  const int c = threadIdx.x & 7;
+  const float wx = ((c & 1 ? b1[0] : b0[0]) + 0.5f) * vx;
+  const float wy = ((c & 2 ? b1[1] : b0[1]) + 0.5f) * vy;
+  const float wz = ((c & 4 ? b1[2] : b0[2]) + 0.5f) * vz;
+  const float X = inv[0] * wx + inv[1] * wy + inv[2] * wz + inv[3];
+  const float Y = inv[4] * wx + inv[5] * wy + inv[6] * wz + inv[7];
+  const float Z = inv[8] * wx + inv[9] * wy + inv[10] * wz + inv[11];
+  if (__any_sync(0xffffffffu, !(Z > 1e-3f))) return false;  // near or behind the camera plane
+  const float u = a.fx * X / Z + a.cx + 0.5f, v = a.fy * Y / Z + a.cy + 0.5f;
+  const int iu = (int)fminf(fmaxf(floorf(u), -2.0f), 65536.0f);
+  const int iv = (int)fminf(fmaxf(floorf(v), -2.0f), 65536.0f);
+  const int u0 = max(__reduce_min_sync(0xffffffffu, iu) - 1, 0), u1 = min(__reduce_max_sync(0xffffffffu, iu) + 1, a.W - 1);
+  const int v0 = max(__reduce_min_sync(0xffffffffu, iv) - 1, 0), v1 = min(__reduce_max_sync(0xffffffffu, iv) + 1, a.H - 1);
+  if (u0 > u1 || v0 > v1) return true;  // entirely off the image (the frustum test's margin)
+  const int tx0 = u0 >> 3, tx1 = u1 >> 3, ty0 = v0 >> 3, ty1 = v1 >> 3;
+  const int ntx = tx1 - tx0 + 1, nt = ntx * (ty1 - ty0 + 1);
+  if (nt > 64) return false;  // a large footprint (close to the camera): not tested
+  const int lane = threadIdx.x & 31;
+  bool any = false;
+  for (int k = lane; k < nt; k += 32) any |= __ldg(a.tiles + (ty0 + k / ntx) * a.tw + tx0 + k % ntx) != 0;
+  return !__any_sync(0xffffffffu, any);
+}
+
 // The z-chunk [zb, zb + ZC) of column (x, y); returns which z-bricks received a negative
 // value (bit j = brick zb/8 - 1 + j, bit 0 for the dilation of a z % 8 == 0 voxel).
 template <int S, int ZC>
-__device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const float* inv, int x, int y, int zb) {
+__device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const float* inv, int x, int y, int zb,
+                                                     bool xin) {
+  // called by the whole warp (x = xb + lane, xin: x < nx)
   typedef typename Vox<S>::V V;
   typedef typename Vox<S>::Wt Wt;
   // bits 0..ZC/8: NEG of z-bricks zb/8 - 1 + j; bit 6: NEG of z-super-brick zb/64, bit 7:
@@ -179,7 +218,16 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   // voxel and steps by delta inside it, as integrate.cs:57-62 does, so it does not depend on
   // where a chunk starts.  Whole bricks run unrolled; only a ragged last brick (nz not a
   // multiple of 8) takes the counted loop.
+  const int xb = x - (int)(threadIdx.x & 31);
   for (int k8 = 0; k8 < zend; k8 += 8) {
+    if (warp_brick_idle(a, inv, xb, y, zb + k8)) {
+      idx += 8 * slice;
+      continue;
+    }
+    if (!xin) {
+      idx += 8 * slice;
+      continue;
+    }
     const float czw = (zb + k8 + 0.5f) * vz;
     px = fmaf(inv[2], czw, pxy[0]);
     py = fmaf(inv[6], czw, pxy[1]);
@@ -203,7 +251,7 @@ struct IntBatch {
 };
 
 template <int S, bool BATCH, int ZC>
-__global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBatch batch) {
+__global__ void __launch_bounds__(256, 5) integrate_kernel(IntArgs a_one, IntBatch batch) {
   __shared__ IntArgs s_args;
   int bxi, byi, bzi;  // this block's position in its volume's block grid
   if constexpr (BATCH) {
@@ -245,7 +293,7 @@ __global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBat
   const int x = xb + lane;
   const int y = yb + threadIdx.y;  // uniform over the warp
   uint32_t flags = 0;  // integrate_column's bits
-  if (x < a.nx && y < a.ny) flags = integrate_column<S, ZC>(a, inv, x, y, zb);
+  if (y < a.ny) flags = integrate_column<S, ZC>(a, inv, x, y, zb, x < a.nx);  // y: uniform over the warp
   if (!__any_sync(0xffffffffu, flags != 0)) return;
   // Brick flags, merged over the warp: lanes 8c-8..8c-1 write brick column c of the block
   // (c = 1..4) and a lane on a brick's low x face also brick column c-1 (dilation); lane c
@@ -321,6 +369,9 @@ IntArgs make_int_args(kf_session* s, int gated) {
   a.bx = s->bx; a.by = s->by; a.bz = s->bz;
   a.supers = s->d_supers;
   a.sbx = s->sbx; a.sby = s->sby; a.sbz = s->sbz;
+  a.tiles = s->d_depth_tiles;
+  a.tw = s->tiles_w;
+  a.th = s->tiles_h;
   return a;
 }
 

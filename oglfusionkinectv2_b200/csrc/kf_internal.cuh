@@ -122,6 +122,10 @@ struct kf_session {
   uint16_t* d_depth_u16 = nullptr;  // upload staging (device)
   float* d_depth_f32_in = nullptr;  // float upload staging (device)
   float* d_depth[3] = {nullptr, nullptr, nullptr};
+  // per 8x8 tile of the level-0 depth: 1 when some pixel of the tile has depth (written with
+  // the pyramid; integrate skips voxel bricks that can only project into empty tiles)
+  uint8_t* d_depth_tiles = nullptr;
+  int tiles_w = 0, tiles_h = 0;
   float4* d_vertex[3] = {nullptr, nullptr, nullptr};
   float4* d_normal[3] = {nullptr, nullptr, nullptr};
   int32_t* d_status[3] = {nullptr, nullptr, nullptr};
