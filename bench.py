@@ -829,7 +829,10 @@ def main():
     g.close()
 
     if rank == 0 and world == 1 and not args.no_reference_quirks:
-        out["reference_quirks"] = reference_quirks_pass(w, base, fbytes, W, K)
+        try:
+            out["reference_quirks"] = reference_quirks_pass(w, base, fbytes, W, K)
+        except Exception as e:  # noqa: BLE001
+            out["reference_quirks"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1:
         # accuracy: ground truth over the timed frames (a deterministic re-run of the same
         # frames) and over the end-to-end frames (that pass's own results); the FP64 oracle
@@ -856,10 +859,14 @@ def main():
                 "tsdf_after_prefix": tsdf_error(vol_prefix, o_vol, w.config)}
         out["accuracy"] = acc
     if rank == 0 and world == 1 and not args.no_forms:
-        log("batched form")
-        out["batched"] = run_batched(args, sub=True)
-        log("served form")
-        out["served"] = run_served(args, sub=True)
+        # the batched and served forms beside the plain line; a failure there is recorded,
+        # it does not lose the plain line
+        for key, fn in (("batched", run_batched), ("served", run_served)):
+            log(f"{key} form")
+            try:
+                out[key] = fn(args, sub=True)
+            except Exception as e:  # noqa: BLE001
+                out[key] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
