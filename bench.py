@@ -838,25 +838,34 @@ def main():
         # frames) and over the end-to-end frames (that pass's own results); the FP64 oracle
         # over the cpu_baseline prefix, poses and TSDF
         prefix = CPU_WARM_FRAMES + max(1, args.cpu_frames)
-        log("accuracy pass")
-        acc_poses, vol_prefix, same = accuracy_pass(w, base, fbytes, W + K, prefix, pose_timed_last)
-        acc = {"ate_vs_ground_truth_mm": {
-                   "timed_frames": 1000 * rmse_translation(acc_poses[W:W + K], w.poses[W:W + K]),
-                   "all_frames_to_timed_end": 1000 * rmse_translation(acc_poses, w.poses[:W + K]),
-                   "rerun_matches_timed_session": same}}
-        if e2e_poses:
-            e2e_gt = w.poses[W + K + 1:W + K + 1 + len(e2e_poses)]
-            acc["ate_vs_ground_truth_mm"]["e2e_frames"] = 1000 * rmse_translation(e2e_poses, e2e_gt)
+        acc = {}
+        acc_poses = vol_prefix = None
+        try:
+            log("accuracy pass")
+            acc_poses, vol_prefix, same = accuracy_pass(w, base, fbytes, W + K, prefix, pose_timed_last)
+            acc["ate_vs_ground_truth_mm"] = {
+                "timed_frames": 1000 * rmse_translation(acc_poses[W:W + K], w.poses[W:W + K]),
+                "all_frames_to_timed_end": 1000 * rmse_translation(acc_poses, w.poses[:W + K]),
+                "rerun_matches_timed_session": same}
+            if e2e_poses:
+                e2e_gt = w.poses[W + K + 1:W + K + 1 + len(e2e_poses)]
+                acc["ate_vs_ground_truth_mm"]["e2e_frames"] = 1000 * rmse_translation(e2e_poses, e2e_gt)
+        except Exception as e:  # noqa: BLE001
+            acc["error"] = f"{type(e).__name__}: {e}"
         if not args.no_cpu_baseline:
             log("cpu baseline")
             out["cpu_baseline"], o_poses, o_vol = cpu_baseline(args, w, frames)
-            n = len(o_poses)
-            acc["vs_fp64_oracle"] = {
-                "frames": f"0-{n - 1} (the cpu_baseline frames, same start pose)",
-                "ate_mm": 1000 * rmse_translation(acc_poses[:n], o_poses),
-                "max_translation_diff_mm": 1000 * max(float(np.linalg.norm(a[:3, 3] - b[:3, 3]))
-                                                      for a, b in zip(acc_poses[:n], o_poses)),
-                "tsdf_after_prefix": tsdf_error(vol_prefix, o_vol, w.config)}
+            if acc_poses is not None:
+                try:
+                    n = len(o_poses)
+                    acc["vs_fp64_oracle"] = {
+                        "frames": f"0-{n - 1} (the cpu_baseline frames, same start pose)",
+                        "ate_mm": 1000 * rmse_translation(acc_poses[:n], o_poses),
+                        "max_translation_diff_mm": 1000 * max(float(np.linalg.norm(a[:3, 3] - b[:3, 3]))
+                                                              for a, b in zip(acc_poses[:n], o_poses)),
+                        "tsdf_after_prefix": tsdf_error(vol_prefix, o_vol, w.config)}
+                except Exception as e:  # noqa: BLE001
+                    acc["vs_fp64_oracle"] = {"error": f"{type(e).__name__}: {e}"}
         out["accuracy"] = acc
     if rank == 0 and world == 1 and not args.no_forms:
         # the batched and served forms beside the plain line; a failure there is recorded,
