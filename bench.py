@@ -756,7 +756,7 @@ def main():
                 raise L.KfError(st, "kf_frame_step_u16_async")
             if i:
                 lib.kf_get_last_result(g.handle, pose, C.byref(t))
-                e2e_poses.append(np.array(pose[:]))
+                e2e_poses.append(np.array(pose[:]).reshape(4, 4, order="F"))
             maybe_mc(i)
         st = lib.kf_frame_sync(g.handle, C.byref(t))
         if st:
@@ -765,7 +765,7 @@ def main():
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         lib.kf_get_last_result(g.handle, pose, C.byref(t))
-        e2e_poses.append(np.array(pose[:]))
+        e2e_poses.append(np.array(pose[:]).reshape(4, 4, order="F"))
         e2e_ms = e0.elapsed_time(e1)
         log(f"e2e pass {e2e_ms:.1f} ms")
         e2e = {"ms": e2e_ms, "wall_s": wall}
@@ -796,6 +796,7 @@ def main():
         peak, peak_kind = measured_peak_hbm()
         algo = algorithmic_bytes(w.config, dom)
         achieved = algo / (per[dom] / 1000.0) / 1e9 if per[dom] > 0 else None
+        traffic = measured_traffic(w.name, dom)
         out = {
             "metric": PLAIN_METRIC,
             "value": value, "unit": "frames/s", "n_gpus": world, "steps": K, "warmup": W,
@@ -809,7 +810,11 @@ def main():
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak if achieved else None),
                          "peak_source": peak_kind, "algorithmic_bytes": algo,
-                         "traffic": measured_traffic(w.name, dom)},
+                         "traffic": traffic,
+                         # the DRAM bytes the kernel really moves (ncu capture) over its time
+                         "traffic_gbs": (traffic / (per[dom] / 1000.0) / 1e9 if traffic and per[dom] > 0 else None),
+                         "traffic_frac": (traffic / (per[dom] / 1000.0) / 1e9 / peak if traffic and per[dom] > 0 else None),
+                         "traffic_source": "profiles/*_traffic.txt (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "tracked_last": bool(tracked_ok),

@@ -169,30 +169,31 @@ int enqueue_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* dept
     inputs = b->d_inputs;
   }
   // the device part of the step: stages with their events, then every member's frame
-  // result gathered and copied to the slot's pinned heads
+  // result gathered and copied to the slot's pinned heads (external event records, so that
+  // a captured step's events are recorded, and readable from the host, on every replay)
   auto body = [&]() -> int {
     int r;
     if (inputs) KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_inputs, b->h_inputs + (size_t)slot * b->cap,
                                                n * sizeof(uint16_t*), cudaMemcpyHostToDevice, b->stream));
-    KF_CUDA_TRY(b, cudaEventRecord(ev[0], b->stream));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[0], b->stream, cudaEventRecordExternal));
     batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
     KF_CUDA_TRY(b, cudaGetLastError());
     if ((r = kf_batch_launch_pyramid(b, n, inputs))) return r;
-    KF_CUDA_TRY(b, cudaEventRecord(ev[1], b->stream));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[1], b->stream, cudaEventRecordExternal));
     if ((r = kf_batch_launch_icp(b))) return r;
-    KF_CUDA_TRY(b, cudaEventRecord(ev[2], b->stream));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[2], b->stream, cudaEventRecordExternal));
     if ((r = kf_batch_launch_integrate(b))) return r;
-    KF_CUDA_TRY(b, cudaEventRecord(ev[3], b->stream));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[3], b->stream, cudaEventRecordExternal));
     if ((r = kf_batch_launch_sdf_recover(b))) return r;
-    KF_CUDA_TRY(b, cudaEventRecord(ev[4], b->stream));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[4], b->stream, cudaEventRecordExternal));
     if ((r = kf_batch_launch_raycast(b, n))) return r;
-    KF_CUDA_TRY(b, cudaEventRecord(ev[5], b->stream));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[5], b->stream, cudaEventRecordExternal));
     batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
     KF_CUDA_TRY(b, cudaGetLastError());
     b->launches += 2;
     KF_CUDA_TRY(b, cudaMemcpyAsync(b->h_heads + (size_t)slot * b->cap * KF_STATE_RESULT_BYTES, b->d_heads,
                                    (size_t)n * KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost, b->stream));
-    KF_CUDA_TRY(b, cudaEventRecord(ev[6], b->stream));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[6], b->stream, cudaEventRecordExternal));
     return KF_OK;
   };
   if (inputs) {

@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
   __shared__ long long s_fix[JTJ ? kWarps : 1][72];
   __shared__ double s_sums[32];
   __shared__ double s_csums[29], s_ccenter[3], s_ae;  // last centred row (for the tail)
+  __shared__ double s_nvalid;                           // its valid-pixel count
   __shared__ double s_gx[8 + 228];                      // the rank-guarded step (rare path)
   __shared__ int s_flag, s_conv;
   __shared__ __align__(16) __nv_bfloat16 s_hi[JTJ ? kWarps : 1][8][40];
@@ -516,6 +517,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
           s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
         }
         if (lane == 30) s_ae = sqrt(s_sums[0] / count);  // getReduction :1167
+        if (lane == 31) s_nvalid = nvalid;
         // next centre: this iteration's centroid of the valid points
         const double cn = lane < 3 ? (nvalid > 0 ? s_sums[29 + lane] / nvalid : s_cd[lane]) : 0.0;
         __syncwarp();
@@ -583,8 +585,12 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
     st->sums[28] = cs[28];
     st->sums[29] = st->sums[30] = st->sums[31] = 0.0;
   }
+  // AE == 0 fails the frame (gFusion.cpp:715-723): in the reference that means no valid
+  // pixel.  Here the energy is a fixed-point sum, which rounds residuals of a few microns to
+  // exactly 0 (per 32-pixel chunk with split-BF16); with valid pixels the frame is tracked.
+  const bool no_energy = ae == 0.0 && !(iters_run && s_nvalid > 0.0);
   int tracked;
-  if (ae > 0.5 || ae == 0.0) {
+  if (ae > 0.5 || no_energy) {
     tracked = 0;
     kf_store_pose(st, s_old);
   } else {

@@ -125,7 +125,8 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   typedef typename Vox<S>::V V;
   typedef typename Vox<S>::Wt Wt;
   // bits 0..ZC/8: NEG of z-bricks zb/8 - 1 + j; bit 6: NEG of z-super-brick zb/64, bit 7:
-  // of zb/64 - 1 (a z % 64 == 0 voxel is that one's +1 layer)
+  // of zb/64 - 1 (a z % 64 == 0 voxel is that one's +1 layer); the same 8 bits shifted by 8
+  // for LOW
   static_assert(ZC == 8 || ZC == 16 || ZC == 32, "z chunk: 8, 16 or 32 voxels");
   uint32_t flags = 0;
 
@@ -150,6 +151,14 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   const float ku = a.cx + 0.5f, kv = a.cy + 0.5f;
   const int zend = min(ZC, a.nz - zb);
   float px, py, pz;
+  // the brick bits of a voxel (jj: index in its brick, jb: the brick's bit) for NEG
+  // (shift 0) or LOW (shift 8)
+  auto mark = [&](int jj, int jb, int k8, int shift) {
+    uint32_t b = 1u << jb;
+    if (jj == 0) b |= (1u << (jb - 1)) | (((zb + k8) & 63) == 0 ? 0xc0u : 0x40u);
+    else b |= 0x40u;
+    flags |= b << shift;
+  };
   // one voxel of the march (integrate.cs:63-113); jj: its index in the current brick
   auto voxel = [&](int jj, int jb, int k8) {
     if (pz < 0.0001f) return;
@@ -204,14 +213,13 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
       if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
       // a non-negative nF never stores a negative value; a brick's first voxel is also
       // the +1 layer of the brick below it (and, at z % 64 == 0, of the super-brick below)
-      if (nF < 0.0f) {
-        flags |= 1u << jb;
-        if (jj == 0) flags |= (1u << (jb - 1)) | (((zb + k8) & 63) == 0 ? 0xc0u : 0x40u);
-        else flags |= 0x40u;
-      }
+      if (nF < 0.0f) mark(jj, jb, k8, 0);
+      // LOW from the value as the raycast reads it back
+      if (__fmul_rn(Vox<S>::raw_nc(&ev, 0), Vox<S>::kRawToF) < KF_BRICK_LOW_LEVEL) mark(jj, jb, k8, 8);
     } else {
       vf[idx] = Vox<S>::encode_value(0.0f);
       vw[idx] = Vox<S>::encode_weight(0.0f);
+      mark(jj, jb, k8, 8);  // zero is below the coarse-step threshold
     }
   };
   // One 8-voxel brick of the column at a time: the position is anchored at the brick's first
@@ -301,7 +309,9 @@ __global__ void __launch_bounds__(256, 5) integrate_kernel(IntArgs a_one, IntBat
   // bits already, so read first and skip those atomics.
   const int lx = (x >> 3) - (xb >> 3) + 1;
   constexpr int kZBits = ZC / 8 + 1;  // z-bricks a chunk touches, with the dilation one
-  const uint32_t zbits = flags & ((1u << kZBits) - 1u);
+  constexpr uint32_t kZMask = (1u << kZBits) - 1u;
+  // NEG bits in 0..kZBits-1, LOW bits in 16..16+kZBits-1
+  const uint32_t zbits = (flags & kZMask) | (((flags >> 8) & kZMask) << 16);
   uint32_t mine = 0;
 #pragma unroll
   for (int c = 0; c < 5; ++c) {
@@ -312,30 +322,32 @@ __global__ void __launch_bounds__(256, 5) integrate_kernel(IntArgs a_one, IntBat
   if (lane < 5 && mine) {
     const int gx = (xb >> 3) - 1 + lane;
     for (int j = 0; j < kZBits; ++j) {
-      if (!((mine >> j) & 1u)) continue;
+      const uint32_t want = (((mine >> j) & 1u) ? KF_BRICK_NEG : 0u) | (((mine >> (16 + j)) & 1u) ? KF_BRICK_LOW : 0u);
+      if (!want) continue;
       const int gz = (zb >> 3) - 1 + j;
       for (int dy = 0; dy < ((y & 7) == 0 ? 2 : 1); ++dy) {
         const int gy = (y >> 3) - dy;
         if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.bx && gy < a.by && gz < a.bz) {
           uint32_t* w = &a.bricks[(uint32_t)gx + (uint32_t)a.bx * ((uint32_t)gy + (uint32_t)a.by * (uint32_t)gz)];
-          if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
+          if ((*(volatile uint32_t*)w & want) != want) atomicOr(w, want);
         }
       }
     }
   }
   // super-bricks: own and, on a super-brick's low face, the one below (x, y, z)
-  const uint32_t sbits = flags & 0xc0u;
+  const uint32_t sbits = flags & 0xc0c0u;
   const uint32_t s_own = __reduce_or_sync(0xffffffffu, sbits);
   const uint32_t s_lowx = __reduce_or_sync(0xffffffffu, (x & 63) == 0 ? sbits : 0u);
   if (lane < 8 && (lane & 1 ? s_own : s_lowx)) {
     const int jx = lane & 1, jy = (lane >> 1) & 1, jz = lane >> 2;
     const uint32_t zsel = jz ? 0x40u : 0x80u;
     const uint32_t src = jx ? s_own : s_lowx;
-    if ((src & zsel) && (jy == 1 || (y & 63) == 0)) {
+    const uint32_t want = ((src & zsel) ? KF_BRICK_NEG : 0u) | ((src & (zsel << 8)) ? KF_BRICK_LOW : 0u);
+    if (want && (jy == 1 || (y & 63) == 0)) {
       const int gx = (xb >> 6) - 1 + jx, gy = (y >> 6) - 1 + jy, gz = (zb >> 6) - 1 + jz;
       if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.sbx && gy < a.sby && gz < a.sbz) {
         uint32_t* w = &a.supers[(uint32_t)gx + (uint32_t)a.sbx * ((uint32_t)gy + (uint32_t)a.sby * (uint32_t)gz)];
-        if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
+        if ((*(volatile uint32_t*)w & want) != want) atomicOr(w, want);
       }
     }
   }

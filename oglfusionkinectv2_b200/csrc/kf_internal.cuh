@@ -211,11 +211,14 @@ struct kf_session {
 
 // ---------------------------------------------------------------------------------------
 // error helpers
+// A failing call's error is also taken off the runtime's per-thread error state, so that
+// a later cudaGetLastError() (after a launch) does not report it again.
 #define KF_CUDA_TRY(s, expr)                                                          \
   do {                                                                                \
     cudaError_t e_ = (expr);                                                          \
     if (e_ != cudaSuccess) {                                                          \
       (s)->last_error = std::string(#expr) + ": " + cudaGetErrorString(e_);          \
+      cudaGetLastError();                                                             \
       return KF_ERR_CUDA;                                                             \
     }                                                                                 \
   } while (0)
@@ -959,6 +962,12 @@ int kf_note_integrate(kf_session* s, cudaStream_t stream);
 // (every KF_BRICK_REBUILD_EVERY integrates, and after a volume upload) clears stale bits,
 // so a clear bit is a guarantee.
 #define KF_BRICK_NEG 1u
+// LOW: some value there may be below KF_BRICK_LOW_LEVEL (raycast's coarse-step threshold 0.8,
+// raycast.cs:199, plus a margin for the trilinear interpolation's rounding).  A region with
+// the bit clear holds no sample below 0.8, so the coarse phase of the march skips it.  Reset
+// sets it everywhere (an all-zero volume is below the threshold everywhere).
+#define KF_BRICK_LOW 2u
+#define KF_BRICK_LOW_LEVEL 0.801f
 #define KF_BRICK_REBUILD_EVERY 16
 int kf_mc_run(kf_session* s, float iso, int method, uint32_t* n_tri);
 int kf_scan_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* d_total,
