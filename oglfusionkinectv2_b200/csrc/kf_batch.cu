@@ -171,29 +171,32 @@ int enqueue_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* dept
   // the device part of the step: stages with their events, then every member's frame
   // result gathered and copied to the slot's pinned heads (external event records, so that
   // a captured step's events are recorded, and readable from the host, on every replay)
+  // events recorded while capturing must be external records to be seen from the host;
+  // outside capture the flag is not allowed
+  unsigned rec_flags = cudaEventRecordDefault;
   auto body = [&]() -> int {
     int r;
     if (inputs) KF_CUDA_TRY(b, cudaMemcpyAsync(b->d_inputs, b->h_inputs + (size_t)slot * b->cap,
                                                n * sizeof(uint16_t*), cudaMemcpyHostToDevice, b->stream));
-    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[0], b->stream, cudaEventRecordExternal));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[0], b->stream, rec_flags));
     batch_clear_kernel<<<n, 128, 0, b->stream>>>(b->states);
     KF_CUDA_TRY(b, cudaGetLastError());
     if ((r = kf_batch_launch_pyramid(b, n, inputs))) return r;
-    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[1], b->stream, cudaEventRecordExternal));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[1], b->stream, rec_flags));
     if ((r = kf_batch_launch_icp(b))) return r;
-    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[2], b->stream, cudaEventRecordExternal));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[2], b->stream, rec_flags));
     if ((r = kf_batch_launch_integrate(b))) return r;
-    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[3], b->stream, cudaEventRecordExternal));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[3], b->stream, rec_flags));
     if ((r = kf_batch_launch_sdf_recover(b))) return r;
-    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[4], b->stream, cudaEventRecordExternal));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[4], b->stream, rec_flags));
     if ((r = kf_batch_launch_raycast(b, n))) return r;
-    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[5], b->stream, cudaEventRecordExternal));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[5], b->stream, rec_flags));
     batch_gather_kernel<<<n, 64, 0, b->stream>>>(b->states, b->d_heads);
     KF_CUDA_TRY(b, cudaGetLastError());
     b->launches += 2;
     KF_CUDA_TRY(b, cudaMemcpyAsync(b->h_heads + (size_t)slot * b->cap * KF_STATE_RESULT_BYTES, b->d_heads,
                                    (size_t)n * KF_STATE_RESULT_BYTES, cudaMemcpyDeviceToHost, b->stream));
-    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[6], b->stream, cudaEventRecordExternal));
+    KF_CUDA_TRY(b, cudaEventRecordWithFlags(ev[6], b->stream, rec_flags));
     return KF_OK;
   };
   if (inputs) {
@@ -204,7 +207,9 @@ int enqueue_step(kf_batch* b, kf_session* const* ss, const uint16_t* const* dept
       b->step_exec[slot] = nullptr;
       const uint64_t l0 = b->launches;
       KF_CUDA_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      rec_flags = cudaEventRecordExternal;
       rc = body();
+      rec_flags = cudaEventRecordDefault;
       cudaGraph_t g = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
       if (rc || ce != cudaSuccess) {

@@ -116,8 +116,6 @@ void free_all(kf_session* s) {
     cudaFree(s->d_normal[l]);
     cudaFree(s->d_status[l]);
   }
-  cudaFree(s->d_depth_tiles);
-  s->d_depth_tiles = nullptr;
   cudaFree(s->d_ref_vertex);
   cudaFree(s->d_ref_normal);
   cudaFree(s->d_sdf_rows);
@@ -561,10 +559,6 @@ int kf_create(const kf_config* cfg, const kf_intrinsics* intr, kf_session** out)
     cudaMemsetAsync(s->d_normal[l], 0, n * 16, s->stream);
     cudaMemsetAsync(s->d_status[l], 0, n * 4, s->stream);
   }
-  s->tiles_w = (s->W[0] + 7) / 8;
-  s->tiles_h = (s->H[0] + 7) / 8;
-  if ((rc = dalloc(s, &s->d_depth_tiles, (size_t)s->tiles_w * s->tiles_h))) return bail(rc);
-  cudaMemsetAsync(s->d_depth_tiles, 1, (size_t)s->tiles_w * s->tiles_h, s->stream);  // no skipping until a frame
   if ((rc = dalloc(s, &s->d_ref_vertex, px))) return bail(rc);
   if ((rc = dalloc(s, &s->d_ref_normal, px))) return bail(rc);
   if ((rc = dalloc(s, &s->d_sdf_rows, px * 8))) return bail(rc);

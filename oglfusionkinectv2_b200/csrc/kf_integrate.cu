@@ -34,8 +34,6 @@ struct IntArgs {
   // eta is surely <= -mu when d - z < behind_cut, and surely >= mu when d - z > free_cut:
   // the ray-length factor sqrt(1 + (x/z)^2 + (y/z)^2) is >= 1 (rounding margin 2^-16)
   float behind_cut, free_cut;
-  const uint8_t* tiles;  // per 8x8 depth tile: some pixel has depth (null: not used)
-  int tw, th;
   int band;  // Q8
   const int* gate;
   const KfDevState* st;
@@ -81,52 +79,14 @@ __device__ __forceinline__ bool box_outside_frustum(const IntArgs& a, const floa
          (o3 & 0xffu) == 0xffu || (o4 & 0xffu) == 0xffu;
 }
 
-// True when no voxel of the warp's 32 x 1 x 8 brick (x in [xb, xb + 32), row y, z in
-// [z0, z0 + 8)) can change: the brick (with a voxel of margin) lies outside one frustum
-// half-space, or every depth pixel it can project to is 0 (integrate.cs:70-75 skips those
-// voxels).  The brick lies in front of the camera, so its projection is inside the box of
-// its corners' projections; the pixel range gets a pixel of margin.  Called by the whole
-// warp; lane & 7 projects one corner.
-__device__ __forceinline__ bool warp_brick_idle(const IntArgs& a, const float* inv, int xb, int y, int z0) {
-  const int b0[3] = {xb - 1, y - 1, z0 - 1};
-  const int b1[3] = {xb + 32, y + 1, z0 + 8};
-  if (box_outside_frustum(a, inv, b0, b1)) return true;
-  if (!a.tiles) return false;
-  const float vx = a.dimx / a.nx, vy = a.dimy / a.ny, vz = a.dimz / a.nz;
-  const int c = threadIdx.x & 7;
-  const float wx = ((c & 1 ? b1[0] : b0[0]) + 0.5f) * vx;
-  const float wy = ((c & 2 ? b1[1] : b0[1]) + 0.5f) * vy;
-  const float wz = ((c & 4 ? b1[2] : b0[2]) + 0.5f) * vz;
-  const float X = inv[0] * wx + inv[1] * wy + inv[2] * wz + inv[3];
-  const float Y = inv[4] * wx + inv[5] * wy + inv[6] * wz + inv[7];
-  const float Z = inv[8] * wx + inv[9] * wy + inv[10] * wz + inv[11];
-  if (__any_sync(0xffffffffu, !(Z > 1e-3f))) return false;  // near or behind the camera plane
-  const float u = a.fx * X / Z + a.cx + 0.5f, v = a.fy * Y / Z + a.cy + 0.5f;
-  const int iu = (int)fminf(fmaxf(floorf(u), -2.0f), 65536.0f);
-  const int iv = (int)fminf(fmaxf(floorf(v), -2.0f), 65536.0f);
-  const int u0 = max(__reduce_min_sync(0xffffffffu, iu) - 1, 0), u1 = min(__reduce_max_sync(0xffffffffu, iu) + 1, a.W - 1);
-  const int v0 = max(__reduce_min_sync(0xffffffffu, iv) - 1, 0), v1 = min(__reduce_max_sync(0xffffffffu, iv) + 1, a.H - 1);
-  if (u0 > u1 || v0 > v1) return true;  // entirely off the image (the frustum test's margin)
-  const int tx0 = u0 >> 3, tx1 = u1 >> 3, ty0 = v0 >> 3, ty1 = v1 >> 3;
-  const int ntx = tx1 - tx0 + 1, nt = ntx * (ty1 - ty0 + 1);
-  if (nt > 64) return false;  // a large footprint (close to the camera): not tested
-  const int lane = threadIdx.x & 31;
-  bool any = false;
-  for (int k = lane; k < nt; k += 32) any |= __ldg(a.tiles + (ty0 + k / ntx) * a.tw + tx0 + k % ntx) != 0;
-  return !__any_sync(0xffffffffu, any);
-}
-
 // The z-chunk [zb, zb + ZC) of column (x, y); returns which z-bricks received a negative
 // value (bit j = brick zb/8 - 1 + j, bit 0 for the dilation of a z % 8 == 0 voxel).
 template <int S, int ZC>
-__device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const float* inv, int x, int y, int zb,
-                                                     bool xin) {
-  // called by the whole warp (x = xb + lane, xin: x < nx)
+__device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const float* inv, int x, int y, int zb) {
   typedef typename Vox<S>::V V;
   typedef typename Vox<S>::Wt Wt;
   // bits 0..ZC/8: NEG of z-bricks zb/8 - 1 + j; bit 6: NEG of z-super-brick zb/64, bit 7:
-  // of zb/64 - 1 (a z % 64 == 0 voxel is that one's +1 layer); the same 8 bits shifted by 8
-  // for LOW
+  // of zb/64 - 1 (a z % 64 == 0 voxel is that one's +1 layer)
   static_assert(ZC == 8 || ZC == 16 || ZC == 32, "z chunk: 8, 16 or 32 voxels");
   uint32_t flags = 0;
 
@@ -151,14 +111,6 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
   const float ku = a.cx + 0.5f, kv = a.cy + 0.5f;
   const int zend = min(ZC, a.nz - zb);
   float px, py, pz;
-  // the brick bits of a voxel (jj: index in its brick, jb: the brick's bit) for NEG
-  // (shift 0) or LOW (shift 8)
-  auto mark = [&](int jj, int jb, int k8, int shift) {
-    uint32_t b = 1u << jb;
-    if (jj == 0) b |= (1u << (jb - 1)) | (((zb + k8) & 63) == 0 ? 0xc0u : 0x40u);
-    else b |= 0x40u;
-    flags |= b << shift;
-  };
   // one voxel of the march (integrate.cs:63-113); jj: its index in the current brick
   auto voxel = [&](int jj, int jb, int k8) {
     if (pz < 0.0001f) return;
@@ -213,29 +165,21 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
       if (bits_of(ew) != bits_of(oldw)) vw[idx] = ew;
       // a non-negative nF never stores a negative value; a brick's first voxel is also
       // the +1 layer of the brick below it (and, at z % 64 == 0, of the super-brick below)
-      if (nF < 0.0f) mark(jj, jb, k8, 0);
-      // LOW from the value as the raycast reads it back
-      if (__fmul_rn(Vox<S>::raw_nc(&ev, 0), Vox<S>::kRawToF) < KF_BRICK_LOW_LEVEL) mark(jj, jb, k8, 8);
+      if (nF < 0.0f) {
+        flags |= 1u << jb;
+        if (jj == 0) flags |= (1u << (jb - 1)) | (((zb + k8) & 63) == 0 ? 0xc0u : 0x40u);
+        else flags |= 0x40u;
+      }
     } else {
       vf[idx] = Vox<S>::encode_value(0.0f);
       vw[idx] = Vox<S>::encode_weight(0.0f);
-      mark(jj, jb, k8, 8);  // zero is below the coarse-step threshold
     }
   };
   // One 8-voxel brick of the column at a time: the position is anchored at the brick's first
   // voxel and steps by delta inside it, as integrate.cs:57-62 does, so it does not depend on
   // where a chunk starts.  Whole bricks run unrolled; only a ragged last brick (nz not a
   // multiple of 8) takes the counted loop.
-  const int xb = x - (int)(threadIdx.x & 31);
   for (int k8 = 0; k8 < zend; k8 += 8) {
-    if (warp_brick_idle(a, inv, xb, y, zb + k8)) {
-      idx += 8 * slice;
-      continue;
-    }
-    if (!xin) {
-      idx += 8 * slice;
-      continue;
-    }
     const float czw = (zb + k8 + 0.5f) * vz;
     px = fmaf(inv[2], czw, pxy[0]);
     py = fmaf(inv[6], czw, pxy[1]);
@@ -259,7 +203,7 @@ struct IntBatch {
 };
 
 template <int S, bool BATCH, int ZC>
-__global__ void __launch_bounds__(256, 5) integrate_kernel(IntArgs a_one, IntBatch batch) {
+__global__ void __launch_bounds__(256, 6) integrate_kernel(IntArgs a_one, IntBatch batch) {
   __shared__ IntArgs s_args;
   int bxi, byi, bzi;  // this block's position in its volume's block grid
   if constexpr (BATCH) {
@@ -301,7 +245,7 @@ __global__ void __launch_bounds__(256, 5) integrate_kernel(IntArgs a_one, IntBat
   const int x = xb + lane;
   const int y = yb + threadIdx.y;  // uniform over the warp
   uint32_t flags = 0;  // integrate_column's bits
-  if (y < a.ny) flags = integrate_column<S, ZC>(a, inv, x, y, zb, x < a.nx);  // y: uniform over the warp
+  if (x < a.nx && y < a.ny) flags = integrate_column<S, ZC>(a, inv, x, y, zb);
   if (!__any_sync(0xffffffffu, flags != 0)) return;
   // Brick flags, merged over the warp: lanes 8c-8..8c-1 write brick column c of the block
   // (c = 1..4) and a lane on a brick's low x face also brick column c-1 (dilation); lane c
@@ -309,9 +253,7 @@ __global__ void __launch_bounds__(256, 5) integrate_kernel(IntArgs a_one, IntBat
   // bits already, so read first and skip those atomics.
   const int lx = (x >> 3) - (xb >> 3) + 1;
   constexpr int kZBits = ZC / 8 + 1;  // z-bricks a chunk touches, with the dilation one
-  constexpr uint32_t kZMask = (1u << kZBits) - 1u;
-  // NEG bits in 0..kZBits-1, LOW bits in 16..16+kZBits-1
-  const uint32_t zbits = (flags & kZMask) | (((flags >> 8) & kZMask) << 16);
+  const uint32_t zbits = flags & ((1u << kZBits) - 1u);
   uint32_t mine = 0;
 #pragma unroll
   for (int c = 0; c < 5; ++c) {
@@ -322,32 +264,30 @@ __global__ void __launch_bounds__(256, 5) integrate_kernel(IntArgs a_one, IntBat
   if (lane < 5 && mine) {
     const int gx = (xb >> 3) - 1 + lane;
     for (int j = 0; j < kZBits; ++j) {
-      const uint32_t want = (((mine >> j) & 1u) ? KF_BRICK_NEG : 0u) | (((mine >> (16 + j)) & 1u) ? KF_BRICK_LOW : 0u);
-      if (!want) continue;
+      if (!((mine >> j) & 1u)) continue;
       const int gz = (zb >> 3) - 1 + j;
       for (int dy = 0; dy < ((y & 7) == 0 ? 2 : 1); ++dy) {
         const int gy = (y >> 3) - dy;
         if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.bx && gy < a.by && gz < a.bz) {
           uint32_t* w = &a.bricks[(uint32_t)gx + (uint32_t)a.bx * ((uint32_t)gy + (uint32_t)a.by * (uint32_t)gz)];
-          if ((*(volatile uint32_t*)w & want) != want) atomicOr(w, want);
+          if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
         }
       }
     }
   }
   // super-bricks: own and, on a super-brick's low face, the one below (x, y, z)
-  const uint32_t sbits = flags & 0xc0c0u;
+  const uint32_t sbits = flags & 0xc0u;
   const uint32_t s_own = __reduce_or_sync(0xffffffffu, sbits);
   const uint32_t s_lowx = __reduce_or_sync(0xffffffffu, (x & 63) == 0 ? sbits : 0u);
   if (lane < 8 && (lane & 1 ? s_own : s_lowx)) {
     const int jx = lane & 1, jy = (lane >> 1) & 1, jz = lane >> 2;
     const uint32_t zsel = jz ? 0x40u : 0x80u;
     const uint32_t src = jx ? s_own : s_lowx;
-    const uint32_t want = ((src & zsel) ? KF_BRICK_NEG : 0u) | ((src & (zsel << 8)) ? KF_BRICK_LOW : 0u);
-    if (want && (jy == 1 || (y & 63) == 0)) {
+    if ((src & zsel) && (jy == 1 || (y & 63) == 0)) {
       const int gx = (xb >> 6) - 1 + jx, gy = (y >> 6) - 1 + jy, gz = (zb >> 6) - 1 + jz;
       if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.sbx && gy < a.sby && gz < a.sbz) {
         uint32_t* w = &a.supers[(uint32_t)gx + (uint32_t)a.sbx * ((uint32_t)gy + (uint32_t)a.sby * (uint32_t)gz)];
-        if ((*(volatile uint32_t*)w & want) != want) atomicOr(w, want);
+        if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
       }
     }
   }
@@ -381,9 +321,6 @@ IntArgs make_int_args(kf_session* s, int gated) {
   a.bx = s->bx; a.by = s->by; a.bz = s->bz;
   a.supers = s->d_supers;
   a.sbx = s->sbx; a.sby = s->sby; a.sbz = s->sbz;
-  a.tiles = s->d_depth_tiles;
-  a.tw = s->tiles_w;
-  a.th = s->tiles_h;
   return a;
 }
 

@@ -18,8 +18,10 @@
 #define KF_TRACK_THREADS 256      // threads per block of the persistent tracking kernels
 #define KF_MAX_TRACK_BLOCKS 1024  // upper bound of the persistent grid
 
-// Words of 8 bytes between two ICP reduction sums (one 128-byte line each).
-#define KF_ACC_STRIDE 16
+// Words of 8 bytes between two ICP reduction sums: 1, so that a warp's atomics on the 32
+// sums of a row fall on two 128-byte lines and coalesce (one sum per line measured slower:
+// 32 separate L2 requests per block instead of two).
+#define KF_ACC_STRIDE 1
 
 // Device-side error word values (KfDevState::error).
 #define KF_DEV_ERR_TIMEOUT 1
@@ -64,9 +66,8 @@ struct KfDevState {
   double icp_hand_cd[3];
   unsigned icp_hand_gi;
   // ICP reduction rows as fixed-point sums (value * 2^32, exact and order-independent),
-  // three buffers used in turn by successive iterations of a launch; every sum on its own
-  // 128-byte line (KF_ACC_STRIDE words apart), so the blocks' 64-bit atomics on the 32
-  // sums of a row spread over the L2 slices instead of queueing on two lines
+  // three buffers used in turn by successive iterations of a launch (KF_ACC_STRIDE words
+  // between sums)
   alignas(128) long long icp_acc[3][32][KF_ACC_STRIDE];
   // the persistent raycast sweep's row-segment queue: next segment, warps done (both zero
   // between launches: the sweep's last warp resets them)
@@ -122,10 +123,6 @@ struct kf_session {
   uint16_t* d_depth_u16 = nullptr;  // upload staging (device)
   float* d_depth_f32_in = nullptr;  // float upload staging (device)
   float* d_depth[3] = {nullptr, nullptr, nullptr};
-  // per 8x8 tile of the level-0 depth: 1 when some pixel of the tile has depth (written with
-  // the pyramid; integrate skips voxel bricks that can only project into empty tiles)
-  uint8_t* d_depth_tiles = nullptr;
-  int tiles_w = 0, tiles_h = 0;
   float4* d_vertex[3] = {nullptr, nullptr, nullptr};
   float4* d_normal[3] = {nullptr, nullptr, nullptr};
   int32_t* d_status[3] = {nullptr, nullptr, nullptr};
@@ -962,12 +959,6 @@ int kf_note_integrate(kf_session* s, cudaStream_t stream);
 // (every KF_BRICK_REBUILD_EVERY integrates, and after a volume upload) clears stale bits,
 // so a clear bit is a guarantee.
 #define KF_BRICK_NEG 1u
-// LOW: some value there may be below KF_BRICK_LOW_LEVEL (raycast's coarse-step threshold 0.8,
-// raycast.cs:199, plus a margin for the trilinear interpolation's rounding).  A region with
-// the bit clear holds no sample below 0.8, so the coarse phase of the march skips it.  Reset
-// sets it everywhere (an all-zero volume is below the threshold everywhere).
-#define KF_BRICK_LOW 2u
-#define KF_BRICK_LOW_LEVEL 0.801f
 #define KF_BRICK_REBUILD_EVERY 16
 int kf_mc_run(kf_session* s, float iso, int method, uint32_t* n_tri);
 int kf_scan_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n, uint32_t* d_total,

@@ -18,8 +18,6 @@ struct PyrArgs {
   const float* in_f32;
   float* depth[3];
   int W[3], H[3];
-  uint8_t* tiles;  // per 8x8 level-0 tile: some pixel has depth
-  int tw, th;
 };
 
 // One thread per level-1 pixel; a 32x8 block also produces a 16x4 level-2 tile.
@@ -28,13 +26,10 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256) depth_mip_kernel(PyrArgs one, const PyrArgs* many,
                                                         const uint16_t* const* inputs) {
   __shared__ float s_l1[8][33];
-  __shared__ int s_tile[2][8];  // the block's 8 x 2 tiles of 8x8 level-0 pixels
   PyrArgs a = BATCH ? many[blockIdx.z] : one;
   if (BATCH && inputs) a.in_u16 = inputs[blockIdx.z];  // this step's frame, read in place
   const int x1 = blockIdx.x * 32 + threadIdx.x;
   const int y1 = blockIdx.y * 8 + threadIdx.y;
-  if (threadIdx.y == 0 && threadIdx.x < 16) s_tile[threadIdx.x >> 3][threadIdx.x & 7] = 0;
-  __syncthreads();
   float m = 0.0f;
   if (x1 < a.W[1] && y1 < a.H[1]) {
     const int W0 = a.W[0];
@@ -53,14 +48,9 @@ __global__ void __launch_bounds__(256) depth_mip_kernel(PyrArgs one, const PyrAr
     *reinterpret_cast<float2*>(a.depth[0] + i0 + W0) = make_float2(d10, d11);
     m = 0.25f * ((d00 + d01) + (d10 + d11));
     a.depth[1][(size_t)y1 * a.W[1] + x1] = m;
-    if (d00 != 0.0f || d01 != 0.0f || d10 != 0.0f || d11 != 0.0f) s_tile[threadIdx.y >> 2][threadIdx.x >> 2] = 1;
   }
   s_l1[threadIdx.y][threadIdx.x] = m;
   __syncthreads();
-  if (threadIdx.y == 1 && threadIdx.x < 16) {
-    const int tx = blockIdx.x * 8 + (threadIdx.x & 7), ty = blockIdx.y * 2 + (threadIdx.x >> 3);
-    if (tx < a.tw && ty < a.th) a.tiles[(size_t)ty * a.tw + tx] = (uint8_t)s_tile[threadIdx.x >> 3][threadIdx.x & 7];
-  }
   if (threadIdx.x < 16 && threadIdx.y < 4) {
     const int x2 = blockIdx.x * 16 + threadIdx.x;
     const int y2 = blockIdx.y * 4 + threadIdx.y;
@@ -171,9 +161,6 @@ PyrArgs make_pyr_args(kf_session* s, const uint16_t* d_u16, const float* d_f32) 
     a.W[l] = s->W[l];
     a.H[l] = s->H[l];
   }
-  a.tiles = s->d_depth_tiles;
-  a.tw = s->tiles_w;
-  a.th = s->tiles_h;
   return a;
 }
 

@@ -133,22 +133,20 @@ __device__ __forceinline__ void raycast_pixel(const RayArgs& a, const float* s_v
           const int vz = min(max((int)floorf(qz), 0), a.nz - 1);
           int cell = 0;  // 0: sample it; else the side of the region to skip (64 or 8)
           int cx = 0, cy = 0, cz = 0, ncx = 1, ncy = 1, ncz = 1;
-          // fine phase: a region without a negative value holds no first negative sample;
-          // coarse phase: a region without a value below 0.8 (with the flags' margin) holds
-          // no sample that switches to the fine step, nor a negative one
-          const uint32_t need = fine ? KF_BRICK_NEG : KF_BRICK_LOW;
-          if (!(__ldg(a.supers + (uint32_t)(vx >> 6) +
-                      (uint32_t)a.sbx * ((uint32_t)(vy >> 6) + (uint32_t)a.sby * (uint32_t)(vz >> 6))) &
-                need)) {
-            cell = 64;
-            cx = vx >> 6; cy = vy >> 6; cz = vz >> 6;
-            ncx = a.sbx; ncy = a.sby; ncz = a.sbz;
-          } else if (!(__ldg(a.bricks + (uint32_t)(vx >> 3) +
-                             (uint32_t)a.bx * ((uint32_t)(vy >> 3) + (uint32_t)a.by * (uint32_t)(vz >> 3))) &
-                       need)) {
-            cell = 8;
-            cx = vx >> 3; cy = vy >> 3; cz = vz >> 3;
-            ncx = a.bx; ncy = a.by; ncz = a.bz;
+          if (fine) {
+            if (!(__ldg(a.supers + (uint32_t)(vx >> 6) +
+                        (uint32_t)a.sbx * ((uint32_t)(vy >> 6) + (uint32_t)a.sby * (uint32_t)(vz >> 6))) &
+                  KF_BRICK_NEG)) {
+              cell = 64;
+              cx = vx >> 6; cy = vy >> 6; cz = vz >> 6;
+              ncx = a.sbx; ncy = a.sby; ncz = a.sbz;
+            } else if (!(__ldg(a.bricks + (uint32_t)(vx >> 3) +
+                               (uint32_t)a.bx * ((uint32_t)(vy >> 3) + (uint32_t)a.by * (uint32_t)(vz >> 3))) &
+                         KF_BRICK_NEG)) {
+              cell = 8;
+              cx = vx >> 3; cy = vy >> 3; cz = vz >> 3;
+              ncx = a.bx; ncy = a.by; ncz = a.bz;
+            }
           }
           if (cell) {
             // the region spans [cell*i, cell*(i+1)) in voxel coordinates; the border ones
@@ -389,10 +387,9 @@ __global__ void __launch_bounds__(128) mip_kernel(RayArgs a, float4* out) {
   out[(size_t)y * a.W + x] = make_float4(sum, 0.0f, 0.0f, 1.0f);
 }
 
-// Exact flags from the volume itself: a brick B is NEG when a value over the voxels
-// [8B, 8B+8] (clamped to the volume) is negative and LOW when one is below
-// KF_BRICK_LOW_LEVEL, a super-brick when one of its 8^3 bricks is (super-bricks are cleared
-// first and set here).  A block takes one row of 32 bricks
+// Exact NEG flags from the volume itself: a brick B is NEG when a value over the voxels
+// [8B, 8B+8] (clamped to the volume) is negative, a super-brick when one of its 8^3 bricks
+// is (super-bricks are cleared first and set here).  A block takes one row of 32 bricks
 // along x at brick (y, z): thread t scans voxel column x0 + t over the brick's 9 x 9 (y, z)
 // window (coalesced along x), the extra warp the first columns of the next row (the +1
 // layer of the last brick), and thread c merges brick c's 9 columns from shared memory.
@@ -407,32 +404,31 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_bricks_kernel(const v
   const int x = blockIdx.x * 256 + threadIdx.x;
   const int y0 = 8 * blockIdx.y, y1 = min(y0 + 8, ny - 1);
   const int z0 = 8 * blockIdx.z, z1 = min(z0 + 8, nz - 1);
-  uint32_t m = 0;  // KF_BRICK_NEG | KF_BRICK_LOW found in this column
+  bool neg = false;
   if (x < nx)
-    for (int z = z0; z <= z1 && m != (KF_BRICK_NEG | KF_BRICK_LOW); ++z) {
-      // the plane's (up to) 9 rows are loaded together; the scan stops once both are found
+    for (int z = z0; z <= z1 && !neg; ++z) {
+      // the plane's (up to) 9 rows are loaded together; the scan stops after a plane
       const uint32_t base = (uint32_t)x + (uint32_t)nx * (uint32_t)ny * (uint32_t)z;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         const int y = min(y0 + k, y1);  // rows past the volume repeat the last one
-        const float r = Vox<S>::raw(f, base + (uint32_t)nx * (uint32_t)y);
-        if (r < 0.0f) m |= KF_BRICK_NEG;
-        if (r * Vox<S>::kRawToF < KF_BRICK_LOW_LEVEL) m |= KF_BRICK_LOW;  // as the raycast scales it
+        neg |= Vox<S>::raw(f, base + (uint32_t)nx * (uint32_t)y) < 0.0f;
       }
     }
-  s_neg[threadIdx.x] = (uint8_t)m;
+  s_neg[threadIdx.x] = neg ? 1 : 0;
   __syncthreads();
   const int c = threadIdx.x;
   const int b = blockIdx.x * 32 + c;
   if (c < 32 && b < bx) {
-    uint32_t flag = 0;
+    uint8_t m = 0;
 #pragma unroll
-    for (int k = 0; k <= 8; ++k) flag |= s_neg[8 * c + k];  // columns past nx - 1 hold 0
+    for (int k = 0; k <= 8; ++k) m |= s_neg[8 * c + k];  // columns past nx - 1 hold 0
+    const uint32_t flag = m ? KF_BRICK_NEG : 0u;
     bricks[(uint32_t)b + (uint32_t)bx * ((uint32_t)blockIdx.y + (uint32_t)by * (uint32_t)blockIdx.z)] = flag;
     if (flag) {
       uint32_t* w = &supers[(uint32_t)(b >> 3) +
                             (uint32_t)sbx * ((uint32_t)(blockIdx.y >> 3) + (uint32_t)sby * (uint32_t)(blockIdx.z >> 3))];
-      if ((*(volatile uint32_t*)w & flag) != flag) atomicOr(w, flag);
+      if (!(*(volatile uint32_t*)w & KF_BRICK_NEG)) atomicOr(w, KF_BRICK_NEG);
     }
   }
 }
@@ -469,10 +465,9 @@ int kf_note_integrate(kf_session* s, cudaStream_t stream) {
 }
 
 int kf_reset_bricks(kf_session* s) {
-  // an all-zero volume has no negative value and is below the coarse-step threshold
-  // everywhere: every word gets KF_BRICK_LOW (bytes 0x02; the other bits are unused)
+  // an all-zero volume has no negative value
   const size_t words = (size_t)s->bx * s->by * s->bz + (size_t)s->sbx * s->sby * s->sbz;
-  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, KF_BRICK_LOW, words * 4, s->stream));
+  KF_CUDA_TRY(s, cudaMemsetAsync(s->d_bricks, 0, words * 4, s->stream));
   s->frames_since_rebuild = 0;
   return KF_OK;
 }
