@@ -305,12 +305,7 @@ typedef struct kf_launch_shape {
   int32_t raycast_rows;      /* raycast tile of 32 x rows pixels: 2, 4 (default) or 8;  */
                              /* 1 = persistent sweep, every warp taking the next 32-pixel */
                              /* row segment from a queue (sessions only, not batches)     */
-  int32_t icp_coarse_pixels; /* ICP pyramid levels 1 and 2 run on ceil(pixels / this)      */
-                             /* blocks of the persistent grid (level 0 on all of them):    */
-                             /* 256..65536, 0 = 512 (default), -1 = every block.  Sessions */
-                             /* with split-BF16 J^T J only (their sums do not depend on the */
-                             /* split); other sessions and batches use every block.        */
-  int32_t reserved[5];
+  int32_t reserved[6];
 } kf_launch_shape;
 KF_API int kf_set_launch_shape(kf_session* s, const kf_launch_shape* shape);
 KF_API int kf_get_launch_shape(kf_session* s, kf_launch_shape* shape);

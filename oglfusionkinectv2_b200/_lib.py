@@ -77,8 +77,7 @@ class kf_volume_view(C.Structure):
 
 
 class kf_launch_shape(C.Structure):
-    _fields_ = [("integrate_z_chunk", C.c_int32), ("raycast_rows", C.c_int32), ("icp_coarse_pixels", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+    _fields_ = [("integrate_z_chunk", C.c_int32), ("raycast_rows", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class kf_ir_camera(C.Structure):

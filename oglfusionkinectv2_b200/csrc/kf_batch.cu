@@ -25,9 +25,7 @@ __global__ void batch_clear_kernel(KfDevState* const* states) {
   if (threadIdx.x == 0) {
     st->barrier_count = 0;
     st->sdf_barrier_count = 0;
-    st->icp_stage = 0;
   }
-  if (threadIdx.x < 3) st->icp_lvl_barrier[threadIdx.x][0] = 0;
   for (int k = threadIdx.x; k < 3 * 32; k += blockDim.x) st->icp_acc[k / 32][k % 32][0] = 0;
 }
 

@@ -1236,13 +1236,10 @@ int kf_get_stream(kf_session* s, void** stream) {
 int kf_set_launch_shape(kf_session* s, const kf_launch_shape* shape) {
   if (!s || !shape || !kf_valid_int_zc(shape->integrate_z_chunk) || !kf_valid_ray_rows(shape->raycast_rows))
     return KF_ERR_INVALID_ARGUMENT;
-  const int icp = shape->icp_coarse_pixels;
-  if (!(icp == 0 || icp == -1 || (icp >= 256 && icp <= 65536))) return KF_ERR_INVALID_ARGUMENT;
   KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   drop_graph(s);  // the captured frames hold the old shapes
   s->int_zc = shape->integrate_z_chunk;
   s->ray_rows = shape->raycast_rows;
-  s->icp_coarse_px = icp == 0 ? 512 : (icp < 0 ? 0 : icp);
   return KF_OK;
 }
 
@@ -1251,7 +1248,6 @@ int kf_get_launch_shape(kf_session* s, kf_launch_shape* shape) {
   std::memset(shape, 0, sizeof(*shape));
   shape->integrate_z_chunk = s->int_zc;
   shape->raycast_rows = s->ray_rows;
-  shape->icp_coarse_pixels = s->icp_coarse_px > 0 ? s->icp_coarse_px : -1;
   return KF_OK;
 }
 
@@ -1298,7 +1294,6 @@ int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* time
   kf_launch_shape sh{};
   sh.integrate_z_chunk = kf_tune_int_zc[zi];
   sh.raycast_rows = kf_tune_ray_rows[ri - 3];
-  sh.icp_coarse_pixels = s->icp_coarse_px > 0 ? s->icp_coarse_px : -1;
   if ((rc = kf_set_launch_shape(s, &sh))) return rc;
   kf_tune_cache_put(s, sh.integrate_z_chunk, sh.raycast_rows);
   if (chosen) *chosen = sh;

@@ -32,8 +32,6 @@
 // makes the valid count and the point sums (for the next centre) columns of the same
 // products.  Each warp converts its 32-pixel chunk's sums to fixed point, so a chunk
 // contributes the same bits whichever block, grid or batch processes it.
-#include <algorithm>
-
 #include "kf_internal.cuh"
 
 namespace {
@@ -53,7 +51,6 @@ struct IcpArgs {
   int same_pixel;         // Q4
   int frame_policy;
   int integrate_every;
-  int lvl_blocks[3];      // blocks that run level l (0: all); non-decreasing towards level 0
   KfDevState* st;
 };
 
@@ -168,6 +165,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
   __shared__ double s_csums[29], s_ccenter[3], s_ae;  // last centred row (for the tail)
   __shared__ double s_nvalid;                           // its valid-pixel count
   __shared__ double s_gx[8 + 228];                      // the rank-guarded step (rare path)
+  __shared__ int s_fast;                                // the rank check's verdict
   __shared__ int s_flag, s_conv;
   __shared__ __align__(16) __nv_bfloat16 s_hi[JTJ ? kWarps : 1][8][40];
   __shared__ __align__(16) __nv_bfloat16 s_mid[JTJ ? kWarps : 1][8][40];
@@ -211,9 +209,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
 
   bool ok = true;
   int iters_run = 0;
-  unsigned gi = 0;  // iterations of this launch so far: selects the sum buffer
-  bool active = false;  // this block ran the previous level
-  __shared__ unsigned s_gi;
+  unsigned gi = 0;  // iterations of this launch so far: grid barrier target and sum buffer
   // the first step's vertices and normals of the next iteration, loaded while the current
   // iteration's system is solved (valid when pre_level is the level that runs)
   const float4 none = make_float4(2.0f, 0.f, 0.f, 0.f), zero = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -222,43 +218,6 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
   for (int level = 2; level >= 0 && ok; --level) {
     const int Wl = a.W[level], Hl = a.H[level];
     const int P = Wl * Hl;
-    // the coarse levels' few pixels run on the first nbl blocks: fewer blocks to reduce and
-    // wait for.  With split-BF16 J^T J the sums (fixed point per 32-pixel chunk) do not depend
-    // on how many blocks share the pixels.
-    const unsigned nbl = a.lvl_blocks[level] > 0 ? min(nb, (unsigned)a.lvl_blocks[level]) : nb;
-    if (local >= nbl) continue;  // this level runs without this block
-    if (!active && level < 2) {
-      // joining a finer level: wait for the coarser levels (their last iteration's block 0
-      // hands over the pose, the centre and the iteration count); bounded like the barrier
-      if (tid == 0) {
-        int okw = 1;
-        const long long t0 = clock64();
-        while (kf_ld_acquire_gpu(&st->icp_stage) < (unsigned)(2 - level)) {
-          if (*(volatile int*)&st->error) { okw = 0; break; }
-          if (clock64() - t0 > KF_BARRIER_SPIN_CYCLES) {
-            atomicExch(&st->error, KF_DEV_ERR_TIMEOUT);
-            okw = 0;
-            break;
-          }
-          __nanosleep(64);
-        }
-        if (okw) {
-          for (int k = 0; k < 16; ++k) s_pose[k] = __ldcg(&st->icp_hand_pose[k]);
-          for (int r = 0; r < 3; ++r) {
-            s_cd[r] = __ldcg(&st->icp_hand_cd[r]);
-            s_c[r] = (float)s_cd[r];
-          }
-          s_gi = __ldcg(&st->icp_hand_gi);
-          make_float_mats(a, s_pose, s_ray, s_T, s_V);
-        }
-        s_flag = okw;
-      }
-      __syncthreads();
-      ok = s_flag != 0;
-      if (!ok) break;
-      gi = s_gi;
-    }
-    active = true;
     for (int it = 0; it < a.iters[level]; ++it) {
       // Ttrack and view stay in shared memory (broadcast reads), which leaves the registers
       // for two pixels in flight per thread
@@ -266,7 +225,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       c[0] = s_c[0]; c[1] = s_c[1]; c[2] = s_c[2];
 
       // ---------------- track + accumulate ----------------
-      long long* accbuf = &a.st->icp_acc[gi % 3u][0][0];  // sum k at accbuf[k * KF_ACC_STRIDE]
+      long long* accbuf = &a.st->icp_acc[gi % 3u][0][0];
       float acc[JTJ ? 1 : 28];
 #pragma unroll
       for (int k = 0; k < (JTJ ? 1 : 28); ++k) acc[k] = 0.0f;
@@ -347,7 +306,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       // Each warp takes two 32-pixel chunks per step (the chunks of two consecutive grid
       // passes), so two pixels' gathers are in flight per thread, and the step after that
       // one's vertices and normals are loaded meanwhile.
-      const int stride = nbl * KF_TRACK_THREADS;
+      const int stride = nb * KF_TRACK_THREADS;
       const float4* Nl = a.normal[level];
       const float4* Vl = a.vertex[level];
       const int first = (local * kWarps + warp) * 32;
@@ -408,9 +367,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
           float v = 0.0f;
 #pragma unroll
           for (int w = 0; w < kWarps; ++w) v += tid < 28 ? s_warp[w][tid] : s_pw[w][tid - 28];
-          // adding zero changes nothing: blocks without pixels at a coarse level skip it
-          const long long q = __float2ll_rn(v * kFix);
-          if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid * KF_ACC_STRIDE), (unsigned long long)q);
+          atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid), (unsigned long long)__float2ll_rn(v * kFix));
         }
       } else {
         // lane (g, t) holds M[g][2t], M[g][2t+1]; lanes t == 3 also sum q_g
@@ -442,8 +399,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) v += s_fix[w][64 + tid - 29] + s_fix[w][64 + tid - 26];
           }
-          // adding zero changes nothing: blocks without pixels at a coarse level skip it
-          if (v != 0) atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid * KF_ACC_STRIDE), (unsigned long long)v);
+          atomicAdd(reinterpret_cast<unsigned long long*>(accbuf + tid), (unsigned long long)v);
         }
       }
       // the buffer of the next iteration was last read before the previous barrier
@@ -453,7 +409,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       // Every block reads the same exact sums and solves the same system in FP64, so all
       // blocks hold bit-identical results without a second hand-over, and the solve's code
       // stays warm in every SM's instruction cache.
-      ok = kf_grid_sync(st, &st->icp_lvl_barrier[level][0], nbl * (unsigned)(it + 1), &s_flag);
+      ok = kf_grid_sync(st, &st->barrier_count, nb * (gi + 1u), &s_flag);
       if (!ok) break;
       {
         // the next iteration runs this level again unless the level's iterations are used up
@@ -461,8 +417,6 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
         const int nl = it + 1 < a.iters[level] ? level : level - 1;
         pre_level = nl;
         pn0 = none; pv0 = zero; pn1 = none; pv1 = zero;
-        const unsigned nbn = nl >= 0 ? (a.lvl_blocks[nl] > 0 ? min(nb, (unsigned)a.lvl_blocks[nl]) : nb) : nb;
-        const int stride = (int)nbn * KF_TRACK_THREADS;  // the next level's
         if (nl >= 0) {
           const int Pn = a.W[nl] * a.H[nl];
           const int f0 = (local * kWarps + warp) * 32;
@@ -473,18 +427,38 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
           }
         }
       }
-      if (tid < 32) s_sums[tid] = (double)__ldcg(accbuf + tid * KF_ACC_STRIDE) * kInvFix;
+      if (tid < 32) s_sums[tid] = (double)__ldcg(accbuf + tid) * kInvFix;
       __syncthreads();
+      if (warp == 1) {
+        // the rank guard's check (KF_ICP_RANK_TAU), in FP32 beside warp 0's FP64 solve
+        const int fast = kf_icp_rank_check_warp(&s_sums[7], s_cd, lane);
+        if (lane == 0) s_fast = fast;
+        asm volatile("bar.sync 1, 64;" ::: "memory");  // warps 0 and 1
+      }
       if (warp == 0) {
         // ---- solve, lane-parallel in warp 0 ----
         // reduce.cs counts every pixel of the (group-7) rows in sums[28]
         const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
         const double nvalid = s_sums[28];
-        // the step in the reference's variables (JacobiSVD::solve, :696-697, with the rank
-        // guard of KF_ICP_RANK_TAU)
+        const double cx = s_cd[0], cy = s_cd[1], cz = s_cd[2];
+        double xp[6];
+        const bool spd = kf_cholesky6_warp(&s_sums[7], &s_sums[1], xp, lane);
+        // back to the reference's variables: w = w', t = t' - w x c
         double x[6];
-        int guarded;
-        kf_icp_solve_warp(&s_sums[7], &s_sums[1], s_cd, x, lane, s_gx, &guarded);
+        x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
+        x[0] = xp[0] - (x[4] * cz - x[5] * cy);
+        x[1] = xp[1] - (x[5] * cx - x[3] * cz);
+        x[2] = xp[2] - (x[3] * cy - x[4] * cx);
+        asm volatile("bar.sync 1, 64;" ::: "memory");  // warp 1's rank check is in s_fast
+        if (!(spd && s_fast)) {
+          // a degenerate view (rare): the rank-guarded minimum-norm step of the world-frame
+          // system (JacobiSVD::solve, :696-697, with the cut of KF_ICP_RANK_TAU)
+          if (lane == 0) kf_icp_world_guarded_step(&s_sums[7], &s_sums[1], s_cd, s_gx, s_gx + 8);
+          __syncwarp();
+#pragma unroll
+          for (int k = 0; k < 6; ++k) x[k] = s_gx[k];
+          __syncwarp();
+        }
         // delta = eulerAngleXYZ(x3, x4, x5), delta[3].xyz = x0..2 (gFusion.cpp:700-703);
         // lanes 0..2 evaluate the three sincos at once
         double sn, cs;
@@ -537,14 +511,6 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
       __syncthreads();
       ++iters_run;
       if (s_conv) break;  // result.norm() < 1e-5 && != 0 leaves this level (:707-708)
-    }
-    if (ok && level > 0 && local == 0 && tid == 0) {
-      // hand the level's result to the blocks that join the next one
-      for (int k = 0; k < 16; ++k) st->icp_hand_pose[k] = s_pose[k];
-      for (int r = 0; r < 3; ++r) st->icp_hand_cd[r] = s_cd[r];
-      st->icp_hand_gi = gi;
-      __threadfence();
-      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&st->icp_stage) : "memory");
     }
   }
 
@@ -632,17 +598,8 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
 
 namespace {
 
-IcpArgs make_icp_args(kf_session* s, int frame_policy, bool batched) {
+IcpArgs make_icp_args(kf_session* s, int frame_policy) {
   IcpArgs a;
-  // the coarse levels on ceil(pixels / icp_coarse_px) blocks (single sessions, split-BF16
-  // J^T J, whose sums do not depend on the split); level 0 on every block
-  for (int l = 0; l < 3; ++l) {
-    const int P = s->W[l] * s->H[l];
-    a.lvl_blocks[l] = (!batched && l > 0 && s->icp_coarse_px > 0 && s->cfg.jtj == KF_JTJ_SPLIT_BF16)
-                          ? std::max(1, (P + s->icp_coarse_px - 1) / s->icp_coarse_px)
-                          : 0;
-  }
-  if (a.lvl_blocks[1] > 0 && a.lvl_blocks[2] > a.lvl_blocks[1]) a.lvl_blocks[2] = a.lvl_blocks[1];
   for (int l = 0; l < 3; ++l) {
     a.vertex[l] = s->d_vertex[l];
     a.normal[l] = s->d_normal[l];
@@ -683,7 +640,7 @@ cudaLaunchConfig_t coop_config(dim3 grid, cudaStream_t stream, cudaLaunchAttribu
 }  // namespace
 
 int kf_launch_icp(kf_session* s, int frame_policy) {
-  const IcpArgs a = make_icp_args(s, frame_policy, false);
+  const IcpArgs a = make_icp_args(s, frame_policy);
   const void* fn = (s->cfg.jtj == KF_JTJ_SPLIT_BF16) ? (const void*)icp_kernel<1, false>
                                                       : (const void*)icp_kernel<0, false>;
   int blocks = kf_occupancy_blocks(s, fn, KF_TRACK_THREADS, 0);
@@ -707,7 +664,7 @@ int kf_batch_prepare_icp(kf_batch* b) {
   IcpArgs* h = nullptr;
   b->icp_args = kf_batch_table(b, sizeof(IcpArgs) * n, reinterpret_cast<void**>(&h));
   if (!b->icp_args) return KF_ERR_CAPACITY;
-  for (int e = 0; e < n; ++e) h[e] = make_icp_args(b->members[e], 1, true);
+  for (int e = 0; e < n; ++e) h[e] = make_icp_args(b->members[e], 1);
   kf_session* s0 = b->members[0];
   const void* fn = (s0->cfg.jtj == KF_JTJ_SPLIT_BF16) ? (const void*)icp_kernel<1, true>
                                                        : (const void*)icp_kernel<0, true>;

@@ -31,9 +31,6 @@ struct IntArgs {
   int W, H;
   float fx, fy, cx, cy;
   float mu, inv_mu, maxw;
-  // eta is surely <= -mu when d - z < behind_cut, and surely >= mu when d - z > free_cut:
-  // the ray-length factor sqrt(1 + (x/z)^2 + (y/z)^2) is >= 1 (rounding margin 2^-16)
-  float behind_cut, free_cut;
   int band;  // Q8
   const int* gate;
   const KfDevState* st;
@@ -121,25 +118,12 @@ __device__ __forceinline__ uint32_t integrate_column(const IntArgs& a, const flo
     const float u = fmaf(a.fx, rx, ku);
     const float v = fmaf(a.fy, ry, kv);
     if (u < 0.0f || u > fW1 || v < 0.0f || v > fH1) return;
-    // uvec2(pixel): u, v >= 0 here, so truncation is floor; adding 2^23 rounded toward zero
-    // leaves floor(u) in the low mantissa bits (exact for u < 2^23), without a conversion
-    // instruction
-    const uint32_t ui = (uint32_t)(__float_as_int(__fadd_rz(u, 8388608.0f)) - 0x4B000000);
-    const uint32_t vi = (uint32_t)(__float_as_int(__fadd_rz(v, 8388608.0f)) - 0x4B000000);
     // explicitly rounded: no template instance may fuse the scaling into the subtraction,
     // so every launch shape computes the same bits
-    const float d = __fmul_rn(__ldg(a.depth + vi * (uint32_t)a.W + ui), 0.001f);
+    const float d = __fmul_rn(__ldg(a.depth + (uint32_t)(int)v * (uint32_t)a.W + (uint32_t)(int)u), 0.001f);
     if (d == 0.0f) return;
-    const float dz = __fsub_rn(d, pz);
-    float diff;
-    if (dz < a.behind_cut) {
-      diff = -2.0f * a.mu;  // far behind the surface: the zeroing branch, as computed below
-    } else if (dz > a.free_cut) {
-      diff = 2.0f * a.mu;   // well in front: sdf = min(1, eta / mu) = 1
-    } else {
-      const float r2 = fmaf(rx, rx, fmaf(ry, ry, 1.0f));
-      diff = __fmul_rn(dz, __fmul_rn(r2, rsqrtf(r2)));  // sqrt(r2), r2 >= 1
-    }
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, 1.0f));
+    const float diff = __fmul_rn(__fsub_rn(d, pz), __fmul_rn(r2, rsqrtf(r2)));  // sqrt(r2), r2 >= 1
     if (diff > -a.mu) {
       const float sdf = fminf(1.0f, __fmul_rn(diff, a.inv_mu));
       const V oldv = vf[idx];
@@ -309,11 +293,6 @@ IntArgs make_int_args(kf_session* s, int gated) {
   a.mu = s->cfg.mu;
   a.inv_mu = 1.0f / s->cfg.mu;
   a.maxw = s->cfg.max_weight;
-  // eta = (d - z) * f with f = r2 * rsqrtf(r2) >= 1 - 3.2e-7 (rsqrtf within 2 ulp, one
-  // rounding) and r2 >= 1 exactly: |d - z| >= mu (1 + 2^-16) gives |eta| > mu after the
-  // product's rounding, so the shortcut takes the same branch and sdf as the full formula
-  a.behind_cut = (float)(-(double)s->cfg.mu * (1.0 + 1.0 / 65536.0));
-  a.free_cut = (float)((double)s->cfg.mu * (1.0 + 1.0 / 65536.0));
   a.band = (s->cfg.quirks & KF_Q8_NARROW_BAND) ? 1 : 0;
   a.gate = gated ? &s->d_state->do_integrate : nullptr;
   a.st = s->d_state;

@@ -57,14 +57,6 @@ struct KfDevState {
   // reduction atomics land elsewhere)
   alignas(128) unsigned barrier_count;      // grid barrier of the ICP launch
   alignas(128) unsigned sdf_barrier_count;  // grid barrier of the SDF launch
-  // the ICP launch's per-level grid barriers (levels 2, 1 may run on fewer blocks than
-  // level 0), the count of finished levels, and the hand-over to the blocks that join a
-  // finer level: pose, accumulation centre and iteration count at its start
-  alignas(128) unsigned icp_lvl_barrier[3][32];
-  alignas(128) unsigned icp_stage;
-  alignas(128) double icp_hand_pose[16];
-  double icp_hand_cd[3];
-  unsigned icp_hand_gi;
   // ICP reduction rows as fixed-point sums (value * 2^32, exact and order-independent),
   // three buffers used in turn by successive iterations of a launch (KF_ACC_STRIDE words
   // between sums)
@@ -195,7 +187,6 @@ struct kf_session {
 
   // launch shapes (kf_set_launch_shape / kf_autotune); every choice computes the same result
   int int_zc = 16;   // integrate: voxels per thread along z (8, 16, 32)
-  int icp_coarse_px = 512;  // ICP levels 2, 1: pixels per block (0: every block)
   int ray_rows = 4;  // raycast: tile rows of 32 pixels (2, 4, 8), or 1: persistent sweep
 
   // depth ingest before the pyramid (off by default): Kinect-v2 undistortion through a
@@ -671,85 +662,83 @@ __device__ inline void kf_icp_world_guarded_step(const double* v21c, const doubl
   for (int k = 0; k < 6; ++k) out[k] = xw[k];
 }
 
-// The ICP step for one warp, from the centred sums (v21c: reduce.cs rows 7..27 of
-// J' = [n, (p - c) x n], bc: rows 1..6) about the centre c; every lane returns the
-// world-frame step x = (t, w) of gFusion.cpp:696-703.  The centred system C' = M^-T C M^-1
-// (M: t' = t - [c]x w) is solved by the lane-parallel Cholesky; that solution is kept when
-// the world-frame C provably keeps every direction under KF_ICP_RANK_TAU:
-// l_min >= 1 / trace(C^-1) and l_max <= trace(C), with trace(C) = sum_i m_i^T C' m_i
-// (m_i = M e_i) and (C^-1)_ii = |L'^-1 M^-T e_i|^2 for C' = L' L'^T.  Otherwise (rare: a
-// degenerate view) lane 0 forms the world-frame system and runs kf_icp_guarded_solve.
-// s_scratch: 8 + 228 doubles of shared memory (the step in the first 6).  *guarded is set
-// when that path ran.
-__device__ inline void kf_icp_solve_warp(const double* v21c, const double* bc, const double* c, double* x,
-                                         int lane, double* s_scratch, int* guarded) {
-  double xp[6], Lrow[6], inv_diag = 0.0;
-  const bool spd = kf_cholesky6_warp(v21c, bc, xp, lane, Lrow, &inv_diag);
-  const double cx = c[0], cy = c[1], cz = c[2];
+// The rank guard's check for one warp, in FP32 (run beside the FP64 solve, off its
+// critical path): 1 when the world-frame C provably keeps every direction under
+// KF_ICP_RANK_TAU, so that the centred system's Cholesky solution is the guarded step.
+// v21c: reduce.cs rows 7..27 of the centred J' = [n, (p - c) x n] about c, i.e.
+// C' = M^-T C M^-1 with M: t' = t - [c]x w.  Bounds: l_min >= 1 / trace(C^-1),
+// l_max <= trace(C), with trace(C) = sum_i m_i^T C' m_i (m_i = M e_i) and
+// (C^-1)_ii = |L'^-1 M^-T e_i|^2 for C' = L' L'^T.  A factor of 2 covers FP32's rounding:
+// the cut is 1e-5, far above FP32's 6e-8, and a Cholesky too ill-conditioned for FP32 gives
+// a large trace (or a non-positive pivot) and fails the check, leaving the decision to the
+// exact FP64 path.
+__device__ inline int kf_icp_rank_check_warp(const double* v21c, const double* c, int lane) {
   auto at = [&](int i, int j) {
     if (i > j) { const int t = i; i = j; j = t; }
-    return v21c[6 * i - (i * (i - 1)) / 2 + (j - i)];
+    return (float)v21c[6 * i - (i * (i - 1)) / 2 + (j - i)];
   };
-  bool fast = false;
-  if (spd) {
-    // lane i < 6: u = M^-T e_i, z = L'^-1 u (forward substitution, L' broadcast by
-    // shuffles), and C_ii = m^T C' m with m = M e_i.  For i < 3: u = (e_i; -(c x e_i)),
-    // m = e_i; for i = 3 + k: u = e_i, m = (-(c x e_k); e_k).
-    const int i = lane < 6 ? lane : 0;
-    const int k3 = i < 3 ? i : i - 3;
-    // c x e_k
-    const double ck0 = k3 == 0 ? 0.0 : (k3 == 1 ? -cz : cy);
-    const double ck1 = k3 == 0 ? cz : (k3 == 1 ? 0.0 : -cx);
-    const double ck2 = k3 == 0 ? -cy : (k3 == 1 ? cx : 0.0);
-    double z[6];
-    double zz = 0.0;
+  const int i = lane < 6 ? lane : 5;
+  float row[6], Lrow[6];
 #pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      double v = j == i ? 1.0 : 0.0;
-      if (i < 3 && j >= 3) v = -(j == 3 ? ck0 : (j == 4 ? ck1 : ck2));
-#pragma unroll
-      for (int k = 0; k < j; ++k) v = fma(-__shfl_sync(0xffffffffu, Lrow[k], j), z[k], v);
-      z[j] = v * __shfl_sync(0xffffffffu, inv_diag, j);
-      zz = fma(z[j], z[j], zz);
-    }
-    double D;
-    if (i < 3) {
-      D = at(i, i);
-    } else {
-      // m = (-ck; e_k): m^T C' m = ck^T C'_tt ck - 2 ck^T C'_t,(3+k) + C'_(3+k),(3+k)
-      const double m0 = -ck0, m1 = -ck1, m2 = -ck2;
-      const double r0 = at(0, 0) * m0 + at(0, 1) * m1 + at(0, 2) * m2;
-      const double r1 = at(1, 0) * m0 + at(1, 1) * m1 + at(1, 2) * m2;
-      const double r2 = at(2, 0) * m0 + at(2, 1) * m1 + at(2, 2) * m2;
-      D = m0 * r0 + m1 * r1 + m2 * r2 + 2.0 * (m0 * at(0, i) + m1 * at(1, i) + m2 * at(2, i)) + at(i, i);
-    }
-    double tinv = lane < 6 ? zz : 0.0;  // (C^-1)_ii
-    double tr = lane < 6 ? D : 0.0;     // C_ii
-#pragma unroll
-    for (int o = 4; o >= 1; o >>= 1) {
-      tinv += __shfl_xor_sync(0xffffffffu, tinv, o);
-      tr += __shfl_xor_sync(0xffffffffu, tr, o);
-    }
-    // lanes 0..7 hold the sums over lanes 0..7 (lanes 6, 7 add nothing)
-    tinv = __shfl_sync(0xffffffffu, tinv, 0);
-    tr = __shfl_sync(0xffffffffu, tr, 0);
-    fast = tinv * tr * KF_ICP_RANK_TAU <= 1.0;
+  for (int j = 0; j < 6; ++j) {
+    row[j] = at(i, j);
+    Lrow[j] = 0.0f;
   }
-  if (fast) {
-    // back to the reference's variables: w = w', t = t' - w x c
-    x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];
-    x[0] = xp[0] - (x[4] * cz - x[5] * cy);
-    x[1] = xp[1] - (x[5] * cx - x[3] * cz);
-    x[2] = xp[2] - (x[3] * cy - x[4] * cx);
-    *guarded = 0;
-    return;
-  }
-  if (lane == 0) kf_icp_world_guarded_step(v21c, bc, c, s_scratch, s_scratch + 8);
-  __syncwarp();
+  float inv_diag = 0.0f;
+  bool spd = true;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) x[k] = s_scratch[k];
-  *guarded = 1;
-  __syncwarp();
+  for (int j = 0; j < 6; ++j) {
+    const float d = __shfl_sync(0xffffffffu, row[j], j);
+    if (!(d > 0.0f)) { spd = false; break; }  // uniform: d is broadcast
+    const float r = rsqrtf(d);
+    const float lij = lane == j ? d * r : (lane > j ? row[j] * r : 0.0f);
+    Lrow[j] = lij;
+    if (lane == j) inv_diag = r;
+#pragma unroll
+    for (int k = j + 1; k < 6; ++k) {
+      const float lkj = __shfl_sync(0xffffffffu, lij, k);
+      if (lane > j) row[k] = fmaf(-lij, lkj, row[k]);
+    }
+  }
+  if (!spd) return 0;
+  const float cx = (float)c[0], cy = (float)c[1], cz = (float)c[2];
+  // lane i < 6: u = M^-T e_i, m = M e_i: for i < 3 u = (e_i; -(c x e_i)), m = e_i; for
+  // i = 3 + k u = e_i, m = (-(c x e_k); e_k)
+  const int k3 = i < 3 ? i : i - 3;
+  const float ck0 = k3 == 0 ? 0.0f : (k3 == 1 ? -cz : cy);
+  const float ck1 = k3 == 0 ? cz : (k3 == 1 ? 0.0f : -cx);
+  const float ck2 = k3 == 0 ? -cy : (k3 == 1 ? cx : 0.0f);
+  float z[6];
+  float zz = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    float v = j == i ? 1.0f : 0.0f;
+    if (i < 3 && j >= 3) v = -(j == 3 ? ck0 : (j == 4 ? ck1 : ck2));
+#pragma unroll
+    for (int k = 0; k < j; ++k) v = fmaf(-__shfl_sync(0xffffffffu, Lrow[k], j), z[k], v);
+    z[j] = v * __shfl_sync(0xffffffffu, inv_diag, j);
+    zz = fmaf(z[j], z[j], zz);
+  }
+  float D;
+  if (i < 3) {
+    D = at(i, i);
+  } else {
+    const float m0 = -ck0, m1 = -ck1, m2 = -ck2;
+    const float r0 = at(0, 0) * m0 + at(0, 1) * m1 + at(0, 2) * m2;
+    const float r1 = at(1, 0) * m0 + at(1, 1) * m1 + at(1, 2) * m2;
+    const float r2 = at(2, 0) * m0 + at(2, 1) * m1 + at(2, 2) * m2;
+    D = m0 * r0 + m1 * r1 + m2 * r2 + 2.0f * (m0 * at(0, i) + m1 * at(1, i) + m2 * at(2, i)) + at(i, i);
+  }
+  float tinv = lane < 6 ? zz : 0.0f;  // (C^-1)_ii
+  float tr = lane < 6 ? D : 0.0f;     // C_ii
+#pragma unroll
+  for (int o = 4; o >= 1; o >>= 1) {
+    tinv += __shfl_xor_sync(0xffffffffu, tinv, o);
+    tr += __shfl_xor_sync(0xffffffffu, tr, o);
+  }
+  tinv = __shfl_sync(0xffffffffu, tinv, 0);
+  tr = __shfl_sync(0xffffffffu, tr, 0);
+  return (tinv * tr * (2.0f * (float)KF_ICP_RANK_TAU) <= 1.0f) ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------------------

@@ -325,15 +325,9 @@ class GFusion:
         self._check(self.lib.kf_set_depth_filter(self._h, int(bool(enable))), "kf_set_depth_filter")
 
     # ---- launch shapes and the autotuner -----------------------------------------------
-    def setLaunchShape(self, integrate_z_chunk: int, raycast_rows: int, icp_coarse_pixels: int = 0) -> None:
-        """icp_coarse_pixels: pixels per block at ICP levels 1, 2 (0: default 512, -1: every block)."""
-        sh = L.kf_launch_shape(int(integrate_z_chunk), int(raycast_rows), int(icp_coarse_pixels))
+    def setLaunchShape(self, integrate_z_chunk: int, raycast_rows: int) -> None:
+        sh = L.kf_launch_shape(int(integrate_z_chunk), int(raycast_rows))
         self._check(self.lib.kf_set_launch_shape(self._h, C.byref(sh)), "kf_set_launch_shape")
-
-    def icpCoarsePixels(self) -> int:
-        sh = L.kf_launch_shape()
-        self._check(self.lib.kf_get_launch_shape(self._h, C.byref(sh)), "kf_get_launch_shape")
-        return sh.icp_coarse_pixels
 
     def launchShape(self) -> tuple:
         sh = L.kf_launch_shape()

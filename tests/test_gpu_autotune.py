@@ -116,29 +116,3 @@ def test_batch_autotune_keeps_results_exact():
         for s, t in zip(batched, alone):
             _assert_same(_state(s), _state(t))
 
-
-def test_icp_coarse_level_blocks_are_bit_identical():
-    """ICP levels 1 and 2 on fewer blocks (ceil(pixels / icp_coarse_pixels)) with split-BF16
-    J^T J: the fixed-point sums of every 32-pixel chunk do not depend on the split, so every
-    setting gives the same poses, volume and maps, frame after frame."""
-    w = small_workload(6, size=96, storage=L.KF_STORAGE_F16U16, jtj=L.KF_JTJ_SPLIT_BF16,
-                       quirks=L.KF_QUIRKS_TRACKING)
-    frames = [w.frame(k) for k in range(w.n_frames)]
-    ref = None
-    for icp in (-1, 256, 512, 4096, 65536):
-        g = GFusion(w.config, w.intrinsics)
-        g.setLaunchShape(16, 4, icp)
-        assert g.icpCoarsePixels() == icp
-        g.Reset(w.poses[0])
-        tracked = [g.frameStep(f) for f in frames]
-        st = _state(g)
-        if ref is None:
-            ref = (tracked, st)
-            assert all(tracked[1:])
-        else:
-            assert tracked == ref[0]
-            _assert_same(st, ref[1])
-    g = GFusion(w.config, w.intrinsics)
-    assert g.icpCoarsePixels() == 512  # the default
-    with pytest.raises(L.KfError):
-        g.setLaunchShape(16, 4, 100)
