@@ -565,32 +565,41 @@ __device__ inline bool kf_cholesky6_warp(const double* v21, const double* b, dou
 // Cyclic Jacobi eigen-decomposition of a symmetric 6x6 matrix (row-major): A is
 // overwritten by its diagonalised form, V receives the eigenvectors in its columns.  At
 // most 32 sweeps; stops when the off-diagonal mass is below 1e-30 of the diagonal's.
-__host__ __device__ inline void kf_jacobi_eigen6(double* A, double* V) {
+__device__ inline void kf_jacobi_eigen6(double* A, double* V) {
+  #pragma unroll 1
   for (int i = 0; i < 36; ++i) V[i] = (i % 7 == 0) ? 1.0 : 0.0;
+  #pragma unroll 1
   for (int sweep = 0; sweep < 32; ++sweep) {
     double off = 0.0, diag = 0.0;
+    #pragma unroll 1
     for (int p = 0; p < 6; ++p) {
       diag += A[p * 7] * A[p * 7];
+      #pragma unroll 1
       for (int q = p + 1; q < 6; ++q) off += A[p * 6 + q] * A[p * 6 + q];
     }
     if (!(off > 1e-30 * diag)) break;
+    #pragma unroll 1
     for (int p = 0; p < 6; ++p)
+      #pragma unroll 1
       for (int q = p + 1; q < 6; ++q) {
         const double apq = A[p * 6 + q];
         if (apq == 0.0) continue;
         const double theta = (A[q * 7] - A[p * 7]) / (2.0 * apq);
         const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
         const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        #pragma unroll 1
         for (int k = 0; k < 6; ++k) {
           const double akp = A[k * 6 + p], akq = A[k * 6 + q];
           A[k * 6 + p] = c * akp - s * akq;
           A[k * 6 + q] = s * akp + c * akq;
         }
+        #pragma unroll 1
         for (int k = 0; k < 6; ++k) {
           const double apk = A[p * 6 + k], aqk = A[q * 6 + k];
           A[p * 6 + k] = c * apk - s * aqk;
           A[q * 6 + k] = s * apk + c * aqk;
         }
+        #pragma unroll 1
         for (int k = 0; k < 6; ++k) {
           const double vkp = V[k * 6 + p], vkq = V[k * 6 + q];
           V[k * 6 + p] = c * vkp - s * vkq;
@@ -602,21 +611,27 @@ __host__ __device__ inline void kf_jacobi_eigen6(double* A, double* V) {
 
 // The rank-guarded step of a world-frame system C x = b (C row-major 6x6), as described
 // at KF_ICP_RANK_TAU.  Returns the number of eigen-directions kept.
-__host__ __device__ inline int kf_icp_guarded_solve(const double* C, const double* b, double* x, double* A,
+__device__ inline int kf_icp_guarded_solve(const double* C, const double* b, double* x, double* A,
                                                     double* V) {
   // A, V: 36 doubles of scratch each
+  #pragma unroll 1
   for (int i = 0; i < 36; ++i) A[i] = C[i];
   kf_jacobi_eigen6(A, V);
   double lmax = 0.0;
+  #pragma unroll 1
   for (int k = 0; k < 6; ++k) lmax = fmax(lmax, A[k * 7]);
+  #pragma unroll 1
   for (int i = 0; i < 6; ++i) x[i] = 0.0;
   int kept = 0;
+  #pragma unroll 1
   for (int k = 0; k < 6; ++k) {
     const double l = A[k * 7];
     if (!(l > 0.0 && l >= KF_ICP_RANK_TAU * lmax)) continue;
     ++kept;
     double vb = 0.0;
+    #pragma unroll 1
     for (int i = 0; i < 6; ++i) vb += V[i * 6 + k] * b[i];
+    #pragma unroll 1
     for (int i = 0; i < 6; ++i) x[i] += V[i * 6 + k] * vb / l;
   }
   return kept;
@@ -625,7 +640,9 @@ __host__ __device__ inline int kf_icp_guarded_solve(const double* C, const doubl
 // The rank-guarded step from the centred sums about c, in the world frame: b = M^T b',
 // C = M^T C' M with M = [[I, -[c]x], [0, I]], then kf_icp_guarded_solve.  It runs only for
 // degenerate views; its matrices live in the caller's scratch sm (6 * 36 + 12 doubles,
-// shared memory), so they take no registers from the caller.
+// shared memory) and its loops are kept rolled, so that this rare path does not raise the
+// register pressure of the kernel around it (measured: unrolled, it slowed every ICP
+// iteration).
 __device__ inline void kf_icp_world_guarded_step(const double* v21c, const double* bc, const double* c, double* out,
                                                  double* sm) {
   const double cx = c[0], cy = c[1], cz = c[2];
@@ -636,29 +653,39 @@ __device__ inline void kf_icp_world_guarded_step(const double* v21c, const doubl
   double* bw = sm + 216;
   double* xw = sm + 222;
   kf_make_jtj(v21c, Cp);
+  #pragma unroll 1
   for (int k = 0; k < 36; ++k) Mx[k] = (k % 7 == 0) ? 1.0 : 0.0;
   // -[c]x in rows 0..2, columns 3..5
   Mx[0 * 6 + 4] = cz;  Mx[0 * 6 + 5] = -cy;
   Mx[1 * 6 + 3] = -cz; Mx[1 * 6 + 5] = cx;
   Mx[2 * 6 + 3] = cy;  Mx[2 * 6 + 4] = -cx;
+  #pragma unroll 1
   for (int r = 0; r < 6; ++r) {
     double v = 0.0;
+    #pragma unroll 1
     for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * bc[k];
     bw[r] = v;
   }
+  #pragma unroll 1
   for (int r = 0; r < 6; ++r)
+    #pragma unroll 1
     for (int cc = 0; cc < 6; ++cc) {
       double v = 0.0;
+      #pragma unroll 1
       for (int k = 0; k < 6; ++k) v += Cp[r * 6 + k] * Mx[k * 6 + cc];
       T[r * 6 + cc] = v;
     }
+  #pragma unroll 1
   for (int r = 0; r < 6; ++r)
+    #pragma unroll 1
     for (int cc = 0; cc < 6; ++cc) {
       double v = 0.0;
+      #pragma unroll 1
       for (int k = 0; k < 6; ++k) v += Mx[k * 6 + r] * T[k * 6 + cc];
       Cw[r * 6 + cc] = v;
     }
   kf_icp_guarded_solve(Cw, bw, xw, sm + 144, sm + 180);
+  #pragma unroll 1
   for (int k = 0; k < 6; ++k) out[k] = xw[k];
 }
 
