@@ -40,6 +40,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes instead of autotuning them during warm-up")
+    p.add_argument("--launch-shape", default=None, metavar="ZC,ROWS",
+                   help="fix the plain form's launch shapes (integrate z-chunk, raycast tile rows; "
+                        "rows 1 = persistent sweep) instead of autotuning them")
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--size", type=int, default=512)
     p.add_argument("--storage", choices=["f16u16", "f32f32", "rg16i"], default="f16u16")
@@ -658,6 +661,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     # after the autotuner (at the first warm-up frame) four frames capture the ring of frame
     # graphs, so at least five warm-up frames
+    fixed = tuple(int(x) for x in args.launch_shape.split(",")) if args.launch_shape else None
+    if fixed:
+        args.no_autotune = True
     K, W = args.steps, max(3 if args.no_autotune else 5, args.warmup)
     n_e2e = 0 if args.no_e2e else K
     n_lat = 0 if args.no_e2e else max(K, 50)
@@ -679,6 +685,8 @@ def main():
 
     g = GFusion(w.config, w.intrinsics)
     g.Reset(w.poses[0])
+    if fixed:
+        g.setLaunchShape(*fixed)
     log("session created")
     mc = MCubes(g)
     stream = torch.cuda.ExternalStream(g.stream())
@@ -805,7 +813,8 @@ def main():
             "config": {**plain_config(w, args, world),
                        "l2": "volume > L2 (126 MB); inputs resident",
                        "mc_calls": mc_calls, "mc_ms_mean": (float(np.mean(mc_ms)) if mc_ms else None),
-                       "launch_shape": tuned or {"integrate_z_chunk": 16, "raycast_rows": 4, "autotune": "off"}},
+                       "launch_shape": tuned or {"integrate_z_chunk": (fixed or (16, 4))[0],
+                                                 "raycast_rows": (fixed or (16, 4))[1], "autotune": "off"}},
             "stage_ms": per, "stage_frames": stage_frames,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak if achieved else None),
