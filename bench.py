@@ -248,14 +248,16 @@ def tsdf_error(raw_gpu, raw_oracle, cfg):
             "unit": "TSDF value (fraction of mu)"}
 
 
-def accuracy_pass(w, base, fbytes, n_steps, prefix, final_pose_ref):
+def accuracy_pass(w, base, fbytes, n_steps, prefix, final_pose_ref, shape):
     """A second session steps frames 0 .. n_steps-1 from the first ground-truth pose, one
-    synchronous frame at a time (every computation is deterministic, so it retraces the timed
-    session: its pose after the last frame is compared with the timed session's, bit for
-    bit).  Returns its per-frame poses and its raw volume after `prefix` frames."""
+    synchronous frame at a time, with the timed session's launch shapes (every computation
+    is deterministic, so it retraces the timed session: its pose after the last frame is
+    compared with the timed session's, bit for bit).  Returns its per-frame poses and its
+    raw volume after `prefix` frames."""
     from oglfusionkinectv2_b200 import GFusion
     ga = GFusion(w.config, w.intrinsics)
     ga.Reset(w.poses[0])
+    ga.setLaunchShape(*shape)
     poses, vol_prefix = [], None
     for i in range(n_steps):
         ga.frameStepDevice(base + i * fbytes)
@@ -856,7 +858,7 @@ def main():
         acc_poses = vol_prefix = None
         try:
             log("accuracy pass")
-            acc_poses, vol_prefix, same = accuracy_pass(w, base, fbytes, W + K, prefix, pose_timed_last)
+            acc_poses, vol_prefix, same = accuracy_pass(w, base, fbytes, W + K, prefix, pose_timed_last, g.launchShape())
             acc["ate_vs_ground_truth_mm"] = {
                 "timed_frames": 1000 * rmse_translation(acc_poses[W:W + K], w.poses[W:W + K]),
                 "all_frames_to_timed_end": 1000 * rmse_translation(acc_poses, w.poses[:W + K]),
