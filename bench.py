@@ -33,6 +33,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 
+TUNE_FRAME = 15  # the warm-up frame after which the plain form autotunes its launch shapes
+PLAIN_WARM = 5  # untimed single-session frames (the ring of frame graphs is captured) before a plain pass
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -283,7 +287,7 @@ def run_batched(args, sub=False):
     from oglfusionkinectv2_b200 import GFusion, GFusionBatch, synth
     K, W = (20, 5) if sub else (args.steps, max(3, args.warmup))
     K_plain = min(K, 20)
-    n_frames = W + K + 2 + K_plain
+    n_frames = W + K + PLAIN_WARM + K_plain
     ws = synth.batched_c3(args.sessions, n_frames=n_frames)
     torch.cuda.set_device(0)
     log(f"rendering {len(ws)} x {n_frames} frames on the device")
@@ -334,14 +338,14 @@ def run_batched(args, sub=False):
         collect(t_prev)
         wall = time.perf_counter() - t0
     launches = batch.launchCount() - launches0
-    # the plain path: the same sessions, one frame step at a time (two untimed frames build
-    # each session's frame graphs)
-    for i in range(W + K, W + K + 2):
+    # the plain path: the same sessions, one frame step at a time (PLAIN_WARM untimed frames
+    # capture each session's ring of frame graphs)
+    for i in range(W + K, W + K + PLAIN_WARM):
         for j, g in enumerate(gs):
             g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
             est[j].append(g.getPose())
     tp = time.perf_counter()
-    for i in range(W + K + 2, W + K + 2 + K_plain):
+    for i in range(W + K + PLAIN_WARM, W + K + PLAIN_WARM + K_plain):
         for j, g in enumerate(gs):
             g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
     plain_wall = time.perf_counter() - tp
@@ -355,11 +359,12 @@ def run_batched(args, sub=False):
         g = GFusion(c32, w.intrinsics)
         g.Reset(w.poses[0])
         g32.append(g)
-    for i in range(W):
+    W32 = max(W, PLAIN_WARM)
+    for i in range(W32):
         for j, g in enumerate(g32):
             g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
     tq = time.perf_counter()
-    for i in range(W, W + K_plain):
+    for i in range(W32, W32 + K_plain):
         for j, g in enumerate(g32):
             g.frameStepDevice(frames[j].data_ptr() + i * fbytes)
     plain32_wall = time.perf_counter() - tq
@@ -661,12 +666,14 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    # after the autotuner (at the first warm-up frame) four frames capture the ring of frame
-    # graphs, so at least five warm-up frames
+    # the autotuner times its candidates after warm-up frame TUNE_FRAME, on a volume that has
+    # fused several views (after the first frame it holds one view's thin shell, on which the
+    # raycast's tile shapes rank differently); four more frames then capture the ring of
+    # frame graphs
     fixed = tuple(int(x) for x in args.launch_shape.split(",")) if args.launch_shape else None
     if fixed:
         args.no_autotune = True
-    K, W = args.steps, max(3 if args.no_autotune else 5, args.warmup)
+    K, W = args.steps, max(3 if args.no_autotune else TUNE_FRAME + 5, args.warmup)
     n_e2e = 0 if args.no_e2e else K
     n_lat = 0 if args.no_e2e else max(K, 50)
     n_frames = W + K + n_e2e + 1 + n_lat
@@ -709,7 +716,7 @@ def main():
     tuned = None
     for i in range(W):
         g.frameStepDevice(base + i * fbytes, sync=False)
-        if i == 0 and not args.no_autotune:
+        if i == TUNE_FRAME and not args.no_autotune:
             # brick and tile shapes for this volume and frame (scratch copies; the session is
             # untouched); the following warm-up frames capture the frame graphs with them
             shape, tms = g.autotune(repeats=5)
@@ -846,7 +853,7 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_reference_quirks:
         try:
-            out["reference_quirks"] = reference_quirks_pass(w, base, fbytes, W, K)
+            out["reference_quirks"] = reference_quirks_pass(w, base, fbytes, W, K, g.launchShape())
         except Exception as e:  # noqa: BLE001
             out["reference_quirks"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1:
@@ -900,15 +907,17 @@ def main():
     return 0
 
 
-def reference_quirks_pass(w, base, fbytes, W, K):
+def reference_quirks_pass(w, base, fbytes, W, K, shape):
     """The same frames with the reference's own behaviour (every quirk bit set: same-pixel
-    ICP association and the narrow TSDF band among them), timed like the main pass."""
+    ICP association and the narrow TSDF band among them), timed like the main pass, with
+    its launch shapes."""
     import torch
     from oglfusionkinectv2_b200 import GFusion, _lib as L
     c = w.config
     cq = type(c)(**{**c.__dict__, "quirks": L.KF_QUIRKS_REFERENCE})
     g = GFusion(cq, w.intrinsics)
     g.Reset(w.poses[0])
+    g.setLaunchShape(*shape)
     for i in range(W):
         g.frameStepDevice(base + i * fbytes, sync=False)
     torch.cuda.synchronize()

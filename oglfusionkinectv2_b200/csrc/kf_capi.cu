@@ -1259,9 +1259,20 @@ int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* time
   if (rc) return rc;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(s, KF_ERR_CUDA, "autotune events");
-  // each candidate: one untimed launch, then `repeats` launches between two events; two
-  // rounds over all candidates, the better mean kept (clock and cache drift even out)
+  // each candidate: one untimed launch, then `repeats` timed launches; two rounds over all
+  // candidates, the better mean kept (clock and cache drift even out).  Integrate
+  // candidates run back to back (in the frame loop only ICP, which touches a few MB, runs
+  // between two integrates); each raycast candidate launch follows an untimed integrate,
+  // as in the frame loop, whose volume traffic leaves L2 as a frame's raycast finds it
+  // (raycasts back to back would find the previous one's bricks in L2 and favour other
+  // shapes).
   float best[7] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+  auto elapsed = [&](float* ms) {
+    if (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(ms, e0, e1) != cudaSuccess)
+      return fail(s, KF_ERR_CUDA, "autotune timing failed");
+    return (int)KF_OK;
+  };
   for (int round = 0; round < 2 && !rc; ++round)
     for (int c = 0; c < 7 && !rc; ++c) {
       const bool ray = c >= 3;
@@ -1270,16 +1281,22 @@ int kf_autotune(kf_session* s, int repeats, kf_launch_shape* chosen, float* time
         return ray ? kf_launch_raycast_shape(s, v, &t) : kf_launch_integrate_shape(s, 0, v, &t);
       };
       if ((rc = launch())) break;
-      if (cudaEventRecord(e0, s->stream) != cudaSuccess) { rc = fail(s, KF_ERR_CUDA, "autotune timing failed"); break; }
-      for (int r = 0; r < repeats && !rc; ++r) rc = launch();
-      if (rc) break;
-      float ms = 0.0f;
-      if (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-        rc = fail(s, KF_ERR_CUDA, "autotune timing failed");
-        break;
+      float total = 0.0f;
+      if (!ray) {
+        if (cudaEventRecord(e0, s->stream) != cudaSuccess) { rc = fail(s, KF_ERR_CUDA, "autotune timing failed"); break; }
+        for (int r = 0; r < repeats && !rc; ++r) rc = launch();
+        if (rc || (rc = elapsed(&total))) break;
+      } else {
+        for (int r = 0; r < repeats && !rc; ++r) {
+          if ((rc = kf_launch_integrate_shape(s, 0, s->int_zc, &t))) break;
+          if (cudaEventRecord(e0, s->stream) != cudaSuccess) { rc = fail(s, KF_ERR_CUDA, "autotune timing failed"); break; }
+          float ms = 0.0f;
+          if ((rc = launch()) || (rc = elapsed(&ms))) break;
+          total += ms;
+        }
+        if (rc) break;
       }
-      best[c] = std::min(best[c], ms / (float)repeats);
+      best[c] = std::min(best[c], total / (float)repeats);
     }
   cudaStreamSynchronize(s->stream);
   if (e0) cudaEventDestroy(e0);

@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
   __shared__ double s_sums[32];
   __shared__ double s_csums[29], s_ccenter[3], s_ae;  // last centred row (for the tail)
   __shared__ double s_nvalid;                           // its valid-pixel count
-  __shared__ double s_gx[8 + 228];                      // the rank-guarded step (rare path)
+  __shared__ double s_gx[8 + 228];                      // the step (+ rank guard's scratch)
   __shared__ int s_fast;                                // the rank check's verdict
   __shared__ int s_flag, s_conv;
   __shared__ __align__(16) __nv_bfloat16 s_hi[JTJ ? kWarps : 1][8][40];
@@ -441,8 +441,19 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
         const double count = a.q1 ? (double)Wl * (double)(Hl / 8) : (double)P;
         const double nvalid = s_sums[28];
         const double cx = s_cd[0], cy = s_cd[1], cz = s_cd[2];
+        // lane 0 factors and solves; the step reaches the other lanes through shared memory
         double xp[6];
-        const bool spd = kf_cholesky6_warp(&s_sums[7], &s_sums[1], xp, lane);
+        bool spd = false;
+        if (lane == 0) {
+          spd = kf_cholesky6_thread(&s_sums[7], &s_sums[1], xp);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) s_gx[k] = xp[k];
+          s_gx[6] = spd ? 1.0 : 0.0;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 6; ++k) xp[k] = s_gx[k];
+        spd = s_gx[6] != 0.0;
         // back to the reference's variables: w = w', t = t' - w x c
         double x[6];
         x[3] = xp[3]; x[4] = xp[4]; x[5] = xp[5];

@@ -479,76 +479,58 @@ __device__ __forceinline__ void kf_sincos_step(double x, double* s, double* c) {
   }
 }
 
-// kf_cholesky6 for one warp: C given as the 21 upper-triangular values of reduce.cs rows
-// 7..27 (row-major), b as 6 values, both in shared or global memory read by every lane.
-// Lane i < 6 factors row i; every lane returns the whole solution in x (zero when C is
-// not numerically positive definite, as kf_cholesky6) and whether C was; lane i < 6 also
-// returns row i of the factor L in Lrow_out (entries 0..i) and 1 / L_ii in *inv_diag_out.
-// The pivots' reciprocals come from kf_rsqrt_newton, so the dependent chain holds
-// multiplies and shuffles, no divides.
-__device__ inline bool kf_cholesky6_warp(const double* v21, const double* b, double* x, int lane,
-                                         double* Lrow_out = nullptr, double* inv_diag_out = nullptr) {
-  auto at = [&](int i, int j) {
-    if (i > j) { const int t = i; i = j; j = t; }
-    return v21[6 * i - (i * (i - 1)) / 2 + (j - i)];
-  };
-  const int i = lane < 6 ? lane : 5;
-  double row[6], Lrow[6], Lcol[6];
-  double dmax = 0.0, inv_diag = 0.0;  // inv_diag: 1 / L_ii of this lane's row
+// kf_cholesky6 by one thread: C given as the 21 upper-triangular values of reduce.cs rows
+// 7..27 (row-major), b as 6 values, both read from shared or global memory.  Returns
+// whether C was numerically positive definite (x = 0 otherwise, as kf_cholesky6).  Fully
+// unrolled in registers: the dependent chain is six pivots (kf_rsqrt_newton: multiplies,
+// no divides) and twelve substitution steps, with no shuffles between lanes (measured
+// 11 us per frame faster than a lane-per-row warp factorisation, whose every pivot and
+// substitution step waited on a shuffle).
+__device__ __forceinline__ bool kf_cholesky6_thread(const double* v21, const double* b, double* x) {
+  double L[6][6];  // lower triangle
+  double inv[6];
+  double dmax = 0.0;
 #pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    row[j] = at(i, j);
-    Lrow[j] = 0.0;
-    Lcol[j] = 0.0;
-    dmax = fmax(dmax, fabs(at(j, j)));
-  }
+  for (int i = 0; i < 6; ++i) dmax = fmax(dmax, fabs(v21[6 * i - (i * (i - 1)) / 2]));
   const double eps = 1e-13 * dmax;
   bool spd = true;
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
-    const double d = __shfl_sync(0xffffffffu, row[j], j);  // C_jj - sum_k L_jk^2
-    if (!(d > eps)) { spd = false; break; }                 // uniform: d is broadcast
-    const double r = kf_rsqrt_newton(d);                    // 1 / L_jj
-    const double lij = lane == j ? d * r : (lane > j ? row[j] * r : 0.0);
-    Lrow[j] = lij;
-    if (lane == j) {
-      Lcol[j] = lij;
-      inv_diag = r;
-    }
+    double dj = v21[6 * j - (j * (j - 1)) / 2];
 #pragma unroll
-    for (int k = j + 1; k < 6; ++k) {
-      const double lkj = __shfl_sync(0xffffffffu, lij, k);
-      if (lane > j) row[k] = fma(-lij, lkj, row[k]);
-      if (lane == j) Lcol[k] = lkj;
+    for (int k = 0; k < j; ++k) dj = fma(-L[j][k], L[j][k], dj);
+    spd = spd && (dj > eps);
+    const double r = kf_rsqrt_newton(spd ? dj : 1.0);
+    inv[j] = r;
+    L[j][j] = dj * r;
+#pragma unroll
+    for (int i = j + 1; i < 6; ++i) {
+      double v = v21[6 * j - (j * (j - 1)) / 2 + (i - j)];
+#pragma unroll
+      for (int k = 0; k < j; ++k) v = fma(-L[i][k], L[j][k], v);
+      L[i][j] = v * r;
     }
   }
-  if (Lrow_out) {
+  double y[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) Lrow_out[k] = Lrow[k];
-    *inv_diag_out = inv_diag;
+  for (int i = 0; i < 6; ++i) {
+    double v = b[i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) v = fma(-L[i][k], y[k], v);
+    y[i] = v * inv[i];
+  }
+#pragma unroll
+  for (int i = 5; i >= 0; --i) {
+    double v = y[i];
+#pragma unroll
+    for (int k = i + 1; k < 6; ++k) v = fma(-L[k][i], x[k], v);
+    x[i] = spd ? v * inv[i] : 0.0;
   }
   if (!spd) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) x[k] = 0.0;
-    return false;
+    for (int i = 0; i < 6; ++i) x[i] = 0.0;
   }
-  // L y = b, then L^T x = y
-  double y = b[i];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    if (lane == k) y = y * inv_diag;
-    const double yk = __shfl_sync(0xffffffffu, y, k);
-    if (lane > k) y = fma(-Lrow[k], yk, y);
-  }
-#pragma unroll
-  for (int k = 5; k >= 0; --k) {
-    if (lane == k) y = y * inv_diag;
-    const double xk = __shfl_sync(0xffffffffu, y, k);
-    if (lane < k) y = fma(-Lcol[k], xk, y);
-  }
-#pragma unroll
-  for (int k = 0; k < 6; ++k) x[k] = __shfl_sync(0xffffffffu, y, k);
-  return true;
+  return spd;
 }
 
 // ---------------------------------------------------------------------------------------

@@ -287,8 +287,19 @@ __global__ void __launch_bounds__(32 * ROWS) raycast_kernel(RayArgs one, const R
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.y == 1 && threadIdx.x < 16)
     a.st_out->raycast_pose[threadIdx.x] = a.st->pose[threadIdx.x];
   __syncthreads();
-  const int x = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  // each warp takes a compact patch of the 32 x ROWS tile (16 x 2 pixels in 2-row tiles,
+  // 8 x 4 otherwise): neighbouring rays march through the same bricks and end at similar
+  // depths, so a warp's taps share cache lines and its lanes finish together (measured
+  // ~1 % faster than a 32 x 1 row per warp)
+  const int t = threadIdx.y * 32 + threadIdx.x, w = t >> 5, l = t & 31;
+  int x, y;
+  if constexpr (ROWS == 2) {
+    x = blockIdx.x * 32 + w * 16 + (l & 15);
+    y = blockIdx.y * 2 + (l >> 4);
+  } else {
+    x = blockIdx.x * 32 + (w & 3) * 8 + (l & 7);
+    y = blockIdx.y * ROWS + (w >> 2) * 4 + (l >> 3);
+  }
   if (x >= a.W || y >= a.H) return;
   raycast_pixel<S>(a, s_view, x, y);
 }
