@@ -671,8 +671,10 @@ __device__ inline void kf_icp_world_guarded_step(const double* v21c, const doubl
   for (int k = 0; k < 6; ++k) out[k] = xw[k];
 }
 
-// The rank guard's check for one warp, in FP32 (run beside the FP64 solve, off its
-// critical path): 1 when the world-frame C provably keeps every direction under
+
+
+// The rank guard's check by one thread, in FP32 (run in warp 1 beside warp 0's FP64
+// solve): 1 when the world-frame C provably keeps every direction under
 // KF_ICP_RANK_TAU, so that the centred system's Cholesky solution is the guarded step.
 // v21c: reduce.cs rows 7..27 of the centred J' = [n, (p - c) x n] about c, i.e.
 // C' = M^-T C M^-1 with M: t' = t - [c]x w.  Bounds: l_min >= 1 / trace(C^-1),
@@ -681,72 +683,64 @@ __device__ inline void kf_icp_world_guarded_step(const double* v21c, const doubl
 // the cut is 1e-5, far above FP32's 6e-8, and a Cholesky too ill-conditioned for FP32 gives
 // a large trace (or a non-positive pivot) and fails the check, leaving the decision to the
 // exact FP64 path.
-__device__ inline int kf_icp_rank_check_warp(const double* v21c, const double* c, int lane) {
-  auto at = [&](int i, int j) {
-    if (i > j) { const int t = i; i = j; j = t; }
-    return (float)v21c[6 * i - (i * (i - 1)) / 2 + (j - i)];
-  };
-  const int i = lane < 6 ? lane : 5;
-  float row[6], Lrow[6];
+__device__ __forceinline__ int kf_icp_rank_check_thread(const double* v21c, const double* c) {
+  float A[6][6];
 #pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    row[j] = at(i, j);
-    Lrow[j] = 0.0f;
-  }
-  float inv_diag = 0.0f;
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = i; j < 6; ++j) {
+      A[i][j] = (float)v21c[6 * i - (i * (i - 1)) / 2 + (j - i)];
+      A[j][i] = A[i][j];
+    }
+  float L[6][6], id[6];
   bool spd = true;
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
-    const float d = __shfl_sync(0xffffffffu, row[j], j);
-    if (!(d > 0.0f)) { spd = false; break; }  // uniform: d is broadcast
-    const float r = rsqrtf(d);
-    const float lij = lane == j ? d * r : (lane > j ? row[j] * r : 0.0f);
-    Lrow[j] = lij;
-    if (lane == j) inv_diag = r;
+    float dj = A[j][j];
 #pragma unroll
-    for (int k = j + 1; k < 6; ++k) {
-      const float lkj = __shfl_sync(0xffffffffu, lij, k);
-      if (lane > j) row[k] = fmaf(-lij, lkj, row[k]);
+    for (int k = 0; k < j; ++k) dj = fmaf(-L[j][k], L[j][k], dj);
+    spd = spd && (dj > 0.0f);
+    const float r = rsqrtf(spd ? dj : 1.0f);
+    id[j] = r;
+    L[j][j] = dj * r;
+#pragma unroll
+    for (int i = j + 1; i < 6; ++i) {
+      float v = A[i][j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) v = fmaf(-L[i][k], L[j][k], v);
+      L[i][j] = v * r;
     }
   }
   if (!spd) return 0;
   const float cx = (float)c[0], cy = (float)c[1], cz = (float)c[2];
-  // lane i < 6: u = M^-T e_i, m = M e_i: for i < 3 u = (e_i; -(c x e_i)), m = e_i; for
-  // i = 3 + k u = e_i, m = (-(c x e_k); e_k)
-  const int k3 = i < 3 ? i : i - 3;
-  const float ck0 = k3 == 0 ? 0.0f : (k3 == 1 ? -cz : cy);
-  const float ck1 = k3 == 0 ? cz : (k3 == 1 ? 0.0f : -cx);
-  const float ck2 = k3 == 0 ? -cy : (k3 == 1 ? cx : 0.0f);
-  float z[6];
-  float zz = 0.0f;
+  float tinv = 0.0f, tr = 0.0f;
 #pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    float v = j == i ? 1.0f : 0.0f;
-    if (i < 3 && j >= 3) v = -(j == 3 ? ck0 : (j == 4 ? ck1 : ck2));
+  for (int i = 0; i < 6; ++i) {
+    const int k3 = i < 3 ? i : i - 3;
+    // c x e_k3
+    const float ck0 = k3 == 0 ? 0.0f : (k3 == 1 ? -cz : cy);
+    const float ck1 = k3 == 0 ? cz : (k3 == 1 ? 0.0f : -cx);
+    const float ck2 = k3 == 0 ? -cy : (k3 == 1 ? cx : 0.0f);
+    float z[6];
 #pragma unroll
-    for (int k = 0; k < j; ++k) v = fmaf(-__shfl_sync(0xffffffffu, Lrow[k], j), z[k], v);
-    z[j] = v * __shfl_sync(0xffffffffu, inv_diag, j);
-    zz = fmaf(z[j], z[j], zz);
-  }
-  float D;
-  if (i < 3) {
-    D = at(i, i);
-  } else {
-    const float m0 = -ck0, m1 = -ck1, m2 = -ck2;
-    const float r0 = at(0, 0) * m0 + at(0, 1) * m1 + at(0, 2) * m2;
-    const float r1 = at(1, 0) * m0 + at(1, 1) * m1 + at(1, 2) * m2;
-    const float r2 = at(2, 0) * m0 + at(2, 1) * m1 + at(2, 2) * m2;
-    D = m0 * r0 + m1 * r1 + m2 * r2 + 2.0f * (m0 * at(0, i) + m1 * at(1, i) + m2 * at(2, i)) + at(i, i);
-  }
-  float tinv = lane < 6 ? zz : 0.0f;  // (C^-1)_ii
-  float tr = lane < 6 ? D : 0.0f;     // C_ii
+    for (int j = 0; j < 6; ++j) {
+      float v = j == i ? 1.0f : 0.0f;
+      if (i < 3 && j >= 3) v = -(j == 3 ? ck0 : (j == 4 ? ck1 : ck2));
 #pragma unroll
-  for (int o = 4; o >= 1; o >>= 1) {
-    tinv += __shfl_xor_sync(0xffffffffu, tinv, o);
-    tr += __shfl_xor_sync(0xffffffffu, tr, o);
+      for (int k = 0; k < j; ++k) v = fmaf(-L[j][k], z[k], v);
+      z[j] = v * id[j];
+      tinv = fmaf(z[j], z[j], tinv);
+    }
+    if (i < 3) {
+      tr += A[i][i];
+    } else {
+      const float m0 = -ck0, m1 = -ck1, m2 = -ck2;
+      const float r0 = A[0][0] * m0 + A[0][1] * m1 + A[0][2] * m2;
+      const float r1 = A[1][0] * m0 + A[1][1] * m1 + A[1][2] * m2;
+      const float r2 = A[2][0] * m0 + A[2][1] * m1 + A[2][2] * m2;
+      tr += m0 * r0 + m1 * r1 + m2 * r2 + 2.0f * (m0 * A[0][i] + m1 * A[1][i] + m2 * A[2][i]) + A[i][i];
+    }
   }
-  tinv = __shfl_sync(0xffffffffu, tinv, 0);
-  tr = __shfl_sync(0xffffffffu, tr, 0);
   return (tinv * tr * (2.0f * (float)KF_ICP_RANK_TAU) <= 1.0f) ? 1 : 0;
 }
 
