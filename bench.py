@@ -48,6 +48,9 @@ def parse():
                    help="fix the plain form's launch shapes (integrate z-chunk, raycast tile rows; "
                         "rows 1 = persistent sweep) instead of autotuning them")
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["c2", "c1"], default="c2",
+                   help="plain form's workload: c2 = the 512^3 precision form (default line); "
+                        "c1 = the 128^3 FP32 plain form (storage and J^T J from the workload)")
     p.add_argument("--size", type=int, default=512)
     p.add_argument("--storage", choices=["f16u16", "f32f32", "rg16i"], default="f16u16")
     p.add_argument("--jtj", choices=["bf16", "fp32"], default="bf16")
@@ -69,15 +72,20 @@ def parse():
 
 def workload(args, n_frames):
     from oglfusionkinectv2_b200 import synth, _lib as L
+    if getattr(args, "workload", "c2") == "c1":
+        return synth.plain_c1(n_frames=n_frames)
     storage = {"f16u16": L.KF_STORAGE_F16U16, "f32f32": L.KF_STORAGE_F32F32, "rg16i": L.KF_STORAGE_RG16I}[args.storage]
     jtj = L.KF_JTJ_SPLIT_BF16 if args.jtj == "bf16" else L.KF_JTJ_FP32
     return synth.precision_c2(n_frames=n_frames, storage=storage, jtj=jtj, size=args.size)
 
 
 def _gen(args_tuple):
-    size, storage, jtj, n, idx = args_tuple
+    name, size, storage, jtj, n, idx = args_tuple
     from oglfusionkinectv2_b200 import synth
-    w = synth.precision_c2(n_frames=n, storage=storage, jtj=jtj, size=size)
+    if name.startswith("c1"):
+        w = synth.plain_c1(n_frames=n)
+    else:
+        w = synth.precision_c2(n_frames=n, storage=storage, jtj=jtj, size=size)
     return idx, w.frame(idx)
 
 
@@ -85,7 +93,7 @@ def gen_frames(w, indices, procs):
     """Render frames in a spawn pool (started before any CUDA call)."""
     import multiprocessing as mp
     c = w.config
-    jobs = [(c.volumeSize[0], c.storage, c.jtj, w.n_frames, i) for i in indices]
+    jobs = [(w.name, c.volumeSize[0], c.storage, c.jtj, w.n_frames, i) for i in indices]
     if procs <= 1 or len(jobs) < 4:
         return {i: w.frame(i) for i in indices}
     ctx = mp.get_context("spawn")
@@ -590,10 +598,18 @@ def splitmix(x: int) -> int:
 PLAIN_METRIC = "frames/s at 512^3 TSDF (single session, plain frame step)"
 
 
+def plain_metric(w):
+    n = w.config.volumeSize[0]
+    return PLAIN_METRIC if n == 512 else PLAIN_METRIC.replace("512^3", f"{n}^3")
+
+
 def plain_config(w, args, world):
     """The workload description both arms report for the plain line."""
-    return {"workload": w.name, "volume": list(w.config.volumeSize), "dim_m": 3.0,
-            "storage": args.storage, "jtj": args.jtj, "solve": "f64 cholesky",
+    from oglfusionkinectv2_b200 import _lib as L
+    storage = {L.KF_STORAGE_F16U16: "f16u16", L.KF_STORAGE_F32F32: "f32f32", L.KF_STORAGE_RG16I: "rg16i"}[w.config.storage]
+    jtj = "bf16" if w.config.jtj == L.KF_JTJ_SPLIT_BF16 else "fp32"
+    return {"workload": w.name, "volume": list(w.config.volumeSize), "dim_m": float(w.config.volumeDimensions[0]),
+            "storage": storage, "jtj": jtj, "solve": "f64 cholesky",
             "depth": "512x424 uint16", "icp_iterations": [10, 5, 4],
             "quirks": hex(w.config.quirks), "parallelism": f"replicas x{world}", "mc_every": w.mc_every}
 
@@ -636,7 +652,7 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     v = steps / dt
     cores = O.Oracle.threads()
-    line = {"impl": "reference", "metric": PLAIN_METRIC, "value": v,
+    line = {"impl": "reference", "metric": plain_metric(w), "value": v,
             "unit": "frames/s", "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": 1000 * dt / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -815,7 +831,7 @@ def main():
         achieved = algo / (per[dom] / 1000.0) / 1e9 if per[dom] > 0 else None
         traffic = measured_traffic(w.name, dom)
         out = {
-            "metric": PLAIN_METRIC,
+            "metric": plain_metric(w),
             "value": value, "unit": "frames/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": dev_ms_max / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -849,11 +865,12 @@ def main():
                           "api": "kf_frame_step_u16_async from pinned host frames, each call reading "
                                  "the previous frame's pose and flags",
                           "latency_ms": e2e["latency_ms"]}
+    shape_used = g.launchShape()  # the timed session's launch shapes, for the passes below
     g.close()
 
     if rank == 0 and world == 1 and not args.no_reference_quirks:
         try:
-            out["reference_quirks"] = reference_quirks_pass(w, base, fbytes, W, K, g.launchShape())
+            out["reference_quirks"] = reference_quirks_pass(w, base, fbytes, W, K, shape_used)
         except Exception as e:  # noqa: BLE001
             out["reference_quirks"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1:
@@ -865,7 +882,7 @@ def main():
         acc_poses = vol_prefix = None
         try:
             log("accuracy pass")
-            acc_poses, vol_prefix, same = accuracy_pass(w, base, fbytes, W + K, prefix, pose_timed_last, g.launchShape())
+            acc_poses, vol_prefix, same = accuracy_pass(w, base, fbytes, W + K, prefix, pose_timed_last, shape_used)
             acc["ate_vs_ground_truth_mm"] = {
                 "timed_frames": 1000 * rmse_translation(acc_poses[W:W + K], w.poses[W:W + K]),
                 "all_frames_to_timed_end": 1000 * rmse_translation(acc_poses, w.poses[:W + K]),
