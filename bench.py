@@ -777,6 +777,7 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        g.resetStageStats()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         t0 = time.perf_counter()
@@ -801,7 +802,10 @@ def main():
         e2e_poses.append(np.array(pose[:]).reshape(4, 4, order="F"))
         e2e_ms = e0.elapsed_time(e1)
         log(f"e2e pass {e2e_ms:.1f} ms")
-        e2e = {"ms": e2e_ms, "wall_s": wall}
+        # the device's own stage times over the same frames: what the end-to-end rate adds
+        # to them is host and copy time
+        e2e_stage, _ = g.stageStats()
+        e2e = {"ms": e2e_ms, "wall_s": wall, "device_ms": float(np.sum(e2e_stage[:5]))}
 
         # frame latency: synchronous steps from pinned host frames, the host clock from the
         # call to the frame's pose on the host (the session continues the same sequence)
@@ -864,7 +868,8 @@ def main():
                           "wall_frames_per_s": n_e2e / e2e["wall_s"],
                           "api": "kf_frame_step_u16_async from pinned host frames, each call reading "
                                  "the previous frame's pose and flags",
-                          "latency_ms": e2e["latency_ms"]}
+                          "latency_ms": e2e["latency_ms"],
+                          "device_stage_ms_per_frame": e2e["device_ms"]}
     shape_used = g.launchShape()  # the timed session's launch shapes, for the passes below
     g.close()
 

@@ -650,14 +650,14 @@ cudaLaunchConfig_t coop_config(dim3 grid, cudaStream_t stream, cudaLaunchAttribu
 
 }  // namespace
 
-int kf_launch_icp(kf_session* s, int frame_policy) {
+int kf_launch_icp(kf_session* s, int frame_policy, bool words_zero) {
   const IcpArgs a = make_icp_args(s, frame_policy);
   const void* fn = (s->cfg.jtj == KF_JTJ_SPLIT_BF16) ? (const void*)icp_kernel<1, false>
                                                       : (const void*)icp_kernel<0, false>;
   int blocks = kf_occupancy_blocks(s, fn, KF_TRACK_THREADS, 0);
   if (blocks <= 0) return KF_ERR_CUDA;
   // the barrier counter and the sum buffers start at zero for every launch
-  KF_CUDA_TRY(s, kf_clear_icp_words(s->d_state, s->stream));
+  if (!words_zero) KF_CUDA_TRY(s, kf_clear_icp_words(s->d_state, s->stream));
   cudaLaunchAttribute attr[1];
   cudaLaunchConfig_t cfg = coop_config(dim3(blocks), s->stream, attr);
   const IcpBatch none = {nullptr, nullptr};

@@ -918,9 +918,11 @@ int kf_launch_depth_ingest(kf_session* s, const uint16_t* d_u16, const float* d_
 int kf_launch_undistort_map(kf_session* s, const kf_ir_camera& ir);
 int kf_launch_vertex(kf_session* s);
 int kf_launch_normal(kf_session* s);
-int kf_launch_vertex_normal(kf_session* s);
-int kf_launch_icp(kf_session* s, int frame_policy);
-int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy);
+// clear_tracking_words: also zero the barrier counters and ICP sums (frame step)
+int kf_launch_vertex_normal(kf_session* s, bool clear_tracking_words = false);
+// words_zero: the barrier counter and sum buffers are known to be zero (no memset)
+int kf_launch_icp(kf_session* s, int frame_policy, bool words_zero = false);
+int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy, bool counter_zero = false);
 int kf_launch_sdf_policy(kf_session* s);
 int kf_launch_integrate(kf_session* s, int gated);
 int kf_launch_raycast(kf_session* s);

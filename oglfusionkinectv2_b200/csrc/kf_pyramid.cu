@@ -72,6 +72,9 @@ struct VNArgs {
   float mcx[3], mcy[3];     // invK[2][0], invK[2][1] per level (-cx_l/fx_l, -cy_l/fy_l)
   int mode;                 // 1 vertex, 2 normal from stored vertex, 3 both from depth
   int down_from_left;       // Q3
+  // frame step: the tracking launches that follow start from zeroed barrier counters and
+  // ICP sum buffers, which block 0 writes here (in place of two memset nodes)
+  KfDevState* clear_state;
 };
 
 // (depth / 1000) * rotate(invK, (u, v, 1))  (depthToVert.cs:56)
@@ -92,6 +95,13 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256) vertex_normal_kernel(VNArgs one, const VNArgs* many) {
   const VNArgs& a = BATCH ? many[blockIdx.y] : one;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!BATCH && a.clear_state && blockIdx.x == 0) {
+    KfDevState* st = a.clear_state;
+    if (threadIdx.x == 0) st->barrier_count = 0u;
+    if (threadIdx.x == 1) st->sdf_barrier_count = 0u;
+    for (int k = threadIdx.x; k < (int)(sizeof(st->icp_acc) / sizeof(long long)); k += blockDim.x)
+      (&st->icp_acc[0][0][0])[k] = 0;
+  }
   if (gid >= a.start[3]) return;
   const int l = gid < a.start[1] ? 0 : (gid < a.start[2] ? 1 : 2);
   const int local = gid - a.start[l];
@@ -148,6 +158,7 @@ VNArgs make_vn_args(kf_session* s, int mode) {
   }
   a.start[3] = acc;
   a.mode = mode;
+  a.clear_state = nullptr;
   a.down_from_left = (s->cfg.quirks & KF_Q3_DOWN_FROM_LEFT) ? 1 : 0;
   return a;
 }
@@ -298,8 +309,9 @@ int kf_launch_pyramid(kf_session* s, const uint16_t* d_u16, const float* d_f32) 
   return KF_OK;
 }
 
-static int launch_vn(kf_session* s, int mode) {
+static int launch_vn(kf_session* s, int mode, bool clear = false) {
   VNArgs a = make_vn_args(s, mode);
+  if (clear) a.clear_state = s->d_state;
   const int threads = 256;
   const int blocks = (a.start[3] + threads - 1) / threads;
   vertex_normal_kernel<false><<<blocks, threads, 0, s->stream>>>(a, nullptr);
@@ -310,7 +322,7 @@ static int launch_vn(kf_session* s, int mode) {
 
 int kf_launch_vertex(kf_session* s) { return launch_vn(s, 1); }
 int kf_launch_normal(kf_session* s) { return launch_vn(s, 2); }
-int kf_launch_vertex_normal(kf_session* s) { return launch_vn(s, 3); }
+int kf_launch_vertex_normal(kf_session* s, bool clear_tracking_words) { return launch_vn(s, 3, clear_tracking_words); }
 
 // ---- batched: every member's uint16 upload buffer -> its pyramid, one launch per kernel ----
 int kf_batch_prepare_pyramid(kf_batch* b) {

@@ -345,12 +345,12 @@ cudaError_t launch_sdf(int storage, int blocks, cudaStream_t stream, const SdfAr
 
 }  // namespace
 
-int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy) {
+int kf_launch_sdf(kf_session* s, int recover, int gated, int frame_policy, bool counter_zero) {
   (void)frame_policy;
   const SdfArgs a = make_sdf_args(s, recover, gated);
   const int blocks = kf_occupancy_blocks(s, sdf_fn<false>(s->cfg.storage), KF_TRACK_THREADS, 0);
   if (blocks <= 0) return KF_ERR_CUDA;
-  KF_CUDA_TRY(s, cudaMemsetAsync(&s->d_state->sdf_barrier_count, 0, sizeof(unsigned), s->stream));
+  if (!counter_zero) KF_CUDA_TRY(s, cudaMemsetAsync(&s->d_state->sdf_barrier_count, 0, sizeof(unsigned), s->stream));
   KF_CUDA_TRY(s, launch_sdf<false>(s->cfg.storage, blocks, s->stream, a, SdfBatch{nullptr, nullptr}));
   kf_note_launch(s);
   return KF_OK;
