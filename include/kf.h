@@ -287,12 +287,19 @@ KF_API int kf_load_volume(kf_session* s, const char* path);
 KF_API int kf_selftest_barrier_timeout(kf_session* s, long long budget_cycles);
 KF_API int kf_get_pose_library_size(kf_session* s, int* n);
 /* Device times in milliseconds of the last call of each stage, in the order
- * pyramid, track, integrate, raycast, recover, mc. */
+ * pyramid, track, integrate, recover, raycast, mc (for frame steps: the last timed frame). */
 KF_API int kf_get_stage_times(kf_session* s, float ms[6]);
-/* Mean device milliseconds per stage (same order) over every kf_frame_step_* call since
- * the last kf_reset_stage_stats; read from per-frame events without stalling the stream. */
+/* Mean device milliseconds per stage (same order) over the timed frames of the
+ * kf_frame_step_* calls since the last kf_reset_stage_stats (*frames: how many); read from
+ * the frame graphs' events without stalling the stream. */
 KF_API int kf_get_stage_stats(kf_session* s, double mean_ms[6], uint64_t* frames);
 KF_API int kf_reset_stage_stats(kf_session* s);
+/* Which frame steps record their stage boundaries: every `every`-th (1, 2 or 4; 0 = none;
+ * default 4).  Each boundary is an event node in the frame's CUDA graph, ~5 us apiece on a
+ * B200, so timing every frame costs ~5 % of a 512^3 frame step.  No counterpart in the
+ * reference, whose stage timers are never assigned (gFusion.h:598-604). */
+KF_API int kf_set_stage_timing(kf_session* s, int every);
+KF_API int kf_get_stage_timing(kf_session* s, int* every);
 /* Kernels this session has launched (a frame step counts every kernel of its graph). */
 KF_API int kf_get_launch_count(kf_session* s, uint64_t* launches);
 KF_API int kf_get_stream(kf_session* s, void** cuda_stream);

@@ -158,6 +158,8 @@ class GFusion {
     check(kf_get_stage_times(s_, t.data()), "kf_get_stage_times");
     return t;
   }
+  // which frame steps record their stage boundaries (every 1, 2 or 4; 0 = none)
+  void setStageTiming(int every) { check(kf_set_stage_timing(s_, every), "kf_set_stage_timing"); }
   kf_session* handle() { return s_; }
 
  private:

@@ -158,6 +158,8 @@ SIGNATURES = {
     "kf_get_stage_times": (_I, [_P, _PF]),
     "kf_get_stage_stats": (_I, [_P, _PD, C.POINTER(C.c_uint64)]),
     "kf_reset_stage_stats": (_I, [_P]),
+    "kf_set_stage_timing": (_I, [_P, _I]),
+    "kf_get_stage_timing": (_I, [_P, C.POINTER(C.c_int)]),
     "kf_get_launch_count": (_I, [_P, C.POINTER(C.c_uint64)]),
     "kf_get_stream": (_I, [_P, C.POINTER(_P)]),
     "kf_mc_extract": (_I, [_P, C.c_float, _I, C.POINTER(C.c_uint32)]),

@@ -246,17 +246,21 @@ uint16_t* slot_frame(kf_session* s, int slot) {
 }
 
 // The device part of one frame of kinect.cpp:654-695 (input already in the slot's frame),
-// with stage events ev[0..5]: start, pyramid, track, integrate, recover, raycast (event
-// record nodes in the captured graph, so they can be timed after every replay).
-int enqueue_frame(kf_session* s, cudaEvent_t* ev, int slot) {
+// with events ev[0..5]: start, pyramid, track, integrate, recover, raycast (event record
+// nodes in the captured graph, so they can be timed after every replay) when `stages`;
+// otherwise the graph holds no event node and run_frame records the frame's end after it.
+int enqueue_frame(kf_session* s, cudaEvent_t* ev, int slot, bool stages) {
   int rc;
-  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[0], s->stream, cudaEventRecordExternal));
+  auto boundary = [&](int k) {
+    return stages ? cudaEventRecordWithFlags(ev[k], s->stream, cudaEventRecordExternal) : cudaSuccess;
+  };
+  KF_CUDA_TRY(s, boundary(0));
   if ((rc = kf_launch_depth_ingest(s, slot_frame(s, slot), nullptr))) return rc;
   // the vertex/normal launch also zeroes the tracking launches' barrier counters and ICP
   // sums (3.5 us per frame less than two memset nodes); in ICP mode nothing else touches the
   // SDF counter before the recover launch, in SDF mode the tracking launch does
   if ((rc = kf_launch_vertex_normal(s, true))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[1], s->stream, cudaEventRecordExternal));
+  KF_CUDA_TRY(s, boundary(1));
   const bool sdf_mode = s->cfg.tracking == KF_TRACK_SDF;
   if (sdf_mode) {
     if ((rc = kf_launch_sdf(s, 0, 0, 1, true))) return rc;
@@ -264,13 +268,13 @@ int enqueue_frame(kf_session* s, cudaEvent_t* ev, int slot) {
   } else {
     if ((rc = kf_launch_icp(s, 1, true))) return rc;
   }
-  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[2], s->stream, cudaEventRecordExternal));
+  KF_CUDA_TRY(s, boundary(2));
   if ((rc = kf_launch_integrate(s, 1))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[3], s->stream, cudaEventRecordExternal));
+  KF_CUDA_TRY(s, boundary(3));
   if ((rc = kf_launch_sdf(s, 1, 1, 0, !sdf_mode))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[4], s->stream, cudaEventRecordExternal));
+  KF_CUDA_TRY(s, boundary(4));
   if ((rc = kf_launch_raycast(s))) return rc;
-  KF_CUDA_TRY(s, cudaEventRecordWithFlags(ev[5], s->stream, cudaEventRecordExternal));
+  KF_CUDA_TRY(s, boundary(5));
   return KF_OK;
 }
 
@@ -291,13 +295,15 @@ int count_kernels(cudaGraph_t g) {
 int harvest(kf_session* s, int slot) {
   if (!s->ring_pending[slot]) return KF_OK;
   KF_CUDA_TRY(s, cudaEventSynchronize(s->ring_ev[slot][5]));
-  for (int i = 0; i < 5; ++i) {
-    float ms = 0.0f;
-    KF_CUDA_TRY(s, cudaEventElapsedTime(&ms, s->ring_ev[slot][i], s->ring_ev[slot][i + 1]));
-    s->stage_ms[i] = ms;
-    s->stage_acc[i] += ms;
+  if (s->ring_stages[slot]) {
+    for (int i = 0; i < 5; ++i) {
+      float ms = 0.0f;
+      KF_CUDA_TRY(s, cudaEventElapsedTime(&ms, s->ring_ev[slot][i], s->ring_ev[slot][i + 1]));
+      s->stage_ms[i] = ms;
+      s->stage_acc[i] += ms;
+    }
+    s->stage_frames += 1;
   }
-  s->stage_frames += 1;
   s->ring_pending[slot] = 0;
   return KF_OK;
 }
@@ -320,7 +326,8 @@ int run_frame(kf_session* s) {
     cudaGraph_t g = nullptr;
     KF_CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     s->capturing = true;
-    int rc = enqueue_frame(s, s->ring_ev[slot], slot);
+    const bool stages = s->stage_every > 0 && slot % s->stage_every == 0;
+    int rc = enqueue_frame(s, s->ring_ev[slot], slot, stages);
     s->capturing = false;
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
     if (rc) {
@@ -329,6 +336,7 @@ int run_frame(kf_session* s) {
     }
     if (e != cudaSuccess) return fail(s, KF_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
     s->frame_kernels = count_kernels(g);
+    s->ring_stages[slot] = stages ? 1 : 0;
     e = cudaGraphInstantiate(&s->frame_exec[slot], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
@@ -339,6 +347,8 @@ int run_frame(kf_session* s) {
   int rc = harvest(s, slot);  // the frame that used this slot kRing frames ago
   if (rc) return rc;
   KF_CUDA_TRY(s, cudaGraphLaunch(s->frame_exec[slot], s->stream));
+  // an untimed frame's end, recorded on the stream outside its graph
+  if (!s->ring_stages[slot]) KF_CUDA_TRY(s, cudaEventRecord(s->ring_ev[slot][5], s->stream));
   if ((rc = kf_note_integrate(s, s->stream))) return rc;
   s->ring_pending[slot] = 1;
   s->frames_run += 1;
@@ -804,9 +814,9 @@ int kf_frame_step_u16_async(kf_session* s, const uint16_t* host_depth_mm) {
   const size_t px = (size_t)s->W[0] * s->H[0];
   const int slot = (int)(s->frames_run % kf_session::kRing);  // the graph slot run_frame uses
   // the upload overlaps the frame still running: it goes on the copy stream once the last
-  // frame of this slot has read its input (the slot's pyramid-stage event), and the frame
-  // waits for it
-  if (s->ring_ev[slot][1]) KF_CUDA_TRY(s, cudaStreamWaitEvent(s->copy_stream, s->ring_ev[slot][1], 0));
+  // frame of this slot (kRing frames ago) has finished with its input, and the frame waits
+  // for it
+  if (s->ring_ev[slot][5]) KF_CUDA_TRY(s, cudaStreamWaitEvent(s->copy_stream, s->ring_ev[slot][5], 0));
   KF_CUDA_TRY(s, cudaMemcpyAsync(slot_frame(s, slot), host_depth_mm, px * 2, cudaMemcpyHostToDevice, s->copy_stream));
   KF_CUDA_TRY(s, cudaEventRecord(s->upload_ev[slot], s->copy_stream));
   KF_CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->upload_ev[slot], 0));
@@ -1192,6 +1202,22 @@ int kf_get_pose_library_size(kf_session* s, int* n) {
   int rc = pull_state(s);
   if (rc) return rc;
   *n = s->h_state->lib_size;
+  return KF_OK;
+}
+
+int kf_set_stage_timing(kf_session* s, int every) {
+  if (!s || !(every == 0 || every == 1 || every == 2 || every == 4)) return KF_ERR_INVALID_ARGUMENT;
+  KF_CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  int rc = harvest_all(s);  // the frames already run keep their stage times
+  if (rc) return rc;
+  drop_graph(s);  // the captured frames hold the old event layout
+  s->stage_every = every;
+  return KF_OK;
+}
+
+int kf_get_stage_timing(kf_session* s, int* every) {
+  if (!s || !every) return KF_ERR_INVALID_ARGUMENT;
+  *every = s->stage_every;
   return KF_OK;
 }
 

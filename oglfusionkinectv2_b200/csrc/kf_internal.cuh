@@ -129,12 +129,17 @@ struct kf_session {
 
   int track_blocks = 0;  // persistent grid of the tracking kernels
 
-  // frame-step CUDA graphs: a ring of instances, each with its own stage events, so the
-  // stage times of every frame can be read back without stalling the stream
+  // frame-step CUDA graphs: a ring of instances, each with its own events, so the stage
+  // times can be read back without stalling the stream.  An event node costs ~5 us of a
+  // ~0.43 ms frame, so only every stage_every-th slot's graph records the frame's start, its
+  // four stage boundaries and its end (by default one slot in four); the others hold no
+  // event node, and their end is recorded on the stream after the graph.
   static const int kRing = 4;
   cudaGraphExec_t frame_exec[kRing] = {};
   cudaEvent_t ring_ev[kRing][6] = {};
   int ring_pending[kRing] = {};  // slot holds an unread frame
+  int ring_stages[kRing] = {};   // slot's graph records the stage boundaries
+  int stage_every = 4;           // kf_set_stage_timing: 0 (none), 1, 2 or 4
   // asynchronous frame steps (kf_frame_step_u16_async): each step's result head is copied into
   // the pinned slot of its frame graph and read by the next call
   char* h_heads = nullptr;            // pinned, kRing * KF_STATE_RESULT_BYTES (first use)

@@ -399,11 +399,20 @@ class GFusion:
 
     def stageStats(self):
         """(mean device ms per stage [pyramid, track, integrate, recover, raycast, mc],
-        frames) over every frame step since resetStageStats()."""
+        frames) over the timed frame steps (setStageTiming) since resetStageStats()."""
         a = (C.c_double * 6)()
         n = C.c_uint64()
         self._check(self.lib.kf_get_stage_stats(self._h, a, C.byref(n)), "kf_get_stage_stats")
         return np.array(list(a)), n.value
+
+    def setStageTiming(self, every: int) -> None:
+        """Record the stage boundaries of every `every`-th frame step (1, 2 or 4; 0 = none)."""
+        self._check(self.lib.kf_set_stage_timing(self._h, int(every)), "kf_set_stage_timing")
+
+    def stageTiming(self) -> int:
+        e = C.c_int()
+        self._check(self.lib.kf_get_stage_timing(self._h, C.byref(e)), "kf_get_stage_timing")
+        return e.value
 
     def resetStageStats(self) -> None:
         self._check(self.lib.kf_reset_stage_stats(self._h), "kf_reset_stage_stats")

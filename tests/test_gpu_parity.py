@@ -234,6 +234,35 @@ def test_frame_step_graph_matches_step_by_step():
     np.testing.assert_array_equal(a.getVerts(), b.getVerts())
 
 
+def test_stage_timing_sampling():
+    """kf_set_stage_timing: the frame graphs of every n-th ring slot record the stage
+    boundaries (default n = 4), the others the frame only; the frames compute the same."""
+    w = small_workload(13, size=64)
+    a, b = GFusion(w.config, w.intrinsics), GFusion(w.config, w.intrinsics)
+    assert a.stageTiming() == 4
+    b.setStageTiming(1)
+    with pytest.raises(L.KfError):
+        b.setStageTiming(3)
+    for s in (a, b):
+        s.Reset(w.poses[0])
+        s.resetStageStats()
+    for k in range(8):
+        f = w.frame(k)
+        assert a.frameStep(f) == b.frameStep(f)
+    ma, na = a.stageStats()
+    mb, nb = b.stageStats()
+    assert (na, nb) == (2, 8)
+    assert np.all(ma[:5] > 0) and np.all(mb[:5] > 0)
+    np.testing.assert_array_equal(a.getPose(), b.getPose())
+    b.setStageTiming(0)  # frames already run keep their times; no more are timed
+    for k in range(8, 13):
+        f = w.frame(k)
+        assert a.frameStep(f) == b.frameStep(f)
+    assert b.stageStats()[1] == 8 and a.stageStats()[1] == 4
+    np.testing.assert_array_equal(a.getPose(), b.getPose())
+    np.testing.assert_array_equal(a.getVolumeRaw(), b.getVolumeRaw())
+
+
 def test_async_frame_steps_match_sync_steps():
     """Pipelined frame steps: each call reads the previous frame's result; the session ends
     exactly where synchronous steps take it."""
