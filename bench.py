@@ -180,7 +180,7 @@ def measured_traffic(workload: str, stage: str):
     """DRAM bytes (read + write) per launch of the stage's kernel from the committed ncu capture
     of this workload (profiles/*_traffic.txt: "<kernel> <workload> dram_bytes_per_launch <n>"),
     or None when none was captured."""
-    kernel = {"integrate": "integrate_kernel", "raycast": "raycast_kernel"}.get(stage)
+    kernel = {"integrate": "integrate_kernel", "raycast": "raycast_kernel", "track": "icp_kernel"}.get(stage)
     for path in glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "*_traffic.txt")):
         for line in open(path):
             f = line.split()
@@ -207,7 +207,24 @@ def algorithmic_bytes(cfg, stage):
         return 2 * bv * n + 4 * p0
     if stage == "raycast":                     # value plane read once, vertex + normal out
         return (bv // 2) * n + 32 * p0
+    if stage == "track":                       # per ICP iteration at level l: 4 float4 maps read
+        return sum(int(it) * 64 * (p0 >> (2 * l)) for l, it in enumerate(cfg.iterations))
     raise ValueError(stage)
+
+
+def stage_rooflines(w, per, peak):
+    out = {}
+    for stage in ("integrate", "raycast", "track"):
+        ms = per.get(stage) or 0.0
+        if ms <= 0:
+            continue
+        algo = algorithmic_bytes(w.config, stage)
+        gbs = algo / (ms / 1000.0) / 1e9
+        traffic = measured_traffic(w.name, stage)
+        out[stage] = {"algorithmic_bytes": algo, "ms": ms, "achieved": gbs, "frac": gbs / peak,
+                      "traffic": traffic,
+                      "traffic_frac": (traffic / (ms / 1000.0) / 1e9 / peak if traffic else None)}
+    return out
 
 
 CPU_WARM_FRAMES = 2  # untimed oracle frames before the timed cpu_baseline sample
@@ -852,7 +869,10 @@ def main():
                          # the DRAM bytes the kernel really moves (ncu capture) over its time
                          "traffic_gbs": (traffic / (per[dom] / 1000.0) / 1e9 if traffic and per[dom] > 0 else None),
                          "traffic_frac": (traffic / (per[dom] / 1000.0) / 1e9 / peak if traffic and per[dom] > 0 else None),
-                         "traffic_source": "profiles/*_traffic.txt (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
+                         "traffic_source": "profiles/*_traffic.txt (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                         # the same figures for the three frame kernels (byte model over the
+                         # stage's event-timed mean; ncu DRAM bytes where captured)
+                         "stages": stage_rooflines(w, per, peak)},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "tracked_last": bool(tracked_ok),
