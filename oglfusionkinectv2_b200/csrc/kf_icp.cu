@@ -682,18 +682,26 @@ int kf_batch_prepare_icp(kf_batch* b) {
   const int total = kf_occupancy_blocks(s0, fn, KF_TRACK_THREADS, 0);
   if (total <= 0) return KF_ERR_CUDA;
   b->icp_blocks = total;
-  return kf_batch_block_map(b, total, &b->icp_map);
+  b->icp_waves = 0;
+  for (int e0 = 0; e0 < n; e0 += KF_BATCH_ICP_WAVE) {
+    int rc = kf_batch_block_map_range(b, total, e0, std::min(n, e0 + KF_BATCH_ICP_WAVE), &b->icp_wave_map[b->icp_waves]);
+    if (rc) return rc;
+    ++b->icp_waves;
+  }
+  return KF_OK;
 }
 
 int kf_batch_launch_icp(kf_batch* b) {
-  cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = coop_config(dim3(b->icp_blocks), b->stream, attr);
-  const IcpBatch batch = {static_cast<const IcpArgs*>(b->icp_args), b->icp_map};
-  const IcpArgs none{};
-  if (b->members[0]->cfg.jtj == KF_JTJ_SPLIT_BF16)
-    KF_CUDA_TRY(b, cudaLaunchKernelEx(&cfg, icp_kernel<1, true>, none, batch));
-  else
-    KF_CUDA_TRY(b, cudaLaunchKernelEx(&cfg, icp_kernel<0, true>, none, batch));
-  b->launches += 1;
+  for (int w = 0; w < b->icp_waves; ++w) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = coop_config(dim3(b->icp_blocks), b->stream, attr);
+    const IcpBatch batch = {static_cast<const IcpArgs*>(b->icp_args), b->icp_wave_map[w]};
+    const IcpArgs none{};
+    if (b->members[0]->cfg.jtj == KF_JTJ_SPLIT_BF16)
+      KF_CUDA_TRY(b, cudaLaunchKernelEx(&cfg, icp_kernel<1, true>, none, batch));
+    else
+      KF_CUDA_TRY(b, cudaLaunchKernelEx(&cfg, icp_kernel<0, true>, none, batch));
+    b->launches += 1;
+  }
   return KF_OK;
 }
