@@ -56,6 +56,26 @@ def test_batch_equals_alone_bit_exact():
     assert (t >= 0).all() and t[1] > 0
 
 
+def test_batch_icp_waves_bit_exact():
+    """More members than one ICP wave holds (KF_BATCH_ICP_WAVE = 32): the batched ICP runs as
+    two cooperative launches; every member still matches its alone run bit for bit."""
+    F, n = 3, 36
+    ws = [small_workload(F, size=48, storage=L.KF_STORAGE_F16U16, jtj=L.KF_JTJ_SPLIT_BF16,
+                         quirks=L.KF_QUIRKS_TRACKING, seed=0xC0FFEE + 101 + 7 * k) for k in range(n)]
+    frames = [[w.frame(k) for k in range(F)] for w in ws]
+    alone = fresh(ws)
+    for i, g in enumerate(alone):
+        for k in range(F):
+            g.frameStep(frames[i][k])
+    together = fresh(ws)
+    batch = GFusionBatch(n)
+    for k in range(F):
+        batch.frameStep(together, [frames[i][k] for i in range(n)])
+    for ga, gb in zip(alone, together):
+        np.testing.assert_array_equal(ga.getPose(), gb.getPose())
+        np.testing.assert_array_equal(ga.getVerts(), gb.getVerts())
+
+
 def test_batch_membership_changes():
     """Sessions join and leave between steps; each still matches its alone run."""
     F = 5
