@@ -309,6 +309,37 @@ def test_pose_library_and_recover():
     assert np.linalg.norm(Pg[:3, 3] - Po[:3, 3]) <= 1e-3
 
 
+def test_frame_graph_recover_matches_step_by_step():
+    """In the frame graph the recover launch is the body of a conditional node that the ICP
+    kernel sets when the frame is not tracked: a lost frame (the wall) runs it, a tracked
+    one does not, and both match the entry points called one by one, bit for bit."""
+    w = small_workload(7, size=64)
+    a, b = GFusion(w.config, w.intrinsics), GFusion(w.config, w.intrinsics)
+    for s in (a, b):
+        s.Reset(w.poses[0])
+    wall = np.full((424, 512), 4200, np.uint16)
+    frames = [w.frame(k) for k in range(5)] + [wall, w.frame(5)]
+    counter, reset = 0, True
+    for k, f in enumerate(frames):
+        ta = a.frameStep(f)
+        b.depthToVertex(f)
+        b.vertexToNormal()
+        tb = b.Track()
+        if tb or reset:
+            b.integrate()
+            if counter > 2:
+                reset = False
+        if not tb:
+            b.recoverPose()
+        counter += 1
+        b.raycast()
+        assert ta == tb, k
+        assert ta == (k != 5), k  # the wall is the one frame not tracked
+        np.testing.assert_array_equal(a.getPose(), b.getPose())
+    np.testing.assert_array_equal(a.getVolumeRaw(), b.getVolumeRaw())
+    np.testing.assert_array_equal(a.getVerts(), b.getVerts())
+
+
 def test_errors_are_reported():
     w = small_workload(1, size=32)
     g = GFusion(w.config, w.intrinsics)
