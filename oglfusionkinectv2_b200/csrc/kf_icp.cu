@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
   __shared__ float s_pw[JTJ ? 1 : kWarps][4];
   __shared__ long long s_fix[JTJ ? kWarps : 1][72];
   __shared__ double s_sums[32];
-  __shared__ double s_csums[29], s_ccenter[3], s_ae;  // last centred row (for the tail)
+  __shared__ double s_csums[29], s_ccenter[3];  // last centred row (for the tail)
   __shared__ double s_nvalid;                           // its valid-pixel count
   __shared__ double s_gx[8 + 228];                      // the step (+ rank guard's scratch)
   __shared__ int s_fast;                                // the rank check's verdict
@@ -496,15 +496,16 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
         // the centred row and its centre; the tail turns the last one into the world form
         if (lane < 28) s_csums[lane] = s_sums[lane];
         if (lane == 28) s_csums[28] = count;
-        if (lane == 29) {
-          const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] +
-                                  x[4] * x[4] + x[5] * x[5]);
-          s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
-        }
-        if (lane == 30) s_ae = sqrt(s_sums[0] / count);  // getReduction :1167
+        // the convergence test and the next centre (this iteration's centroid of the valid
+        // points) in every lane: one instruction stream, no divergent FP64 square root or
+        // division on the hand-over's path
+        const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3] +
+                                x[4] * x[4] + x[5] * x[5]);
+        if (lane == 29) s_conv = (nrm < 1e-5 && nrm != 0.0) ? 1 : 0;
         if (lane == 31) s_nvalid = nvalid;
-        // next centre: this iteration's centroid of the valid points
-        const double cn = lane < 3 ? (nvalid > 0 ? s_sums[29 + lane] / nvalid : s_cd[lane]) : 0.0;
+        const int ci = lane < 3 ? lane : 2;
+        const double centroid = s_sums[29 + ci] / nvalid;  // unused when nvalid == 0
+        const double cn = nvalid > 0 ? centroid : s_cd[ci];
         __syncwarp();
         if (lane < 16) {
           s_pose[lane] = pn;
@@ -527,7 +528,7 @@ __global__ void __launch_bounds__(KF_TRACK_THREADS, 2) icp_kernel(IcpArgs a_one,
 
   // ---------------- Track() tail (:715-723) + frame policy, block 0 only -----------------
   if (local != 0 || tid != 0 || !ok) return;
-  const double ae = iters_run ? s_ae : 0.0;
+  const double ae = iters_run ? sqrt(s_csums[0] / s_csums[28]) : 0.0;  // getReduction :1167
   st->ae = ae;
   if (iters_run) {
     // the last reduction row in the reference's world form: b = M b', C = M C' M^T,
